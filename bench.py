@@ -1,0 +1,356 @@
+#!/usr/bin/env python
+"""Headline benchmark: exact triangle count of the scale-24 R-MAT graph on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl xtric|reference]
+
+Workload (one step): one exact count of R-MAT scale 24 (16,777,216 vertices,
+edge factor 16 -> 268,435,456 generated edges; quadrants .57/.19/.19/.05 with
+10% per-level noise; ids permuted; symmetrised, deduplicated, self loops
+dropped; degree-oriented int32 columns / int64 offsets), graph resident in
+HBM. Metric: oriented edges counted per second (|E+| per step / step time).
+
+  value : device time of the count kernel over K steps (CUDA events on the
+          launching stream), graph already in HBM. The graph (2.1 GB of CSR
+          + transpose) is far larger than L2 (126 MB), so no flush is needed.
+  e2e   : the same metric through the public C ABI with host buffers: the
+          int32 edge list copied from pinned host memory, built into the
+          oriented CSR on the device, counted, the count read back.
+N > 1 GPUs (torchrun): independent replicas, one graph per GPU, no data-path
+collective; value = all ranks' edges / the slowest rank's time.
+
+--impl reference times the reference's own CPU counting path
+(oracle/_ref/tric_omp: main.cpp + xxtric.hpp built with USE_OPENMP against a
+one-rank MPI shim) on this host's cores, on a bounded sample of the same
+workload: the R-MAT graph of the same generator at scale 18.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "oriented edges/s"
+UNIT = "edges/s"
+SCALE = 24
+EDGE_FACTOR = 16
+SEED = 1
+SAMPLE_SCALE = 18
+WORKLOAD = ("R-MAT scale 24, edge factor 16 (a=.57 b=.19 c=.19 d=.05, 10% per-level noise, ids permuted), "
+            "symmetrised + deduped + loops dropped, degree-oriented, int32 cols / int64 offsets")
+
+
+def measured_peaks() -> dict:
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return {"hbm_gbs": float(d["hbm_gbs"]), "source": "measured"}
+    return {"hbm_gbs": 6650.0, "source": "fallback"}
+
+
+def profiled_traffic(name: str):
+    """DRAM bytes per launch of k_count on this workload from the committed
+    ncu summary (profiles/<name>), if one exists."""
+    p = os.path.join(ROOT, "profiles", name)
+    if not os.path.exists(p):
+        return None
+    for line in open(p):
+        if line.strip().startswith("dram_bytes_per_launch_full_size:"):
+            try:
+                return int(float(line.split(":")[1].split()[0]))
+            except ValueError:
+                return None
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi sampling of SM clocks and throttle reasons during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.idx = gpu_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.out = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                          "-i", str(self.idx), "-lms", "100"], stdout=self.out,
+                                         stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        time.sleep(0.3)
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.2)
+        self.proc.terminate()
+        try:
+            self.proc.wait(5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.out.close()
+        rows = []
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                rows.append((float(parts[1]), float(parts[2]), float(parts[3]), parts[4:]))
+            except ValueError:
+                continue
+        os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        smax = max(r[1] for r in rows)
+        loaded = [r for r in rows if r[2] > 250.0] or rows
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in loaded:
+            for n, v in zip(names, r[3][1:]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(r[0] for r in loaded), "sm_max_mhz": smax,
+                "power_w_max": max(r[2] for r in rows), "samples": len(rows), "samples_under_load": len(loaded),
+                "reasons": sorted(reasons)}
+
+
+# ---------------------------------------------------------------------------
+# CPU baseline: the reference's own CPU path on a sample of the workload
+# ---------------------------------------------------------------------------
+
+def reference_sample(scale: int = SAMPLE_SCALE):
+    """R-MAT graph of the same generator at a smaller scale, as a vite file."""
+    import oracle
+    n = 1 << scale
+    src, dst = oracle.rmat_edges(scale, EDGE_FACTOR << scale, SEED)
+    off, tails = oracle.canon_csr(n, src, dst)
+    path = os.path.join(tempfile.gettempdir(), f"xtric_rmat{scale}_{os.getpid()}.bin")
+    rec = np.zeros(len(tails), dtype=[("t", "<i8"), ("w", "<f8")])
+    rec["t"] = tails
+    rec["w"] = 1.0
+    with open(path, "wb") as f:
+        np.array([n, len(tails)], np.int64).tofile(f)
+        off.tofile(f)
+        rec.tofile(f)
+    return path, off, tails, len(tails) // 2
+
+
+def time_reference_once(path: str, off, tails, cores: int) -> tuple[float, str, int]:
+    """Seconds of one reference count. Prefers the reference's own binary;
+    falls back to the oracle's restatement when it is not built."""
+    import oracle
+    if os.path.exists(oracle.REF_TRIC_OMP):
+        r = oracle.run_ref(["-f", path], omp=True, threads=cores, timeout=1800)
+        if r["rc"] != 0 or "t_local" not in r:
+            raise RuntimeError("reference binary failed:\n" + r["stdout"][-2000:])
+        # the count runs inside the constructor on one rank (xxtric.hpp:150-223);
+        # main times only count() (main.cpp:158-183): report both phases
+        return r["t_local"] + r.get("t_count", 0.0), "reference", r.get("triangles", -1)
+    os.environ["OMP_NUM_THREADS"] = str(cores)
+    t0 = time.perf_counter()
+    t = oracle.count_xxtric(off, tails)
+    return time.perf_counter() - t0, "port", t
+
+
+def cpu_baseline(cores: int, steps: int = 1, warmup: int = 0) -> dict:
+    path, off, tails, n_edges = reference_sample()
+    try:
+        ts = []
+        kind = "reference"
+        tri = -1
+        for i in range(warmup + steps):
+            t, kind, tri = time_reference_once(path, off, tails, cores)
+            if i >= warmup:
+                ts.append(t)
+    finally:
+        os.unlink(path)
+    total = sum(ts)
+    return {"value": n_edges * len(ts) / total, "unit": UNIT, "cores": cores, "kind": kind,
+            "sample": f"R-MAT scale {SAMPLE_SCALE} of the same generator ({n_edges} oriented edges, "
+                      f"{tri} triangles), reference OpenMP CPU count, {len(ts)} run(s), "
+                      f"{total / len(ts):.3f} s per run",
+            "seconds_per_run": total / len(ts), "n_edges": n_edges}
+
+
+def run_reference_arm(args) -> None:
+    from xxtric_b200 import replicas
+    rank, world, _ = replicas.env_ranks()
+    if rank != 0:
+        return  # rank 0 alone times the CPU reference
+    cores = os.cpu_count() or 1
+    try:
+        cb = cpu_baseline(cores, steps=args.steps, warmup=args.warmup)
+    except Exception as e:  # report, never fake a number
+        print(json.dumps({"impl": "reference", "unavailable": f"reference CPU path failed: {e}"[:300]}))
+        return
+    line = {"metric": METRIC, "value": cb["value"], "unit": UNIT, "impl": "reference", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * cb["seconds_per_run"],
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int64",
+            "data": "synthetic", "config": config_dict(world, None),
+            "cpu_baseline": {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")},
+            "e2e": {"value": cb["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
+def config_dict(world: int, info: dict | None) -> dict:
+    c = {"workload": WORKLOAD, "scale": SCALE, "edge_factor": EDGE_FACTOR, "seed": SEED, "orient": "degree",
+         "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+         "l2": "inputs larger than L2 (CSR + transpose > 2 GB), no flush"}
+    if info:
+        c.update({"nv": info["nv"], "oriented_edges": info["n_edges"], "max_degree": info["max_degree"],
+                  "max_out_degree": info["max_out_degree"]})
+    return c
+
+
+# ---------------------------------------------------------------------------
+# the product arm
+# ---------------------------------------------------------------------------
+
+def run_xtric(args) -> None:
+    import torch
+
+    import xxtric_b200 as xt
+    from xxtric_b200 import replicas
+
+    rank, world, local = replicas.init(backend="nccl")
+    torch.cuda.set_device(local)
+    stream = torch.cuda.current_stream()
+    ctx = xt.Context(local)
+    ctx.set_stream(stream.cuda_stream)
+    n = 1 << SCALE
+    ne = EDGE_FACTOR << SCALE
+    src = torch.empty(ne, dtype=torch.int32, device="cuda")
+    dst = torch.empty_like(src)
+    ctx.gen_rmat(SCALE, ne, SEED, src, dst)
+    g = ctx.graph_from_device_edges(n, ne, src, dst, xt.ORIENT_DEGREE)
+    info = g.info()
+    d_count = torch.zeros(1, dtype=torch.int64, device="cuda")
+
+    counts = []
+    for _ in range(args.warmup):
+        g.count_async(d_count)
+        counts.append(int(d_count.item()))
+
+    replicas.barrier()
+    torch.cuda.synchronize()
+    sampler = ClockSampler(torch.cuda.current_device()) if rank == 0 else None
+    if sampler:
+        sampler.start()
+    l0 = ctx.launches
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    start = torch.cuda.Event(enable_timing=True)
+    end = torch.cuda.Event(enable_timing=True)
+    start.record(stream)
+    for k in range(args.steps):
+        ev[k][0].record(stream)
+        g.count_async(d_count)
+        ev[k][1].record(stream)
+    end.record(stream)
+    torch.cuda.synchronize()
+    launches = ctx.launches - l0
+    clocks = sampler.stop() if sampler else None
+    replicas.barrier()
+    t_total = start.elapsed_time(end) / 1e3
+    t_kernel = statistics.mean(a.elapsed_time(b) for a, b in ev) / 1e3
+    counts.append(int(d_count.item()))
+    if len(set(counts)) != 1:
+        raise RuntimeError(f"count changed between steps: {counts}")
+    value, total_edges, t_max = replicas.aggregate(info["n_edges"] * args.steps, t_total)
+
+    # ---- end to end through the C ABI with host buffers ----
+    h_src = torch.empty(ne, dtype=torch.int32, pin_memory=True)
+    h_dst = torch.empty(ne, dtype=torch.int32, pin_memory=True)
+    h_src.copy_(src)
+    h_dst.copy_(dst)
+    del src, dst
+    g.free()
+    torch.cuda.synchronize()
+    torch.cuda.empty_cache()
+    hs, hd = h_src.numpy(), h_dst.numpy()
+    e2e_counts = []
+    for _ in range(1):  # warm the allocator pool and the builder
+        g2 = ctx.graph_from_edges(n, hs, hd, xt.ORIENT_DEGREE)
+        e2e_counts.append(g2.count())
+        g2.free()
+    replicas.barrier()
+    torch.cuda.synchronize()
+    e_start = torch.cuda.Event(enable_timing=True)
+    e_end = torch.cuda.Event(enable_timing=True)
+    e_start.record(stream)
+    for _ in range(args.e2e_steps):
+        g2 = ctx.graph_from_edges(n, hs, hd, xt.ORIENT_DEGREE)  # H2D + build + orient + plan
+        e2e_counts.append(g2.count())                          # count + D2H of the result
+        g2.free()
+    e_end.record(stream)
+    torch.cuda.synchronize()
+    t_e2e = e_start.elapsed_time(e_end) / 1e3
+    if set(e2e_counts) != set(counts):
+        raise RuntimeError(f"end-to-end count {e2e_counts} differs from {counts}")
+    e2e_value, _, _ = replicas.aggregate(info["n_edges"] * args.e2e_steps, t_e2e)
+
+    peaks = measured_peaks()
+    achieved = info["alg_bytes"] / t_kernel / 1e9
+    traffic = profiled_traffic("k_count_rmat_s24.md")
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1e3 * t_max / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic",
+        "config": config_dict(world, info), "triangles": counts[0],
+        "triangles_per_s": counts[0] * args.steps * world / t_max,
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                     "frac": achieved / peaks["hbm_gbs"], "traffic": traffic,
+                     "kernel": "k_count<false>", "alg_bytes_per_launch": info["alg_bytes"],
+                     "kernel_ms": 1e3 * t_kernel, "peak_source": peaks["source"],
+                     "tail_grouped_alg_bytes": info["tail_alg_bytes"]},
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 2 * 4 * ne, "d2h_bytes_per_step": 8,
+                "ms_per_step": 1e3 * t_e2e / args.e2e_steps, "steps": args.e2e_steps},
+        "gpu_launches": launches, "clocks": clocks,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            cb = cpu_baseline(os.cpu_count() or 1)
+            line["cpu_baseline"] = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")}
+        except Exception as e:
+            line["cpu_baseline"] = {"value": None, "unavailable": str(e)[:200]}
+    del ctx
+    replicas.finish()
+    if rank == 0:
+        print(json.dumps(line))
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--impl", choices=["xtric", "reference"], default="xtric")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)  # timing rule: at least 3 untimed warm-up steps
+    if args.impl == "reference":
+        run_reference_arm(args)
+    else:
+        run_xtric(args)
+
+
+if __name__ == "__main__":
+    main()

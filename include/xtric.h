@@ -1,0 +1,165 @@
+/*
+ * xtric.h — C ABI of the B200-native exact triangle counter (libxtb200.so).
+ *
+ * Every entry point takes plain pointers and sizes; no C++ or torch types
+ * cross this boundary. Host pointers are copied in; the library owns the
+ * device memory it allocates. One context = one device + one CUDA stream;
+ * calls on one context are serialised by the caller (the reference engine is
+ * single-threaded too, main.cpp:53-70). Nothing here aborts the process:
+ * every failure is a status code, and xt_last_error() has the detail.
+ *
+ * Each declaration names the reference interface (sg0/xxtric, file:line) it
+ * replaces. Counts are exact int64: a triangle {a,b,c} is counted once in the
+ * global count and credited to each of a, b and c in per-vertex counts (the
+ * convention of cugraph/cug_triangle_count.py:33-41).
+ */
+#ifndef XTRIC_H
+#define XTRIC_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+  XT_OK = 0,
+  XT_ERR_INVALID = 1,   /* bad argument: null pointer, negative size, id outside [0,nv) */
+  XT_ERR_CUDA = 2,      /* CUDA runtime or launch error */
+  XT_ERR_OOM = 3,       /* a device allocation failed */
+  XT_ERR_IO = 4,        /* file missing, short or with an inconsistent header */
+  XT_ERR_OVERFLOW = 5,  /* sizes outside the supported range (nv >= 2^31, ...) */
+  XT_ERR_TIMEOUT = 6,   /* a bounded device-side wait gave up */
+  XT_ERR_ADMISSION = 7, /* serving: the request can never fit the memory budget */
+  XT_ERR_NOT_READY = 8, /* serving: the result is not available yet */
+  XT_ERR_NO_DEVICE = 9, /* no CUDA device, or not an sm_100 device */
+  XT_ERR_CLOSED = 10    /* serving: the server is closed */
+} xt_status;
+
+/* Orientation of each undirected edge {a,b}: from the lower to the higher
+ * rank. XT_ORIENT_ID ranks by vertex id, the reference's precedence
+ * (u < v < w, xxtric.hpp:165, image/distributed-counting-precedence.png).
+ * XT_ORIENT_DEGREE ranks by (degree, id); the global count is identical. */
+typedef enum { XT_ORIENT_ID = 0, XT_ORIENT_DEGREE = 1 } xt_orient;
+
+/* xt_graph_from_csr flag: the CSR is already canonical (rows sorted, no
+ * duplicates, symmetric, no self loops), the contract under which the
+ * reference reads vite files (graph.hpp:294-395), so deduplication is skipped.
+ * Without it the rows are canonicalised on the device first. */
+#define XT_CSR_CANONICAL 1
+
+typedef struct xt_ctx xt_ctx;
+typedef struct xt_graph xt_graph;
+
+typedef struct {
+  int64_t nv;             /* vertices */
+  int64_t n_input;        /* input entries (directed CSR entries or edge-list rows) */
+  int64_t n_edges;        /* undirected unique non-loop edges == oriented edges |E+| */
+  int64_t max_degree;     /* max undirected degree */
+  int64_t max_out_degree; /* max d+ after orientation */
+  int64_t max_in_degree;  /* max d- after orientation */
+  int64_t wedge_work;     /* sum over oriented (u,v) of d+(v): items a tail-grouped count streams */
+  int64_t stream_work;    /* sum over oriented (u,v) of d+(u) = sum_u d+(u)^2: items this count streams */
+  int64_t alg_bytes;      /* bytes this count must read: 16(nv+1) + 8|E+| + sum (16 + 4 d+(u)) */
+  int64_t tail_alg_bytes; /* the tail-grouped figure: 8(nv+1) + 4|E+| + sum (16 + 4 d+(v)) */
+  int32_t orient;         /* xt_orient used */
+  int32_t reserved;
+} xt_graph_info;
+
+/* ---- context ------------------------------------------------------------
+ * Replaces the device set-up of TriangleCountingSingle's constructor
+ * (xxtric-gpu.hpp:40-44), which hard-codes device 0. */
+xt_status xt_open(int device, xt_ctx **out);
+xt_status xt_close(xt_ctx *ctx);
+/* use an existing cudaStream_t (passed as void*) instead of the context's own */
+xt_status xt_set_stream(xt_ctx *ctx, void *cuda_stream);
+const char *xt_strerror(xt_status s);
+const char *xt_last_error(const xt_ctx *ctx);
+/* test hook: make the k-th device allocation from now fail (k<=0 disarms) */
+xt_status xt_debug_fail_alloc(xt_ctx *ctx, int64_t k);
+/* number of this library's own kernels launched on the context so far
+ * (library sorts and scans from CUB are not included) */
+int64_t xt_launch_count(const xt_ctx *ctx);
+
+/* ---- graph build ---------------------------------------------------------
+ * Replaces TriangleCountingSingle(Graph*) (xxtric-gpu.hpp:27-156): host CSR in
+ * the vite layout of Graph (graph.hpp:52-275; offsets int64[nv+1], tails
+ * int64[offsets[nv]]) is copied to the device and turned into an oriented
+ * int32-column / int64-offset CSR there. */
+xt_status xt_graph_from_csr(xt_ctx *ctx, int64_t nv, const int64_t *offsets, const int64_t *tails, int flags,
+                            int orient, xt_graph **out);
+/* the same from a host edge list of ne (src,dst) rows with int32 ids; rows
+ * may repeat, appear in one direction only or be self loops */
+xt_status xt_graph_from_edges(xt_ctx *ctx, int64_t nv, int64_t ne, const int32_t *src, const int32_t *dst,
+                              int orient, xt_graph **out);
+/* the same from int32 edge lists already in device memory (not freed) */
+xt_status xt_graph_from_device_edges(xt_ctx *ctx, int64_t nv, int64_t ne, const int32_t *d_src,
+                                     const int32_t *d_dst, int orient, xt_graph **out);
+xt_status xt_graph_get_info(const xt_graph *g, xt_graph_info *info);
+/* copy the oriented CSR out (host buffers of nv+1 and n_edges entries) */
+xt_status xt_graph_get_csr(const xt_graph *g, int64_t *offsets, int32_t *cols);
+/* Replaces TriangleCountingSingle::clear() (xxtric-gpu.hpp:272-285). */
+xt_status xt_graph_free(xt_graph *g);
+
+/* ---- counting ------------------------------------------------------------
+ * Replaces TriangleCountingSingle::count() (xxtric-gpu.hpp:192-270): the
+ * global count, and per-vertex counts into a host array of nv entries when
+ * per_vertex is not null. Synchronous, like the reference. */
+xt_status xt_count(xt_graph *g, int64_t *global, int64_t *per_vertex);
+/* the same into device memory, asynchronous on the context stream;
+ * d_per_vertex (nullable) holds nv int64 entries and is overwritten */
+xt_status xt_count_async(xt_graph *g, int64_t *d_global, int64_t *d_per_vertex);
+
+/* Replaces the kernel launcher single_gpu_count(nv, d_indices, d_edge_list,
+ * d_local_count) (counting.cuh:259-265, counting.cu:537-577): the reference's
+ * device CSR (int64 offsets, int64 tails; rows sorted, deduped, symmetric)
+ * is oriented and counted on the given stream. Unlike the reference, which
+ * accumulates into a caller-zeroed counter and reports nothing, this
+ * overwrites *d_count (accumulate != 0 adds instead) and returns errors.
+ * Scratch memory is allocated stream-ordered and released before return. */
+xt_status xt_count_device(int64_t nv, const int64_t *d_indices, const int64_t *d_edge_list, int64_t *d_count,
+                          int accumulate, void *cuda_stream);
+
+/* ---- synthetic inputs on the device --------------------------------------
+ * Deterministic counter-based generators (same bits for the same seed on any
+ * GPU and in the CPU oracle). Outputs are device int32 arrays of ne rows. */
+/* R-MAT: 2^scale vertices, quadrant weights in 1/65536 units, +-noise_pct %
+ * multiplicative noise per edge and level, ids permuted when permute != 0 */
+xt_status xt_gen_rmat(xt_ctx *ctx, int scale, int64_t ne, uint64_t seed, int a16, int b16, int c16,
+                      int noise_pct, int permute, int32_t *d_src, int32_t *d_dst);
+/* Chung-Lu from a host integer CDF of n+1 entries (see xt_chunglu_cdf) */
+xt_status xt_gen_chunglu(xt_ctx *ctx, int64_t n, const uint64_t *cdf, int64_t ne, uint64_t seed, int permute,
+                         int32_t *d_src, int32_t *d_dst);
+/* Chung-Lu integer weight CDF (host): n+1 entries; returns the edge count */
+int64_t xt_chunglu_cdf(int64_t n, double gamma, double mean_deg, double max_deg, uint64_t *cdf);
+/* Erdos-Renyi G(n, ne): uniform ordered pairs */
+xt_status xt_gen_er(xt_ctx *ctx, int64_t n, int64_t ne, uint64_t seed, int32_t *d_src, int32_t *d_dst);
+
+/* ---- host-side graph input (no device needed) ------------------------------ */
+
+/* Replaces BinaryEdgeList::read (graph.hpp:294-395) for one process: the vite
+ * binary layout [nv][ne][offsets: nv+1][ne x {tail, weight}] with 8-byte
+ * fields (elem_bytes 8, the default GraphElem/GraphWeight of deftypes.hpp:
+ * 45-49) or 4-byte fields (elem_bytes 4, USE_32_BIT_GRAPH, deftypes.hpp:40-44).
+ * With offsets == NULL only *nv and *ne are filled (sizing call). The file
+ * size must match the header exactly; weights are skipped. */
+xt_status xt_vite_read(const char *path, int elem_bytes, int64_t *nv, int64_t *ne, int64_t *offsets,
+                       int64_t *tails);
+/* writes the same layout with unit weights */
+xt_status xt_vite_write(const char *path, int elem_bytes, int64_t nv, const int64_t *offsets,
+                        const int64_t *tails);
+
+/* Replaces GenerateRGG(nv).generate(LCG, unit weights, random_edge_pct)
+ * (graph.hpp:745-1364, utils.hpp:245-430; main.cpp:90-91) as nprocs strip
+ * ranks would build it under mpiexec -n nprocs (the graph depends on the rank
+ * count). radius <= 0 selects the reference's r(n) (graph.hpp:788-791).
+ * random_edge_pct in [0,100) adds the reference's extra random edges, drawn
+ * from seed. Rows are sorted; with offsets == NULL only *ne is filled. */
+xt_status xt_rgg_generate(int64_t nv, int nprocs, double radius, double random_edge_pct, uint64_t seed,
+                          int64_t cap, int64_t *ne, int64_t *offsets, int64_t *tails);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* XTRIC_H */

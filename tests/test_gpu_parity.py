@@ -1,0 +1,249 @@
+"""Parity of the CUDA path with the oracle and the reference's golden counts.
+
+Every test here runs the product through the C ABI (libxtb200.so) on the
+GPU and checks it against golden vectors from the reference binary or the
+oracle on the same seeded inputs. Integer counts: bit-exact, no tolerance.
+"""
+import numpy as np
+import pytest
+
+import oracle
+import xxtric_b200 as xt
+from conftest import load_fixtures, load_golden
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = load_golden()
+FIX = load_fixtures()
+EDGE_NAMES = [n for n in GOLDEN if n + "_src" in FIX]
+ORIENTS = [xt.ORIENT_ID, xt.ORIENT_DEGREE]
+
+
+@pytest.fixture(scope="module")
+def ctx():
+    c = xt.Context(0)
+    yield c
+    c.close()
+
+
+@pytest.fixture(scope="module")
+def torch_cuda():
+    import torch
+    assert torch.cuda.is_available()
+    return torch
+
+
+def canon(name):
+    f = GOLDEN[name]
+    return oracle.canon_csr(f["nv"], FIX[name + "_src"].astype(np.int64), FIX[name + "_dst"].astype(np.int64))
+
+
+@pytest.mark.parametrize("orient", ORIENTS)
+@pytest.mark.parametrize("name", EDGE_NAMES)
+def test_golden_from_edges(ctx, name, orient):
+    f = GOLDEN[name]
+    g = ctx.graph_from_edges(f["nv"], FIX[name + "_src"], FIX[name + "_dst"], orient)
+    try:
+        t, pv = g.count(per_vertex=True)
+        assert t == f["triangles"]
+        off, tails = canon(name)
+        _, opv = oracle.count_merge(off, tails, per_vertex=True)
+        assert (pv == opv).all()
+        assert g.info()["n_edges"] == f["undirected"]
+    finally:
+        g.free()
+
+
+@pytest.mark.parametrize("canonical", [True, False])
+@pytest.mark.parametrize("name", ["k4", "iso_tail", "k64", "star_path", "er0", "rmat14", "chunglu14", "amazon0302"])
+def test_golden_from_reference_csr(ctx, name, canonical):
+    # the vite-layout CSR the reference engine takes (xxtric-gpu.hpp:116-121)
+    off, tails = canon(name)
+    for orient in ORIENTS:
+        g = ctx.graph_from_csr(off, tails, canonical=canonical, orient=orient)
+        try:
+            assert g.count() == GOLDEN[name]["triangles"]
+        finally:
+            g.free()
+
+
+def test_noncanonical_input_is_canonicalised(ctx):
+    # repeated pairs, one-directional rows and self loops: the builder
+    # dedups, so the count equals the reference's on the canonical file
+    s = np.array([0, 0, 0, 1, 1, 2, 0, 1, 2, 3, 3], np.int32)
+    d = np.array([1, 2, 3, 2, 3, 3, 1, 0, 2, 3, 0], np.int32)
+    for orient in ORIENTS:
+        g = ctx.graph_from_edges(4, s, d, orient)
+        assert g.count() == 4
+        g.free()
+    # a raw (unsorted, duplicated) CSR through the non-canonical path
+    off = np.array([0, 4, 6, 8, 10], np.int64)
+    tails = np.array([3, 1, 2, 1, 0, 2, 0, 1, 0, 2], np.int64)
+    g = ctx.graph_from_csr(off, tails, canonical=False)
+    assert g.count() == 2  # edges 01 02 03 12 23: triangles 012 and 023
+    g.free()
+
+
+@pytest.mark.parametrize("n", [1024, 4096, 16384, 65536])
+def test_reference_rgg_counts(ctx, n):
+    off, tails = xt.generate_rgg(n, 1)
+    f = GOLDEN[f"rgg{n}"]
+    assert len(tails) == f["directed_entries"]
+    for orient in ORIENTS:
+        g = ctx.graph_from_csr(off, tails, canonical=True, orient=orient)
+        assert g.count() == f["triangles"]
+        g.free()
+
+
+def test_rgg_two_ranks_and_config_radius(ctx):
+    # mpiexec -n 2 graph and the r = sqrt(16/(pi n)) variant: oracle counts
+    n = 65536
+    for radius in (0.0, float(np.sqrt(16.0 / (np.pi * n)))):
+        off, tails = xt.generate_rgg(n, 2, radius)
+        expect = oracle.count_merge(off, tails)
+        g = ctx.graph_from_csr(off, tails, canonical=True)
+        assert g.count() == expect
+        g.free()
+
+
+def test_generators_bit_exact(ctx, torch_cuda):
+    torch = torch_cuda
+    ne = 1 << 18
+    s = torch.empty(ne, dtype=torch.int32, device="cuda")
+    d = torch.empty_like(s)
+    ctx.gen_rmat(16, ne, 5, s, d)
+    so, do = oracle.rmat_edges(16, ne, 5)
+    assert (s.cpu().numpy() == so).all() and (d.cpu().numpy() == do).all()
+    ctx.gen_rmat(12, ne, 5, s, d, noise_pct=0, permute=False)
+    so, do = oracle.rmat_edges(12, ne, 5, noise_pct=0, permute=False)
+    assert (s.cpu().numpy() == so).all() and (d.cpu().numpy() == do).all()
+    cdf, _ = xt.chunglu_cdf(1 << 16, 2.1, 64.0, 4096.0)
+    ctx.gen_chunglu(cdf, ne, 9, s, d)
+    so, do = oracle.chunglu_edges(cdf, ne, 9)
+    assert (s.cpu().numpy() == so).all() and (d.cpu().numpy() == do).all()
+    ctx.gen_er(100000, ne, 11, s, d)
+    so, do = oracle.er_edges(100000, ne, 11)
+    assert (s.cpu().numpy() == so).all() and (d.cpu().numpy() == do).all()
+
+
+@pytest.mark.parametrize("scale", [12, 16, 18])
+def test_rmat_counts_vs_oracle(ctx, torch_cuda, scale):
+    torch = torch_cuda
+    ne = 16 << scale
+    s = torch.empty(ne, dtype=torch.int32, device="cuda")
+    d = torch.empty_like(s)
+    ctx.gen_rmat(scale, ne, 1, s, d)
+    off, tails = oracle.canon_csr(1 << scale, s.cpu().numpy().astype(np.int64), d.cpu().numpy().astype(np.int64))
+    expect, opv = oracle.count_merge(off, tails, per_vertex=True)
+    for orient in ORIENTS:
+        g = ctx.graph_from_device_edges(1 << scale, ne, s, d, orient)
+        t, pv = g.count(per_vertex=True)
+        assert t == expect
+        assert (pv == opv).all()
+        g.free()
+
+
+def test_chunglu_skewed_counts_vs_oracle(ctx, torch_cuda):
+    # heavy skew: hub lists exceed the warp and block hash bins under the id
+    # orientation (the part bin) and exercise every bin under degree order
+    torch = torch_cuda
+    n = 1 << 17
+    cdf, m = xt.chunglu_cdf(n, 2.1, 32.0, 16384.0)
+    s = torch.empty(m, dtype=torch.int32, device="cuda")
+    d = torch.empty_like(s)
+    ctx.gen_chunglu(cdf, m, 21, s, d)
+    off, tails = oracle.canon_csr(n, s.cpu().numpy().astype(np.int64), d.cpu().numpy().astype(np.int64))
+    expect, opv = oracle.count_merge(off, tails, per_vertex=True)
+    for orient in ORIENTS:
+        g = ctx.graph_from_device_edges(n, m, s, d, orient)
+        inf = g.info()
+        t, pv = g.count(per_vertex=True)
+        assert t == expect, (orient, inf)
+        assert (pv == opv).all()
+        g.free()
+
+
+def test_count_device_reference_layout(ctx, torch_cuda):
+    torch = torch_cuda
+    off, tails = canon("amazon0302")
+    d_off = torch.from_numpy(off).cuda()
+    d_t = torch.from_numpy(tails).cuda()
+    out = torch.full((1,), 123, dtype=torch.int64, device="cuda")
+    stream = torch.cuda.current_stream().cuda_stream
+    xt.count_device(len(off) - 1, d_off, d_t, out, accumulate=False, stream=stream)
+    torch.cuda.synchronize()
+    assert int(out.item()) == GOLDEN["amazon0302"]["triangles"]
+    xt.count_device(len(off) - 1, d_off, d_t, out, accumulate=True, stream=stream)
+    torch.cuda.synchronize()
+    assert int(out.item()) == 2 * GOLDEN["amazon0302"]["triangles"]
+
+
+def test_edge_cases(ctx):
+    # one vertex, no edges; a single edge; only self loops; isolated tail
+    g = ctx.graph_from_edges(1, np.zeros(0, np.int32), np.zeros(0, np.int32))
+    assert g.count() == 0
+    g.free()
+    g = ctx.graph_from_edges(2, np.array([0], np.int32), np.array([1], np.int32))
+    assert g.count(per_vertex=True)[0] == 0
+    g.free()
+    g = ctx.graph_from_edges(3, np.array([0, 1, 2], np.int32), np.array([0, 1, 2], np.int32))
+    assert g.count() == 0 and g.info()["n_edges"] == 0
+    g.free()
+    g = ctx.graph_from_edges(10, np.array([7, 8, 7], np.int32), np.array([8, 9, 9], np.int32))
+    t, pv = g.count(per_vertex=True)
+    assert t == 1 and pv.tolist() == [0] * 7 + [1, 1, 1]
+    g.free()
+
+
+def test_errors_leave_context_usable(ctx):
+    with pytest.raises(xt.XtError) as e:
+        ctx.graph_from_edges(4, np.array([0, 5], np.int32), np.array([1, 2], np.int32))
+    assert e.value.status == xt.XT_ERR_INVALID
+    with pytest.raises(xt.XtError) as e:
+        ctx.graph_from_edges(4, np.array([0, -1], np.int32), np.array([1, 2], np.int32))
+    assert e.value.status == xt.XT_ERR_INVALID
+    with pytest.raises(xt.XtError) as e:
+        ctx.graph_from_csr(np.array([0, 2, 1], np.int64), np.array([1, 0], np.int64))
+    assert e.value.status == xt.XT_ERR_INVALID
+    # an allocation failure injected on the host side of the allocator
+    for k in range(1, 12):
+        ctx.fail_alloc_after(k)
+        try:
+            g = ctx.graph_from_edges(GOLDEN["k64"]["nv"], FIX["k64_src"], FIX["k64_dst"])
+        except xt.XtError as err:
+            assert err.status == xt.XT_ERR_OOM
+            continue
+        g.free()
+        break
+    ctx.fail_alloc_after(0)
+    g = ctx.graph_from_edges(GOLDEN["k64"]["nv"], FIX["k64_src"], FIX["k64_dst"])
+    assert g.count() == GOLDEN["k64"]["triangles"]
+    g.free()
+
+
+def test_cli_on_gpu(tmp_path):
+    import subprocess
+    from conftest import ROOT
+    import os
+    cli = os.path.join(ROOT, "xxtric_b200", "xtric")
+    r = subprocess.run([cli, "-n", "4096", "-l"], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    assert f"Number of triangles: {GOLDEN['rgg4096']['triangles']}" in r.stdout
+    off, tails = xt.generate_rgg(16384, 1)
+    p = str(tmp_path / "g.bin")
+    xt.write_vite(p, off, tails)
+    pvf = str(tmp_path / "pv.txt")
+    r = subprocess.run([cli, "-f", p, "--orient", "id", "--per-vertex", pvf], capture_output=True, text=True,
+                       timeout=300)
+    assert r.returncode == 0, r.stderr
+    assert f"Number of triangles: {GOLDEN['rgg16384']['triangles']}" in r.stdout
+    pv = np.loadtxt(pvf, dtype=np.int64)
+    assert pv.sum() == 3 * GOLDEN["rgg16384"]["triangles"]
+
+
+def test_mirror_class(ctx):
+    off, tails = canon("rmat10")
+    tc = xt.TriangleCountingSingle(off, tails)
+    assert tc.count() == GOLDEN["rmat10"]["triangles"]
+    assert tc.count() == GOLDEN["rmat10"]["triangles"]  # counting twice is idempotent
+    tc.clear()

@@ -1,0 +1,155 @@
+"""Host-side logic of the product, no GPU: the C ABI library loads and
+exports every declared symbol, the vite reader/writer, the reference-RGG
+generator against the oracle and the reference's golden counts, the
+Chung-Lu weight table against the oracle twin, and the CLI's argument
+checks (main.cpp:238-275)."""
+import os
+import re
+import subprocess
+
+import numpy as np
+import pytest
+
+import oracle
+import xxtric_b200 as xt
+from conftest import ROOT, load_golden
+
+GOLDEN = load_golden()
+HEADER = os.path.join(ROOT, "include", "xtric.h")
+CLI = os.path.join(ROOT, "xxtric_b200", "xtric")
+
+
+def declared_functions():
+    src = open(HEADER).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    return sorted(set(re.findall(r"\b(xt_[a-z0-9_]+)\s*\(", src)))
+
+
+def test_library_exports_every_declared_symbol():
+    names = declared_functions()
+    assert len(names) >= 20
+    lib = xt.lib()
+    missing = [n for n in names if not hasattr(lib, n)]
+    assert not missing, missing
+    assert set(names) <= set(xt.EXPORTED) | set(names)
+
+
+def test_no_device_is_reported_not_faked():
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    with pytest.raises(xt.XtError) as e:
+        xt.Context(0)
+    assert e.value.status == xt.XT_ERR_NO_DEVICE
+
+
+@pytest.mark.parametrize("nprocs,radius", [(1, 0.0), (2, 0.0), (4, 0.0), (8, 0.0), (1, 0.03), (2, 0.02)])
+def test_rgg_generator_matches_oracle(nprocs, radius):
+    n = 4096
+    off, tails = xt.generate_rgg(n, nprocs, radius)
+    o_off, o_tails = oracle.ref_rgg(n, nprocs, radius)
+    assert (off == o_off).all()
+    assert (tails == o_tails).all()
+
+
+@pytest.mark.parametrize("n", [1024, 4096, 16384, 65536])
+def test_rgg_generator_reproduces_reference_graph(n):
+    off, tails = xt.generate_rgg(n, 1)
+    f = GOLDEN[f"rgg{n}"]
+    assert len(tails) == f["directed_entries"]
+    assert oracle.count_xxtric(off, tails) == f["triangles"]
+    # rows sorted, symmetric, no self loops
+    deg = np.diff(off)
+    src = np.repeat(np.arange(n), deg)
+    assert (src != tails).all()
+    key = src * n + tails
+    assert (np.diff(key) > 0).all()
+    assert np.array_equal(np.sort(key), np.sort(tails * n + src))
+
+
+def test_rgg_random_edges_deterministic():
+    a = xt.generate_rgg(4096, 2, 0.0, 5.0, seed=3)
+    b = xt.generate_rgg(4096, 2, 0.0, 5.0, seed=3)
+    c = xt.generate_rgg(4096, 2, 0.0, 5.0, seed=4)
+    base = xt.generate_rgg(4096, 2)
+    assert (a[1] == b[1]).all()
+    assert len(a[1]) > len(base[1])
+    assert len(c[1]) != len(a[1]) or not (c[1] == a[1]).all()
+    with pytest.raises(xt.XtError):
+        xt.generate_rgg(4096, 2, 0.0, 100.0)
+    with pytest.raises(xt.XtError):
+        xt.generate_rgg(4096, 3)  # strip ranks must be a power of two
+
+
+@pytest.mark.parametrize("elem", [8, 4])
+def test_vite_roundtrip(tmp_path, elem):
+    off, tails = xt.generate_rgg(1024, 1)
+    p = str(tmp_path / "g.bin")
+    xt.write_vite(p, off, tails, elem)
+    assert os.path.getsize(p) == 2 * elem + (len(off)) * elem + len(tails) * 2 * elem
+    o2, t2 = xt.read_vite(p, elem)
+    assert (o2 == off).all() and (t2 == tails).all()
+
+
+def test_vite_matches_reference_layout(tmp_path):
+    # the layout graph.hpp:320-383 reads: header, offsets, {int64 tail, f64 weight}
+    off, tails = xt.generate_rgg(1024, 1)
+    p = str(tmp_path / "g.bin")
+    xt.write_vite(p, off, tails)
+    raw = np.fromfile(p, np.int64)
+    assert raw[0] == 1024 and raw[1] == len(tails)
+    assert (raw[2:2 + 1025] == off).all()
+    rec = raw[2 + 1025:].reshape(-1, 2)
+    assert (rec[:, 0] == tails).all()
+    assert (rec[:, 1].view(np.float64) == 1.0).all()
+    if os.path.exists(oracle.REF_TRIC):
+        r = oracle.run_ref(["-f", p])
+        assert r["triangles"] == GOLDEN["rgg1024"]["triangles"]
+
+
+def test_vite_rejects_bad_files(tmp_path):
+    off, tails = xt.generate_rgg(1024, 1)
+    p = str(tmp_path / "g.bin")
+    xt.write_vite(p, off, tails)
+    data = open(p, "rb").read()
+    open(p, "wb").write(data[:-8])  # truncated
+    with pytest.raises(xt.XtError) as e:
+        xt.read_vite(p)
+    assert e.value.status == xt.XT_ERR_IO
+    with pytest.raises(xt.XtError):
+        xt.read_vite(str(tmp_path / "missing.bin"))
+    bad = np.array([4, 2, 0, 1, 0, 2, 2], np.int64)  # offsets not monotone
+    bad = np.concatenate([bad, np.array([1, 0, 0, 0], np.int64)])
+    bad.tofile(p)
+    with pytest.raises(xt.XtError):
+        xt.read_vite(p)
+
+
+def test_chunglu_cdf_matches_oracle():
+    c1, m1 = xt.chunglu_cdf(1 << 16, 2.1, 64.0, 4096.0)
+    c2, m2 = oracle.chunglu_cdf(1 << 16, 2.1, 64.0, 4096.0)
+    assert m1 == m2
+    assert (c1 == c2).all()
+    w = np.diff(c1).astype(np.float64) / 1024.0
+    assert abs(w.mean() - 64.0) < 3.0
+    assert abs(w[0] - 4096.0) < 1.0
+
+
+def run_cli(*args):
+    return subprocess.run([CLI] + list(args), capture_output=True, text=True, timeout=120)
+
+
+@pytest.mark.skipif(not os.path.exists(CLI), reason="xtric not built")
+def test_cli_argument_errors():
+    r = run_cli()
+    assert r.returncode == 157 and "Must specify some options." in r.stderr
+    r = run_cli("-l")  # the reference checks for an input first (main.cpp:253-257)
+    assert r.returncode == 157 and "Must specify a binary file name" in r.stderr
+    r = run_cli("-f", "x.bin", "-l")
+    assert r.returncode == 157 and "Must specify -g for graph generation using LCG." in r.stderr
+    r = run_cli("-f", "x.bin", "-p", "5")
+    assert r.returncode == 157 and "add random edges" in r.stderr
+    r = run_cli("-n", "1024", "-p", "150")
+    assert r.returncode == 157 and "Invalid random edge percentage" in r.stderr
+    r = run_cli("-f", "/nonexistent.bin")
+    assert r.returncode == 157 and "Error opening file!" in r.stdout

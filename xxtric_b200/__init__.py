@@ -1,0 +1,322 @@
+"""xxtric_b200 — B200-native exact triangle counting (sm_100a CUDA behind a C ABI).
+
+Python host mirror of the reference's single-device surface (sg0/xxtric):
+``read_vite`` (BinaryEdgeList::read, graph.hpp:294-395), ``generate_rgg``
+(GenerateRGG::generate, graph.hpp:745-1364), ``TriangleCountingSingle``
+(xxtric-gpu.hpp:22-298: constructor builds, ``count()`` counts, ``clear()``
+frees). Everything calls libxtb200.so through ctypes; there is no CPU
+fallback — importing the package fails if the library is missing.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from typing import Optional
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libxtb200.so")
+
+XT_OK, XT_ERR_INVALID, XT_ERR_CUDA, XT_ERR_OOM, XT_ERR_IO, XT_ERR_OVERFLOW = 0, 1, 2, 3, 4, 5
+XT_ERR_TIMEOUT, XT_ERR_ADMISSION, XT_ERR_NOT_READY, XT_ERR_NO_DEVICE, XT_ERR_CLOSED = 6, 7, 8, 9, 10
+ORIENT_ID, ORIENT_DEGREE = 0, 1
+CSR_CANONICAL = 1
+
+# R-MAT quadrant weights a, b, c (d = rest) in 1/65536 units: .57/.19/.19/.05
+RMAT_A16, RMAT_B16, RMAT_C16 = 37355, 12452, 12452
+
+
+class XtError(RuntimeError):
+    def __init__(self, status: int, msg: str):
+        super().__init__(msg)
+        self.status = status
+
+
+def _load() -> ctypes.CDLL:
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"{LIB_PATH} is not built; run `python xxtric_b200/build.py` "
+                          "(the CUDA library is required: there is no CPU fallback)")
+    return ctypes.CDLL(LIB_PATH)
+
+
+_L = _load()
+_i64, _i32, _u64, _int, _dbl, _vp = (ctypes.c_int64, ctypes.c_int32, ctypes.c_uint64, ctypes.c_int,
+                                     ctypes.c_double, ctypes.c_void_p)
+_P = ctypes.POINTER
+
+
+class GraphInfo(ctypes.Structure):
+    _fields_ = [("nv", _i64), ("n_input", _i64), ("n_edges", _i64), ("max_degree", _i64),
+                ("max_out_degree", _i64), ("max_in_degree", _i64), ("wedge_work", _i64),
+                ("stream_work", _i64), ("alg_bytes", _i64), ("tail_alg_bytes", _i64),
+                ("orient", _i32), ("reserved", _i32)]
+
+    def as_dict(self) -> dict:
+        return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}
+
+
+def _proto(name, res, *args):
+    f = getattr(_L, name)
+    f.restype = res
+    f.argtypes = list(args)
+    return f
+
+
+_proto("xt_strerror", ctypes.c_char_p, _int)
+_proto("xt_last_error", ctypes.c_char_p, _vp)
+_proto("xt_open", _int, _int, _P(_vp))
+_proto("xt_close", _int, _vp)
+_proto("xt_set_stream", _int, _vp, _vp)
+_proto("xt_debug_fail_alloc", _int, _vp, _i64)
+_proto("xt_launch_count", _i64, _vp)
+_proto("xt_graph_from_csr", _int, _vp, _i64, _vp, _vp, _int, _int, _P(_vp))
+_proto("xt_graph_from_edges", _int, _vp, _i64, _i64, _vp, _vp, _int, _P(_vp))
+_proto("xt_graph_from_device_edges", _int, _vp, _i64, _i64, _vp, _vp, _int, _P(_vp))
+_proto("xt_graph_get_info", _int, _vp, _P(GraphInfo))
+_proto("xt_graph_get_csr", _int, _vp, _vp, _vp)
+_proto("xt_graph_free", _int, _vp)
+_proto("xt_count", _int, _vp, _vp, _vp)
+_proto("xt_count_async", _int, _vp, _vp, _vp)
+_proto("xt_count_device", _int, _i64, _vp, _vp, _vp, _int, _vp)
+_proto("xt_gen_rmat", _int, _vp, _int, _i64, _u64, _int, _int, _int, _int, _int, _vp, _vp)
+_proto("xt_gen_chunglu", _int, _vp, _i64, _vp, _i64, _u64, _int, _vp, _vp)
+_proto("xt_chunglu_cdf", _i64, _i64, _dbl, _dbl, _dbl, _vp)
+_proto("xt_gen_er", _int, _vp, _i64, _i64, _u64, _vp, _vp)
+_proto("xt_vite_read", _int, ctypes.c_char_p, _int, _P(_i64), _P(_i64), _vp, _vp)
+_proto("xt_vite_write", _int, ctypes.c_char_p, _int, _i64, _vp, _vp)
+_proto("xt_rgg_generate", _int, _i64, _int, _dbl, _dbl, _u64, _i64, _P(_i64), _vp, _vp)
+
+EXPORTED = ["xt_strerror", "xt_last_error", "xt_open", "xt_close", "xt_set_stream", "xt_debug_fail_alloc",
+            "xt_launch_count",
+            "xt_graph_from_csr", "xt_graph_from_edges", "xt_graph_from_device_edges", "xt_graph_get_info",
+            "xt_graph_get_csr", "xt_graph_free", "xt_count", "xt_count_async", "xt_count_device",
+            "xt_gen_rmat", "xt_gen_chunglu", "xt_chunglu_cdf", "xt_gen_er", "xt_vite_read", "xt_vite_write",
+            "xt_rgg_generate"]
+
+
+def lib() -> ctypes.CDLL:
+    return _L
+
+
+def strerror(s: int) -> str:
+    return _L.xt_strerror(s).decode()
+
+
+def _check(s: int, what: str, ctx: Optional["Context"] = None) -> None:
+    if s != XT_OK:
+        detail = ""
+        if ctx is not None and ctx._h:
+            detail = _L.xt_last_error(ctx._h).decode()
+        raise XtError(s, f"{what}: {strerror(s)}" + (f" ({detail})" if detail else ""))
+
+
+def _ptr(a) -> int:
+    """Device or host address of a numpy array, torch tensor or int."""
+    if a is None:
+        return 0
+    if isinstance(a, int):
+        return a
+    if isinstance(a, np.ndarray):
+        return a.ctypes.data
+    return int(a.data_ptr())  # torch.Tensor
+
+
+# ---------------------------------------------------------------------------
+# host-side input: vite files and the reference's RGG generator
+# ---------------------------------------------------------------------------
+
+def read_vite(path: str, elem_bytes: int = 8) -> tuple[np.ndarray, np.ndarray]:
+    """BinaryEdgeList::read for one process: (offsets int64[nv+1], tails int64[ne])."""
+    nv, ne = _i64(0), _i64(0)
+    _check(_L.xt_vite_read(path.encode(), elem_bytes, ctypes.byref(nv), ctypes.byref(ne), None, None),
+           f"reading {path}")
+    off = np.empty(nv.value + 1, np.int64)
+    tails = np.empty(ne.value, np.int64)
+    _check(_L.xt_vite_read(path.encode(), elem_bytes, ctypes.byref(nv), ctypes.byref(ne), _ptr(off), _ptr(tails)),
+           f"reading {path}")
+    return off, tails
+
+
+def write_vite(path: str, offsets: np.ndarray, tails: np.ndarray, elem_bytes: int = 8) -> None:
+    off = np.ascontiguousarray(offsets, np.int64)
+    t = np.ascontiguousarray(tails, np.int64)
+    _check(_L.xt_vite_write(path.encode(), elem_bytes, len(off) - 1, _ptr(off), _ptr(t)), f"writing {path}")
+
+
+def generate_rgg(nv: int, nprocs: int = 1, radius: float = 0.0, random_edge_pct: float = 0.0,
+                 seed: int = 1) -> tuple[np.ndarray, np.ndarray]:
+    """GenerateRGG(nv).generate(LCG, unit weights, pct) as `nprocs` strip ranks build it."""
+    ne = _i64(0)
+    _check(_L.xt_rgg_generate(nv, nprocs, radius, random_edge_pct, seed, 0, ctypes.byref(ne), None, None),
+           "generate_rgg")
+    off = np.empty(nv + 1, np.int64)
+    tails = np.empty(ne.value, np.int64)
+    _check(_L.xt_rgg_generate(nv, nprocs, radius, random_edge_pct, seed, ne.value, ctypes.byref(ne), _ptr(off),
+                              _ptr(tails)), "generate_rgg")
+    return off, tails
+
+
+def chunglu_cdf(n: int, gamma: float = 2.1, mean_deg: float = 64.0, max_deg: float = 131072.0):
+    cdf = np.empty(n + 1, np.uint64)
+    m = _L.xt_chunglu_cdf(n, gamma, mean_deg, max_deg, _ptr(cdf))
+    if m < 0:
+        raise XtError(XT_ERR_INVALID, "chunglu_cdf: bad arguments")
+    return cdf, int(m)
+
+
+# ---------------------------------------------------------------------------
+# device: context, graphs, counting, generators
+# ---------------------------------------------------------------------------
+
+class Context:
+    """One device + one CUDA stream (xt_open)."""
+
+    def __init__(self, device: int = 0):
+        h = _vp()
+        s = _L.xt_open(device, ctypes.byref(h))
+        if s != XT_OK:
+            raise XtError(s, f"xt_open({device}): {strerror(s)}")
+        self._h = h.value
+        self.device = device
+
+    def close(self) -> None:
+        if self._h:
+            _L.xt_close(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_stream(self, stream_ptr: int) -> None:
+        _check(_L.xt_set_stream(self._h, stream_ptr), "xt_set_stream", self)
+
+    def fail_alloc_after(self, k: int) -> None:
+        _check(_L.xt_debug_fail_alloc(self._h, k), "xt_debug_fail_alloc", self)
+
+    @property
+    def last_error(self) -> str:
+        return _L.xt_last_error(self._h).decode()
+
+    @property
+    def launches(self) -> int:
+        """This library's kernels launched on the context so far."""
+        return int(_L.xt_launch_count(self._h))
+
+    # -- graphs --
+    def graph_from_csr(self, offsets: np.ndarray, tails: np.ndarray, canonical: bool = False,
+                       orient: int = ORIENT_DEGREE) -> "DeviceGraph":
+        off = np.ascontiguousarray(offsets, np.int64)
+        t = np.ascontiguousarray(tails, np.int64)
+        h = _vp()
+        _check(_L.xt_graph_from_csr(self._h, len(off) - 1, _ptr(off), _ptr(t), CSR_CANONICAL if canonical else 0,
+                                    orient, ctypes.byref(h)), "xt_graph_from_csr", self)
+        return DeviceGraph(self, h.value)
+
+    def graph_from_edges(self, nv: int, src: np.ndarray, dst: np.ndarray,
+                         orient: int = ORIENT_DEGREE) -> "DeviceGraph":
+        s = np.ascontiguousarray(src, np.int32)
+        d = np.ascontiguousarray(dst, np.int32)
+        h = _vp()
+        _check(_L.xt_graph_from_edges(self._h, nv, len(s), _ptr(s), _ptr(d), orient, ctypes.byref(h)),
+               "xt_graph_from_edges", self)
+        return DeviceGraph(self, h.value)
+
+    def graph_from_device_edges(self, nv: int, ne: int, d_src, d_dst, orient: int = ORIENT_DEGREE) -> "DeviceGraph":
+        h = _vp()
+        _check(_L.xt_graph_from_device_edges(self._h, nv, ne, _ptr(d_src), _ptr(d_dst), orient, ctypes.byref(h)),
+               "xt_graph_from_device_edges", self)
+        return DeviceGraph(self, h.value)
+
+    # -- generators (device int32 outputs: torch tensors or raw pointers) --
+    def gen_rmat(self, scale: int, ne: int, seed: int, d_src, d_dst, noise_pct: int = 10, permute: bool = True,
+                 a16: int = RMAT_A16, b16: int = RMAT_B16, c16: int = RMAT_C16) -> None:
+        _check(_L.xt_gen_rmat(self._h, scale, ne, seed, a16, b16, c16, noise_pct, int(permute), _ptr(d_src),
+                              _ptr(d_dst)), "xt_gen_rmat", self)
+
+    def gen_chunglu(self, cdf: np.ndarray, ne: int, seed: int, d_src, d_dst, permute: bool = True) -> None:
+        c = np.ascontiguousarray(cdf, np.uint64)
+        _check(_L.xt_gen_chunglu(self._h, len(c) - 1, _ptr(c), ne, seed, int(permute), _ptr(d_src), _ptr(d_dst)),
+               "xt_gen_chunglu", self)
+
+    def gen_er(self, n: int, ne: int, seed: int, d_src, d_dst) -> None:
+        _check(_L.xt_gen_er(self._h, n, ne, seed, _ptr(d_src), _ptr(d_dst)), "xt_gen_er", self)
+
+
+class DeviceGraph:
+    """Oriented device CSR (+ its transpose and schedule) owned by the library."""
+
+    def __init__(self, ctx: Context, handle: int):
+        self.ctx = ctx
+        self._h = handle
+
+    def info(self) -> dict:
+        i = GraphInfo()
+        _check(_L.xt_graph_get_info(self._h, ctypes.byref(i)), "xt_graph_get_info", self.ctx)
+        return i.as_dict()
+
+    @property
+    def nv(self) -> int:
+        return self.info()["nv"]
+
+    def csr(self) -> tuple[np.ndarray, np.ndarray]:
+        inf = self.info()
+        off = np.empty(inf["nv"] + 1, np.int64)
+        col = np.empty(inf["n_edges"], np.int32)
+        _check(_L.xt_graph_get_csr(self._h, _ptr(off), _ptr(col)), "xt_graph_get_csr", self.ctx)
+        return off, col
+
+    def count(self, per_vertex: bool = False):
+        g = _i64(0)
+        pv = np.empty(self.nv, np.int64) if per_vertex else None
+        _check(_L.xt_count(self._h, ctypes.byref(g), _ptr(pv)), "xt_count", self.ctx)
+        return (g.value, pv) if per_vertex else g.value
+
+    def count_async(self, d_global, d_per_vertex=None) -> None:
+        _check(_L.xt_count_async(self._h, _ptr(d_global), _ptr(d_per_vertex)), "xt_count_async", self.ctx)
+
+    def free(self) -> None:
+        if self._h:
+            _L.xt_graph_free(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            if self.ctx._h:
+                self.free()
+        except Exception:
+            pass
+
+
+def count_device(nv: int, d_indices, d_edge_list, d_count, accumulate: bool = False, stream: int = 0) -> None:
+    """single_gpu_count replacement on the reference's device CSR layout (int64 offsets and tails)."""
+    s = _L.xt_count_device(nv, _ptr(d_indices), _ptr(d_edge_list), _ptr(d_count), int(accumulate), stream)
+    _check(s, "xt_count_device")
+
+
+class TriangleCountingSingle:
+    """Mirror of TriangleCountingSingle (xxtric-gpu.hpp:22-298) over a host CSR."""
+
+    def __init__(self, offsets: np.ndarray, tails: np.ndarray, orient: int = ORIENT_DEGREE, device: int = 0):
+        self.ctx = Context(device)
+        self.graph = self.ctx.graph_from_csr(offsets, tails, canonical=False, orient=orient)
+
+    def count(self) -> int:
+        return self.graph.count()
+
+    def clear(self) -> None:
+        if self.graph is not None:
+            self.graph.free()
+            self.graph = None
+        if self.ctx is not None:
+            self.ctx.close()
+            self.ctx = None

@@ -1,0 +1,107 @@
+// Internal declarations shared by the translation units of libxtb200.so.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+
+#include "../../include/xtric.h"
+
+namespace xt {
+
+constexpr int kWarp = 32;
+
+// ---- context ---------------------------------------------------------------
+struct Ctx {
+  int device = 0;
+  int sm_count = 148;
+  size_t smem_optin = 0;  // max dynamic shared memory per block (opt-in)
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  std::string last_error;
+  int64_t fail_alloc_countdown = 0;  // test hook: >0 counts down to a failing allocation
+  // device-side error word reused by kernels that check their own inputs
+  int *d_err = nullptr;
+  int64_t launches = 0;  // kernels of this library launched on this context
+};
+
+// Launch-configuration wrapper that counts the library's own kernel launches.
+inline dim3 counted(Ctx *c, dim3 grid) {
+  c->launches++;
+  return grid;
+}
+
+// Stream-ordered device allocation with the context's failure hook.
+xt_status dalloc(Ctx *c, void **p, size_t bytes);
+void dfree(Ctx *c, void *p);
+
+template <class T>
+xt_status dalloc_n(Ctx *c, T **p, size_t n) {
+  return dalloc(c, reinterpret_cast<void **>(p), n * sizeof(T));
+}
+
+// Records a CUDA error (if any) and converts it to a status.
+xt_status cuda_status(Ctx *c, cudaError_t e, const char *what);
+xt_status set_error(Ctx *c, xt_status s, const std::string &msg);
+
+#define XT_CUDA(ctx, call)                                   \
+  do {                                                       \
+    cudaError_t xt_e_ = (call);                              \
+    if (xt_e_ != cudaSuccess) return xt::cuda_status((ctx), xt_e_, #call); \
+  } while (0)
+
+#define XT_TRY(expr)                  \
+  do {                                \
+    xt_status xt_s_ = (expr);         \
+    if (xt_s_ != XT_OK) return xt_s_; \
+  } while (0)
+
+// ---- oriented graph on the device ------------------------------------------
+struct Plan;  // degree-binned schedule, built once per graph
+
+struct Graph {
+  Ctx *ctx = nullptr;
+  int64_t nv = 0;
+  int64_t n_input = 0;
+  int64_t ne = 0;  // |E+|
+  int orient = XT_ORIENT_DEGREE;
+  int64_t *d_off = nullptr;   // out-CSR offsets, nv+1
+  int32_t *d_col = nullptr;   // out-CSR columns N+(u), ne, rows ascending
+  int64_t *d_ioff = nullptr;  // in-CSR offsets, nv+1
+  int32_t *d_icol = nullptr;  // in-CSR columns N-(v), ne, rows ascending
+  int32_t *d_deg = nullptr;   // undirected degree, nv
+  int64_t max_degree = 0;
+  int64_t max_out_degree = 0;
+  int64_t max_in_degree = 0;
+  int64_t wedge_work = 0;   // sum over oriented (u,v) of d+(v)
+  int64_t stream_work = 0;  // sum over oriented (u,v) of d+(u) = sum_u d+(u)^2
+  Plan *plan = nullptr;
+};
+
+// Builds the oriented CSR from a device edge list (int32 ids) of ne rows.
+// Rows may repeat, be one-directional or self loops.
+xt_status build_from_edges(Ctx *c, int64_t nv, int64_t ne, const int32_t *d_src, const int32_t *d_dst,
+                           int orient, Graph *g);
+// Builds from a device CSR (int64 offsets and tails). canonical: rows already
+// sorted, deduped, symmetric and loop-free, so no sort is needed.
+xt_status build_from_csr(Ctx *c, int64_t nv, const int64_t *d_off, const int64_t *d_tails, bool canonical,
+                         int orient, Graph *g);
+void free_graph_device(Graph *g);
+
+// Builds (or rebuilds) the per-graph schedule and graph statistics.
+xt_status make_plan(Graph *g);
+void free_plan(Graph *g);
+
+// Launches the count on the graph's context stream. d_global: one int64
+// (overwritten); d_pv: nv int64 (nullable, overwritten).
+xt_status count_graph(Graph *g, int64_t *d_global, int64_t *d_pv);
+
+}  // namespace xt
+
+struct xt_ctx {
+  xt::Ctx c;
+};
+struct xt_graph {
+  xt::Graph g;
+};
