@@ -60,8 +60,10 @@ typedef struct {
   int64_t max_out_degree; /* max d+ after orientation */
   int64_t max_in_degree;  /* max d- after orientation */
   int64_t wedge_work;     /* sum over oriented (u,v) of d+(v): items a tail-grouped count streams */
-  int64_t stream_work;    /* sum over oriented (u,v) of d+(u) = sum_u d+(u)^2: items this count streams */
-  int64_t alg_bytes;      /* bytes this count must read: 16(nv+1) + 8|E+| + sum (16 + 4 d+(u)) */
+  int64_t stream_work;    /* sum over u of C(d+(u),2): candidate columns this count streams (the
+                             suffix of N+(u) after each out-neighbour) */
+  int64_t alg_bytes;      /* bytes this count reads at least once: 16(nv+1) offsets + 4|E+| member
+                             columns + 16|E+| in-records + 4 stream_work candidates */
   int64_t tail_alg_bytes; /* the tail-grouped figure: 8(nv+1) + 4|E+| + sum (16 + 4 d+(v)) */
   int32_t orient;         /* xt_orient used */
   int32_t reserved;
@@ -74,6 +76,9 @@ xt_status xt_open(int device, xt_ctx **out);
 xt_status xt_close(xt_ctx *ctx);
 /* use an existing cudaStream_t (passed as void*) instead of the context's own */
 xt_status xt_set_stream(xt_ctx *ctx, void *cuda_stream);
+/* wait for all work queued on the context's stream (the generators and
+ * xt_count_async return before their kernels finish) */
+xt_status xt_synchronize(xt_ctx *ctx);
 const char *xt_strerror(xt_status s);
 const char *xt_last_error(const xt_ctx *ctx);
 /* test hook: make the k-th device allocation from now fail (k<=0 disarms) */
@@ -97,8 +102,12 @@ xt_status xt_graph_from_edges(xt_ctx *ctx, int64_t nv, int64_t ne, const int32_t
 xt_status xt_graph_from_device_edges(xt_ctx *ctx, int64_t nv, int64_t ne, const int32_t *d_src,
                                      const int32_t *d_dst, int orient, xt_graph **out);
 xt_status xt_graph_get_info(const xt_graph *g, xt_graph_info *info);
-/* copy the oriented CSR out (host buffers of nv+1 and n_edges entries) */
+/* copy the oriented CSR out (host buffers of nv+1 and n_edges entries), in
+ * the library's internal numbering: vertices renumbered by orientation rank,
+ * so every row holds only higher ids, ascending */
 xt_status xt_graph_get_csr(const xt_graph *g, int64_t *offsets, int32_t *cols);
+/* internal id -> input id (host buffer of nv entries) */
+xt_status xt_graph_get_perm(const xt_graph *g, int32_t *new_to_old);
 /* Replaces TriangleCountingSingle::clear() (xxtric-gpu.hpp:272-285). */
 xt_status xt_graph_free(xt_graph *g);
 

@@ -70,6 +70,8 @@ _proto("xt_close", _int, _vp)
 _proto("xt_set_stream", _int, _vp, _vp)
 _proto("xt_debug_fail_alloc", _int, _vp, _i64)
 _proto("xt_launch_count", _i64, _vp)
+_proto("xt_synchronize", _int, _vp)
+_proto("xt_graph_get_perm", _int, _vp, _vp)
 _proto("xt_graph_from_csr", _int, _vp, _i64, _vp, _vp, _int, _int, _P(_vp))
 _proto("xt_graph_from_edges", _int, _vp, _i64, _i64, _vp, _vp, _int, _P(_vp))
 _proto("xt_graph_from_device_edges", _int, _vp, _i64, _i64, _vp, _vp, _int, _P(_vp))
@@ -88,7 +90,7 @@ _proto("xt_vite_write", _int, ctypes.c_char_p, _int, _i64, _vp, _vp)
 _proto("xt_rgg_generate", _int, _i64, _int, _dbl, _dbl, _u64, _i64, _P(_i64), _vp, _vp)
 
 EXPORTED = ["xt_strerror", "xt_last_error", "xt_open", "xt_close", "xt_set_stream", "xt_debug_fail_alloc",
-            "xt_launch_count",
+            "xt_launch_count", "xt_synchronize", "xt_graph_get_perm",
             "xt_graph_from_csr", "xt_graph_from_edges", "xt_graph_from_device_edges", "xt_graph_get_info",
             "xt_graph_get_csr", "xt_graph_free", "xt_count", "xt_count_async", "xt_count_device",
             "xt_gen_rmat", "xt_gen_chunglu", "xt_chunglu_cdf", "xt_gen_er", "xt_vite_read", "xt_vite_write",
@@ -237,19 +239,31 @@ class Context:
                "xt_graph_from_device_edges", self)
         return DeviceGraph(self, h.value)
 
-    # -- generators (device int32 outputs: torch tensors or raw pointers) --
+    def synchronize(self) -> None:
+        _check(_L.xt_synchronize(self._h), "xt_synchronize", self)
+
+    # -- generators (device int32 outputs: torch tensors or raw pointers). They
+    # run on the context stream; sync=True waits for them, so the outputs can
+    # be read from any other stream right away.
     def gen_rmat(self, scale: int, ne: int, seed: int, d_src, d_dst, noise_pct: int = 10, permute: bool = True,
-                 a16: int = RMAT_A16, b16: int = RMAT_B16, c16: int = RMAT_C16) -> None:
+                 a16: int = RMAT_A16, b16: int = RMAT_B16, c16: int = RMAT_C16, sync: bool = True) -> None:
         _check(_L.xt_gen_rmat(self._h, scale, ne, seed, a16, b16, c16, noise_pct, int(permute), _ptr(d_src),
                               _ptr(d_dst)), "xt_gen_rmat", self)
+        if sync:
+            self.synchronize()
 
-    def gen_chunglu(self, cdf: np.ndarray, ne: int, seed: int, d_src, d_dst, permute: bool = True) -> None:
+    def gen_chunglu(self, cdf: np.ndarray, ne: int, seed: int, d_src, d_dst, permute: bool = True,
+                    sync: bool = True) -> None:
         c = np.ascontiguousarray(cdf, np.uint64)
         _check(_L.xt_gen_chunglu(self._h, len(c) - 1, _ptr(c), ne, seed, int(permute), _ptr(d_src), _ptr(d_dst)),
                "xt_gen_chunglu", self)
+        if sync:
+            self.synchronize()
 
-    def gen_er(self, n: int, ne: int, seed: int, d_src, d_dst) -> None:
+    def gen_er(self, n: int, ne: int, seed: int, d_src, d_dst, sync: bool = True) -> None:
         _check(_L.xt_gen_er(self._h, n, ne, seed, _ptr(d_src), _ptr(d_dst)), "xt_gen_er", self)
+        if sync:
+            self.synchronize()
 
 
 class DeviceGraph:
@@ -268,7 +282,14 @@ class DeviceGraph:
     def nv(self) -> int:
         return self.info()["nv"]
 
+    def perm(self) -> np.ndarray:
+        """internal id -> input id."""
+        p = np.empty(self.nv, np.int32)
+        _check(_L.xt_graph_get_perm(self._h, _ptr(p)), "xt_graph_get_perm", self.ctx)
+        return p
+
     def csr(self) -> tuple[np.ndarray, np.ndarray]:
+        """The oriented CSR in internal numbering (see perm())."""
         inf = self.info()
         off = np.empty(inf["nv"] + 1, np.int64)
         col = np.empty(inf["n_edges"], np.int32)

@@ -1,22 +1,27 @@
-// GPU CSR builder: canonicalise (drop self loops, symmetrise, dedup), orient
-// each undirected edge from the lower to the higher rank, and emit the
-// oriented out-CSR (int64 offsets, int32 ascending columns) together with
-// its transpose (the in-lists N-(v)) that the head-grouped count streams.
+// GPU CSR builder: canonicalise (drop self loops, symmetrise, dedup), rank
+// the vertices, orient each undirected edge from the lower to the higher rank
+// and emit
+//   * the oriented out-CSR in rank numbering (int64 offsets, int32 ascending
+//     columns), and
+//   * per head v, one in-record per edge u->v holding the suffix of N+(u)
+//     after v (the candidates w with rank(w) > rank(v)).
 //
 // Reference behaviour replaced: the reference trusts its input CSR
 // (graph.hpp:294-395 reads it verbatim; a duplicated pair over-counts) and
-// orients implicitly by vertex id inside the count loop (xxtric.hpp:165,
-// counting.cu:619). Here the builder makes any edge list canonical first, so
-// the count of a canonical input equals the reference's count on it.
+// orients implicitly by vertex id inside the count loop (xxtric.hpp:165-185:
+// v = adj(i)[m] > i, then w = adj(i)[n] for n > m). Here the builder makes any
+// edge list canonical first, so the count of a canonical input equals the
+// reference's count on it; the in-record suffix is exactly the reference's
+// n > m range, taken from the head's side.
 #include <cub/cub.cuh>
 
 #include "xt_internal.cuh"
 
 namespace xt {
 
-static int bits_for(int64_t nv) {
+static int bits_for(int64_t n) {
   int b = 1;
-  while ((int64_t(1) << b) < nv) b++;
+  while ((int64_t(1) << b) < n) b++;
   return b;
 }
 
@@ -28,10 +33,13 @@ static unsigned grid_for(int64_t n, int block, int sm_count) {
   return (unsigned)g;
 }
 
+#define XT_GRID_STRIDE(i, n) \
+  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < (n); i += int64_t(gridDim.x) * blockDim.x)
+
 // key = (min << b) | max; self loops keep min == max and are dropped later.
 __global__ void k_edge_keys(const int32_t *__restrict__ src, const int32_t *__restrict__ dst, int64_t ne,
                             int64_t nv, int b, uint64_t *__restrict__ keys, int *__restrict__ err) {
-  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < ne; i += int64_t(gridDim.x) * blockDim.x) {
+  XT_GRID_STRIDE(i, ne) {
     int64_t s = src[i], d = dst[i];
     if (s < 0 || d < 0 || s >= nv || d >= nv) {
       atomicOr(err, 1);
@@ -45,7 +53,7 @@ __global__ void k_edge_keys(const int32_t *__restrict__ src, const int32_t *__re
 
 __global__ void k_unique_flags(const uint64_t *__restrict__ keys, int64_t n, int b, uint8_t *__restrict__ flags) {
   const uint64_t mask = (uint64_t(1) << b) - 1;
-  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x) {
+  XT_GRID_STRIDE(i, n) {
     uint64_t k = keys[i];
     bool first = (i == 0) || (keys[i - 1] != k);
     flags[i] = (first && ((k >> b) != (k & mask))) ? 1 : 0;
@@ -54,61 +62,66 @@ __global__ void k_unique_flags(const uint64_t *__restrict__ keys, int64_t n, int
 
 __global__ void k_degrees(const uint64_t *__restrict__ uniq, int64_t m, int b, int32_t *__restrict__ deg) {
   const uint64_t mask = (uint64_t(1) << b) - 1;
-  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < m; i += int64_t(gridDim.x) * blockDim.x) {
+  XT_GRID_STRIDE(i, m) {
     uint64_t k = uniq[i];
     atomicAdd(&deg[k >> b], 1);
     atomicAdd(&deg[k & mask], 1);
   }
 }
 
-__device__ __forceinline__ bool rank_less(int64_t a, int64_t b_, const int32_t *__restrict__ deg) {
-  int32_t da = deg[a], db = deg[b_];
-  return da < db || (da == db && a < b_);
+// (degree, id) sort keys of every vertex
+__global__ void k_rank_keys(const int32_t *__restrict__ deg, int64_t nv, uint64_t *__restrict__ vk) {
+  XT_GRID_STRIDE(x, nv) vk[x] = (uint64_t(uint32_t(deg[x])) << 32) | uint64_t(x);
 }
 
-// (lo,hi) -> (src,dst) by (degree, id) rank
-__global__ void k_orient_degree(uint64_t *__restrict__ keys, int64_t m, int b, const int32_t *__restrict__ deg) {
-  const uint64_t mask = (uint64_t(1) << b) - 1;
-  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < m; i += int64_t(gridDim.x) * blockDim.x) {
-    uint64_t k = keys[i];
-    int64_t lo = int64_t(k >> b), hi = int64_t(k & mask);
-    if (!rank_less(lo, hi, deg)) keys[i] = (uint64_t(hi) << b) | uint64_t(lo);
+// sorted (degree, id) keys -> internal->input and input->internal maps
+__global__ void k_rank_perm(const uint64_t *__restrict__ vk, int64_t nv, int32_t *__restrict__ n2o,
+                            int32_t *__restrict__ o2n) {
+  XT_GRID_STRIDE(r, nv) {
+    const int32_t old = int32_t(vk[r] & 0xffffffffu);
+    n2o[r] = old;
+    o2n[old] = int32_t(r);
   }
 }
 
-// (src,dst) -> (dst,src)
-__global__ void k_swap_keys(const uint64_t *__restrict__ in, int64_t m, int b, uint64_t *__restrict__ out) {
+// unique (lo,hi) in input ids -> (src<<b|dst) in internal ids, src < dst
+__global__ void k_relabel_edges(uint64_t *__restrict__ keys, int64_t m, int b, const int32_t *__restrict__ o2n) {
   const uint64_t mask = (uint64_t(1) << b) - 1;
-  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < m; i += int64_t(gridDim.x) * blockDim.x) {
-    uint64_t k = in[i];
-    out[i] = ((k & mask) << b) | (k >> b);
+  XT_GRID_STRIDE(i, m) {
+    const uint64_t k = keys[i];
+    const uint64_t a = uint64_t(o2n[k >> b]), c = uint64_t(o2n[k & mask]);
+    keys[i] = a < c ? ((a << b) | c) : ((c << b) | a);
   }
 }
 
-// Sorted keys (row << b | col) -> CSR. off[u] = index of the first key whose
-// row is >= u: thread i writes the rows in (row[i-1], row[i]] so every entry
-// of off is written exactly once, deterministically.
-__global__ void k_finish_csr(const uint64_t *__restrict__ keys, int64_t m, int64_t nv, int b,
-                             int64_t *__restrict__ off, int32_t *__restrict__ col) {
+// Sorted keys (row << b | col) -> row lengths and columns. The thread at a
+// run's first key adds -start, the one at its last key adds end, so each
+// non-empty row ends with end - start (len must start zeroed). The offsets
+// are then the exclusive scan of the lengths.
+__global__ void k_csr_runs(const uint64_t *__restrict__ keys, int64_t m, int b, int64_t *__restrict__ len,
+                           int32_t *__restrict__ col) {
   const uint64_t mask = (uint64_t(1) << b) - 1;
-  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i <= m; i += int64_t(gridDim.x) * blockDim.x) {
-    int64_t prev = (i == 0) ? -1 : int64_t(keys[i - 1] >> b);
-    int64_t cur = (i == m) ? nv : int64_t(keys[i] >> b);
-    for (int64_t u = prev + 1; u <= cur; u++) off[u] = i;
-    if (i < m) col[i] = int32_t(keys[i] & mask);
+  XT_GRID_STRIDE(i, m) {
+    const uint64_t k = keys[i];
+    const uint64_t row = k >> b;
+    if (i == 0 || (keys[i - 1] >> b) != row)
+      atomicAdd(reinterpret_cast<unsigned long long *>(&len[row]), (unsigned long long)(-i));
+    if (i + 1 == m || (keys[i + 1] >> b) != row)
+      atomicAdd(reinterpret_cast<unsigned long long *>(&len[row]), (unsigned long long)(i + 1));
+    if (col) col[i] = int32_t(k & mask);
   }
 }
 
-// CSR input: row index of every entry (warp per row) and range checks.
-__global__ void k_csr_rows(const int64_t *__restrict__ off, int64_t nv, int64_t ne_in, int32_t *__restrict__ rows,
+// row index of every CSR entry (warp per row); optional range checks
+__global__ void k_csr_rows(const int64_t *__restrict__ off, int64_t nv, int64_t ne, int32_t *__restrict__ rows,
                            int *__restrict__ err) {
   const int lane = threadIdx.x & 31;
   const int64_t warp = (blockIdx.x * int64_t(blockDim.x) + threadIdx.x) >> 5;
   const int64_t nwarps = (int64_t(gridDim.x) * blockDim.x) >> 5;
   for (int64_t u = warp; u < nv; u += nwarps) {
     int64_t e0 = off[u], e1 = off[u + 1];
-    if (e0 < 0 || e1 < e0 || e1 > ne_in) {
-      if (lane == 0) atomicOr(err, 2);
+    if (e0 < 0 || e1 < e0 || e1 > ne) {
+      if (lane == 0 && err) atomicOr(err, 2);
       continue;
     }
     for (int64_t e = e0 + lane; e < e1; e += 32) rows[e] = int32_t(u);
@@ -117,7 +130,7 @@ __global__ void k_csr_rows(const int64_t *__restrict__ off, int64_t nv, int64_t 
 
 __global__ void k_csr_tails32(const int64_t *__restrict__ tails, int64_t n, int64_t nv, int32_t *__restrict__ out,
                               int *__restrict__ err) {
-  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x) {
+  XT_GRID_STRIDE(i, n) {
     int64_t t = tails[i];
     if (t < 0 || t >= nv) {
       atomicOr(err, 1);
@@ -127,28 +140,39 @@ __global__ void k_csr_tails32(const int64_t *__restrict__ tails, int64_t n, int6
   }
 }
 
-// Canonical CSR input: keep entry (u,t) when u ranks below t; the kept
-// entries stay in (row, column) order, so no sort is needed.
-__global__ void k_csr_orient_keys(const int32_t *__restrict__ rows, const int32_t *__restrict__ tails, int64_t n,
-                                  const int64_t *__restrict__ off, int orient, int b, uint64_t *__restrict__ keys,
-                                  uint8_t *__restrict__ flags) {
-  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x) {
-    int64_t u = rows[i], t = tails[i];
-    bool keep;
-    if (orient == XT_ORIENT_ID) {
-      keep = u < t;
-    } else {
-      int64_t du = off[u + 1] - off[u], dt = off[t + 1] - off[t];
-      keep = du < dt || (du == dt && u < t);
-    }
-    flags[i] = keep ? 1 : 0;
+// canonical CSR input: each undirected edge once, as the entry (u,t), u < t;
+// the kept entries stay in (row, column) order
+__global__ void k_csr_lower_keys(const int32_t *__restrict__ rows, const int32_t *__restrict__ tails, int64_t n,
+                                 int b, uint64_t *__restrict__ keys, uint8_t *__restrict__ flags) {
+  XT_GRID_STRIDE(i, n) {
+    const int64_t u = rows[i], t = tails[i];
+    flags[i] = u < t ? 1 : 0;
     keys[i] = (uint64_t(u) << b) | uint64_t(t);
   }
 }
 
 __global__ void k_degree_from_off(const int64_t *__restrict__ off, int64_t nv, int32_t *__restrict__ deg) {
-  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < nv; i += int64_t(gridDim.x) * blockDim.x)
-    deg[i] = int32_t(off[i + 1] - off[i]);
+  XT_GRID_STRIDE(i, nv) deg[i] = int32_t(off[i + 1] - off[i]);
+}
+
+// (head << pb | position) for every out-CSR position
+__global__ void k_in_keys(const int32_t *__restrict__ col, int64_t m, int pb, uint64_t *__restrict__ ik) {
+  XT_GRID_STRIDE(p, m) ik[p] = (uint64_t(uint32_t(col[p])) << pb) | uint64_t(p);
+}
+
+// sorted in-keys -> in-records (suffix of N+(u) after the head)
+__global__ void k_in_records(const uint64_t *__restrict__ ik, int64_t m, int pb, const int32_t *__restrict__ rowof,
+                             const int64_t *__restrict__ off, InRec *__restrict__ rec) {
+  const uint64_t pmask = (uint64_t(1) << pb) - 1;
+  XT_GRID_STRIDE(i, m) {
+    const int64_t p = int64_t(ik[i] & pmask);
+    const int32_t u = rowof[p];
+    InRec r;
+    r.s = p + 1;
+    r.len = int32_t(off[u + 1] - p - 1);
+    r.u = u;
+    rec[i] = r;
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -189,6 +213,28 @@ static xt_status select_flagged(Ctx *c, const uint64_t *in, const uint8_t *flags
   return XT_OK;
 }
 
+// sorted (row << b | col) keys -> off[nv+1] (and col[m] when col != null)
+static xt_status keys_to_csr(Ctx *c, const uint64_t *keys, int64_t m, int64_t nv, int b, int64_t *off,
+                             int32_t *col) {
+  int64_t *len = nullptr;
+  XT_TRY(dalloc_n(c, &len, size_t(nv + 1)));
+  cudaError_t e = cudaMemsetAsync(len, 0, sizeof(int64_t) * (nv + 1), c->stream);
+  if (e == cudaSuccess && m > 0) {
+    k_csr_runs<<<counted(c, grid_for(m, 256, c->sm_count)), 256, 0, c->stream>>>(keys, m, b, len, col);
+    e = cudaGetLastError();
+  }
+  size_t bytes = 0;
+  void *tmp = nullptr;
+  if (e == cudaSuccess) e = cub::DeviceScan::ExclusiveSum(nullptr, bytes, len, off, nv + 1, c->stream);
+  xt_status s = cuda_status(c, e, "csr offsets");
+  if (s == XT_OK) s = dalloc(c, &tmp, bytes);
+  if (s == XT_OK)
+    s = cuda_status(c, cub::DeviceScan::ExclusiveSum(tmp, bytes, len, off, nv + 1, c->stream), "csr offsets");
+  dfree(c, tmp);
+  dfree(c, len);
+  return s;
+}
+
 static xt_status check_err(Ctx *c, const char *what) {
   int h = 0;
   XT_CUDA(c, cudaMemcpyAsync(&h, c->d_err, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
@@ -201,36 +247,72 @@ static xt_status check_err(Ctx *c, const char *what) {
   return XT_OK;
 }
 
-// Sorted oriented keys (src<<b|dst, m of them) -> out-CSR and in-CSR.
-static xt_status finish_graph(Ctx *c, uint64_t *okeys, int64_t m, int64_t nv, int b, Graph *g) {
+// uniq: m unique undirected edges (lo << b | hi) in input ids, sorted;
+// scratch: m more keys; deg: undirected degree in input ids (taken over by g).
+static xt_status orient_and_finish(Ctx *c, uint64_t *uniq, uint64_t *scratch, int64_t m, int64_t nv, int b,
+                                   int32_t *deg, int orient, Graph *g) {
   const int B = 256;
   g->ne = m;
+  g->d_deg = deg;
+  uint64_t *okeys = uniq;
+  if (orient == XT_ORIENT_DEGREE) {
+    uint64_t *vk = nullptr, *vk2 = nullptr;
+    int32_t *o2n = nullptr;
+    XT_TRY(dalloc_n(c, &vk, size_t(nv)));
+    xt_status s = dalloc_n(c, &vk2, size_t(nv));
+    if (s == XT_OK) s = dalloc_n(c, &o2n, size_t(nv));
+    if (s == XT_OK) s = dalloc_n(c, &g->d_perm, size_t(nv));
+    if (s == XT_OK) {
+      k_rank_keys<<<counted(c, grid_for(nv, B, c->sm_count)), B, 0, c->stream>>>(deg, nv, vk);
+      s = sort_keys(c, vk, vk2, nv, 32 + b);
+    }
+    if (s == XT_OK) {
+      k_rank_perm<<<counted(c, grid_for(nv, B, c->sm_count)), B, 0, c->stream>>>(vk2, nv, g->d_perm, o2n);
+      if (m > 0) k_relabel_edges<<<counted(c, grid_for(m, B, c->sm_count)), B, 0, c->stream>>>(uniq, m, b, o2n);
+      s = cuda_status(c, cudaGetLastError(), "relabel");
+    }
+    if (s == XT_OK && m > 0) {
+      s = sort_keys(c, uniq, scratch, m, 2 * b);
+      okeys = scratch;
+    }
+    dfree(c, vk);
+    dfree(c, vk2);
+    dfree(c, o2n);
+    if (s != XT_OK) return s;
+  }
+  // out-CSR. Columns are read as aligned 16-byte groups: pad so the last
+  // group of the last row stays inside the allocation.
   XT_TRY(dalloc_n(c, &g->d_off, size_t(nv + 1)));
-  XT_TRY(dalloc_n(c, &g->d_col, size_t(m > 0 ? m : 1)));
-  k_finish_csr<<<counted(c, grid_for(m + 1, B, c->sm_count)), B, 0, c->stream>>>(okeys, m, nv, b, g->d_off, g->d_col);
-  XT_CUDA(c, cudaGetLastError());
-  // transpose: sort (dst<<b|src)
-  uint64_t *t0 = nullptr, *t1 = nullptr;
-  XT_TRY(dalloc_n(c, &t0, size_t(m > 0 ? m : 1)));
-  xt_status s = dalloc_n(c, &t1, size_t(m > 0 ? m : 1));
-  if (s != XT_OK) {
-    dfree(c, t0);
-    return s;
+  XT_TRY(dalloc_n(c, &g->d_col, size_t(m) + kColPad));
+  XT_CUDA(c, cudaMemsetAsync(g->d_col + m, 0xff, sizeof(int32_t) * kColPad, c->stream));
+  XT_TRY(keys_to_csr(c, okeys, m, nv, b, g->d_off, g->d_col));
+  // in-records grouped by head, in increasing out-position
+  XT_TRY(dalloc_n(c, &g->d_ioff, size_t(nv + 1)));
+  XT_TRY(dalloc_n(c, &g->d_irec, size_t(m > 0 ? m : 1)));
+  if (m == 0) {
+    XT_CUDA(c, cudaMemsetAsync(g->d_ioff, 0, sizeof(int64_t) * (nv + 1), c->stream));
+    return XT_OK;
   }
-  k_swap_keys<<<counted(c, grid_for(m, B, c->sm_count)), B, 0, c->stream>>>(okeys, m, b, t0);
-  s = (m > 0) ? sort_keys(c, t0, t1, m, 2 * b) : XT_OK;
-  dfree(c, t0);
-  if (s != XT_OK) {
-    dfree(c, t1);
-    return s;
-  }
-  s = dalloc_n(c, &g->d_ioff, size_t(nv + 1));
-  if (s == XT_OK) s = dalloc_n(c, &g->d_icol, size_t(m > 0 ? m : 1));
+  const int pb = bits_for(m);
+  uint64_t *ik = (okeys == scratch) ? uniq : scratch;  // the buffer no longer needed
+  uint64_t *ik2 = nullptr;
+  int32_t *rowof = nullptr;
+  xt_status s = dalloc_n(c, &ik2, size_t(m));
+  if (s == XT_OK) s = dalloc_n(c, &rowof, size_t(m));
   if (s == XT_OK) {
-    k_finish_csr<<<counted(c, grid_for(m + 1, B, c->sm_count)), B, 0, c->stream>>>(t1, m, nv, b, g->d_ioff, g->d_icol);
-    s = cuda_status(c, cudaGetLastError(), "k_finish_csr");
+    k_csr_rows<<<counted(c, grid_for(nv * 32, B, c->sm_count)), B, 0, c->stream>>>(g->d_off, nv, m, rowof, nullptr);
+    k_in_keys<<<counted(c, grid_for(m, B, c->sm_count)), B, 0, c->stream>>>(g->d_col, m, pb, ik);
+    s = cuda_status(c, cudaGetLastError(), "in-keys");
   }
-  dfree(c, t1);
+  if (s == XT_OK) s = sort_keys(c, ik, ik2, m, b + pb);
+  if (s == XT_OK) s = keys_to_csr(c, ik2, m, nv, pb, g->d_ioff, nullptr);
+  if (s == XT_OK) {
+    k_in_records<<<counted(c, grid_for(m, B, c->sm_count)), B, 0, c->stream>>>(ik2, m, pb, rowof, g->d_off,
+                                                                               g->d_irec);
+    s = cuda_status(c, cudaGetLastError(), "in-records");
+  }
+  dfree(c, ik2);
+  dfree(c, rowof);
   return s;
 }
 
@@ -254,28 +336,26 @@ xt_status build_from_edges(Ctx *c, int64_t nv, int64_t ne, const int32_t *d_src,
   do {
     if ((s = dalloc_n(c, &k0, n1)) != XT_OK) break;
     if ((s = dalloc_n(c, &k1, n1)) != XT_OK) break;
-    if ((s = dalloc_n(c, &flags, n1)) != XT_OK) break;
     if (ne > 0) {
-      k_edge_keys<<<counted(c, grid_for(ne, B, c->sm_count)), B, 0, c->stream>>>(d_src, d_dst, ne, nv, b, k0, c->d_err);
+      if ((s = dalloc_n(c, &flags, n1)) != XT_OK) break;
+      k_edge_keys<<<counted(c, grid_for(ne, B, c->sm_count)), B, 0, c->stream>>>(d_src, d_dst, ne, nv, b, k0,
+                                                                                 c->d_err);
       if ((s = cuda_status(c, cudaGetLastError(), "k_edge_keys")) != XT_OK) break;
       if ((s = check_err(c, "edge list")) != XT_OK) break;
       if ((s = sort_keys(c, k0, k1, ne, 2 * b)) != XT_OK) break;
       k_unique_flags<<<counted(c, grid_for(ne, B, c->sm_count)), B, 0, c->stream>>>(k1, ne, b, flags);
       if ((s = select_flagged(c, k1, flags, k0, ne, &m)) != XT_OK) break;
+      dfree(c, flags);
+      flags = nullptr;
     }
     // k0[0..m) = unique undirected (lo,hi), sorted
     if ((s = dalloc_n(c, &deg, size_t(nv))) != XT_OK) break;
     if ((s = cuda_status(c, cudaMemsetAsync(deg, 0, sizeof(int32_t) * nv, c->stream), "memset")) != XT_OK) break;
     k_degrees<<<counted(c, grid_for(m, B, c->sm_count)), B, 0, c->stream>>>(k0, m, b, deg);
-    if (orient == XT_ORIENT_DEGREE && m > 0) {
-      k_orient_degree<<<counted(c, grid_for(m, B, c->sm_count)), B, 0, c->stream>>>(k0, m, b, deg);
-      if ((s = sort_keys(c, k0, k1, m, 2 * b)) != XT_OK) break;
-      std::swap(k0, k1);
-    }
-    if ((s = cuda_status(c, cudaGetLastError(), "orient")) != XT_OK) break;
-    g->d_deg = deg;
-    deg = nullptr;
-    s = finish_graph(c, k0, m, nv, b, g);
+    if ((s = cuda_status(c, cudaGetLastError(), "degrees")) != XT_OK) break;
+    int32_t *d = deg;
+    deg = nullptr;  // owned by g from here
+    s = orient_and_finish(c, k0, k1, m, nv, b, d, orient, g);
   } while (0);
   dfree(c, k0);
   dfree(c, k1);
@@ -289,6 +369,7 @@ xt_status build_from_csr(Ctx *c, int64_t nv, const int64_t *d_off, const int64_t
                          int orient, Graph *g) {
   if (nv < 1) return set_error(c, XT_ERR_INVALID, "nv must be >= 1");
   if (nv > (int64_t(1) << 31) - 1) return set_error(c, XT_ERR_OVERFLOW, "nv must be below 2^31");
+  if (orient != XT_ORIENT_ID && orient != XT_ORIENT_DEGREE) return set_error(c, XT_ERR_INVALID, "bad orientation");
   int64_t ne_in = 0;
   XT_CUDA(c, cudaMemcpyAsync(&ne_in, d_off + nv, sizeof(int64_t), cudaMemcpyDeviceToHost, c->stream));
   XT_CUDA(c, cudaStreamSynchronize(c->stream));
@@ -300,17 +381,15 @@ xt_status build_from_csr(Ctx *c, int64_t nv, const int64_t *d_off, const int64_t
   do {
     if ((s = dalloc_n(c, &rows, n1)) != XT_OK) break;
     if ((s = dalloc_n(c, &t32, n1)) != XT_OK) break;
-    k_csr_rows<<<counted(c, grid_for(nv * 32, B, c->sm_count)), B, 0, c->stream>>>(d_off, nv, ne_in, rows, c->d_err);
-    k_csr_tails32<<<counted(c, grid_for(ne_in, B, c->sm_count)), B, 0, c->stream>>>(d_tails, ne_in, nv, t32, c->d_err);
+    k_csr_rows<<<counted(c, grid_for(nv * 32, B, c->sm_count)), B, 0, c->stream>>>(d_off, nv, ne_in, rows,
+                                                                                   c->d_err);
+    k_csr_tails32<<<counted(c, grid_for(ne_in, B, c->sm_count)), B, 0, c->stream>>>(d_tails, ne_in, nv, t32,
+                                                                                    c->d_err);
     if ((s = cuda_status(c, cudaGetLastError(), "k_csr_rows")) != XT_OK) break;
     if ((s = check_err(c, "csr")) != XT_OK) break;
     if (!canonical) {
       s = build_from_edges(c, nv, ne_in, rows, t32, orient, g);
       if (s == XT_OK) g->n_input = ne_in;
-      break;
-    }
-    if (orient != XT_ORIENT_ID && orient != XT_ORIENT_DEGREE) {
-      s = set_error(c, XT_ERR_INVALID, "bad orientation");
       break;
     }
     g->ctx = c;
@@ -320,24 +399,30 @@ xt_status build_from_csr(Ctx *c, int64_t nv, const int64_t *d_off, const int64_t
     const int b = bits_for(nv);
     uint64_t *keys = nullptr, *sel = nullptr;
     uint8_t *flags = nullptr;
+    int32_t *deg = nullptr;
     int64_t m = 0;
     do {
       if ((s = dalloc_n(c, &keys, n1)) != XT_OK) break;
       if ((s = dalloc_n(c, &sel, n1)) != XT_OK) break;
       if ((s = dalloc_n(c, &flags, n1)) != XT_OK) break;
-      if ((s = dalloc_n(c, &g->d_deg, size_t(nv))) != XT_OK) break;
-      k_degree_from_off<<<counted(c, grid_for(nv, B, c->sm_count)), B, 0, c->stream>>>(d_off, nv, g->d_deg);
+      if ((s = dalloc_n(c, &deg, size_t(nv))) != XT_OK) break;
+      k_degree_from_off<<<counted(c, grid_for(nv, B, c->sm_count)), B, 0, c->stream>>>(d_off, nv, deg);
       if (ne_in > 0) {
-        k_csr_orient_keys<<<counted(c, grid_for(ne_in, B, c->sm_count)), B, 0, c->stream>>>(rows, t32, ne_in, d_off, orient, b,
-                                                                               keys, flags);
-        if ((s = cuda_status(c, cudaGetLastError(), "k_csr_orient_keys")) != XT_OK) break;
+        k_csr_lower_keys<<<counted(c, grid_for(ne_in, B, c->sm_count)), B, 0, c->stream>>>(rows, t32, ne_in, b,
+                                                                                           keys, flags);
+        if ((s = cuda_status(c, cudaGetLastError(), "k_csr_lower_keys")) != XT_OK) break;
         if ((s = select_flagged(c, keys, flags, sel, ne_in, &m)) != XT_OK) break;
       }
-      s = finish_graph(c, sel, m, nv, b, g);
+      dfree(c, flags);
+      flags = nullptr;
+      int32_t *d = deg;
+      deg = nullptr;
+      s = orient_and_finish(c, sel, keys, m, nv, b, d, orient, g);
     } while (0);
     dfree(c, keys);
     dfree(c, sel);
     dfree(c, flags);
+    dfree(c, deg);
     if (s != XT_OK) free_graph_device(g);
   } while (0);
   dfree(c, rows);
@@ -351,13 +436,15 @@ void free_graph_device(Graph *g) {
   dfree(g->ctx, g->d_off);
   dfree(g->ctx, g->d_col);
   dfree(g->ctx, g->d_ioff);
-  dfree(g->ctx, g->d_icol);
+  dfree(g->ctx, g->d_irec);
   dfree(g->ctx, g->d_deg);
+  dfree(g->ctx, g->d_perm);
   g->d_off = nullptr;
   g->d_col = nullptr;
   g->d_ioff = nullptr;
-  g->d_icol = nullptr;
+  g->d_irec = nullptr;
   g->d_deg = nullptr;
+  g->d_perm = nullptr;
 }
 
 }  // namespace xt

@@ -230,7 +230,7 @@ xt_status xt_graph_get_info(const xt_graph *gr, xt_graph_info *info) {
   info->max_in_degree = g.max_in_degree;
   info->wedge_work = g.wedge_work;
   info->stream_work = g.stream_work;
-  info->alg_bytes = 16 * (g.nv + 1) + 8 * g.ne + 16 * g.ne + 4 * g.stream_work;
+  info->alg_bytes = 16 * (g.nv + 1) + 20 * g.ne + 4 * g.stream_work;
   info->tail_alg_bytes = 8 * (g.nv + 1) + 4 * g.ne + 16 * g.ne + 4 * g.wedge_work;
   info->orient = g.orient;
   return XT_OK;
@@ -245,6 +245,27 @@ xt_status xt_graph_get_csr(const xt_graph *gr, int64_t *offsets, int32_t *cols) 
   if (g.ne > 0)
     XT_CUDA(c, cudaMemcpyAsync(cols, g.d_col, sizeof(int32_t) * g.ne, cudaMemcpyDeviceToHost, c->stream));
   XT_CUDA(c, cudaStreamSynchronize(c->stream));
+  return XT_OK;
+}
+
+xt_status xt_synchronize(xt_ctx *ctx) {
+  if (!ctx) return XT_ERR_INVALID;
+  cudaSetDevice(ctx->c.device);
+  XT_CUDA(&ctx->c, cudaStreamSynchronize(ctx->c.stream));
+  return XT_OK;
+}
+
+xt_status xt_graph_get_perm(const xt_graph *gr, int32_t *new_to_old) {
+  if (!gr || !new_to_old) return XT_ERR_INVALID;
+  const Graph &g = gr->g;
+  Ctx *c = g.ctx;
+  cudaSetDevice(c->device);
+  if (g.d_perm) {
+    XT_CUDA(c, cudaMemcpyAsync(new_to_old, g.d_perm, sizeof(int32_t) * g.nv, cudaMemcpyDeviceToHost, c->stream));
+    XT_CUDA(c, cudaStreamSynchronize(c->stream));
+  } else {
+    for (int64_t i = 0; i < g.nv; i++) new_to_old[i] = int32_t(i);
+  }
   return XT_OK;
 }
 

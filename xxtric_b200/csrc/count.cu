@@ -1,46 +1,49 @@
-// Degree-binned schedule and the exact triangle-count kernels.
+// Degree-binned schedule and the exact triangle-count kernel.
 //
-// Orientation sends every undirected edge from its lower- to its higher-rank
-// end, so every triangle {u,v,w} with rank u < v < w appears exactly once as
-// u->v, u->w, v->w. The reference finds it from the lowest corner with a
-// binary search per wedge (xxtric.hpp:150-207, counting.cu:579-638). Here it
-// is found from the MIDDLE corner v: the out-list N+(v) is hashed once into
-// shared memory, and the out-lists N+(u) of v's in-neighbours u are streamed
-// through the hash; each hit w closes the triangle (u,v,w). The items read
-// are sum_u d+(u)^2 instead of the tail-grouped sum over edges of d+(v),
-// and every probe is a shared-memory lookup.
+// Vertices are numbered by orientation rank (see build.cu), so every triangle
+// {u,v,w} with u < v < w is the edges u->v, u->w, v->w. The reference finds it
+// from the lowest corner i=u: for every pair m < n of its sorted row it
+// binary-searches adj(v) for w (xxtric.hpp:150-207, check_edgelist
+// xxtric.hpp:516-545). Here it is found from the MIDDLE corner v:
+//   1. N+(v) is loaded once into shared memory as a membership structure:
+//      a bitmap over [min N+(v), max N+(v)] when that range is small enough,
+//      else an open-addressing hash table (load factor <= 1/4);
+//   2. for every in-edge u->v, the suffix of N+(u) after v (the reference's
+//      n > m range) is streamed through it. A candidate below min N+(v) is
+//      skipped and one above max N+(v) ends that suffix (the reference's
+//      edge_above_min / edge_within_max prunes, xxtric.hpp:576-588).
+// Items streamed: sum over u of C(d+(u), 2), each tested in shared memory.
 //
-// Schedule (make_plan): per head v, work(v) = sum over u in N-(v) of d+(u).
+// Schedule (make_plan): per head v, work(v) = total suffix length.
 //   warp bin : d+(v) <= kWarpDmax and work(v) <= kWarpWork -> one warp per v
-//   block bin: d+(v) <= kBlockDmax -> CTA tasks over chunks of N-(v) of
-//              about kBlockWork items each
-//   part bin : d+(v) >  kBlockDmax -> N+(v) split into hash parts of
-//              kBlockDmax keys, each part x each chunk one CTA task
-// One persistent kernel drains the CTA tasks first (largest unit of work),
-// then the warp tasks, each from a global atomic cursor.
+//   block bin: otherwise -> CTA tasks over chunks of v's in-records of about
+//              kBlockWork items; N+(v) beyond kBlockDmax members is split
+//              into parts, one task per (part, chunk)
+// One persistent kernel drains the CTA tasks first (the large ones), then the
+// warp tasks, each from its own global atomic cursor.
 #include <cub/cub.cuh>
 
 #include "xt_internal.cuh"
 
 namespace xt {
 
-constexpr int kThreads = 512;
+constexpr int kThreads = 256;
 constexpr int kWarps = kThreads / 32;
-constexpr int kWarpDmax = 64;     // warp hash: 128 slots
-constexpr int kWarpSlots = 128;
-constexpr int64_t kWarpWork = 2048;
-constexpr int kBlockDmax = 2048;  // CTA hash: up to 4096 slots
-constexpr int kBlockSlots = 4096;
-constexpr int64_t kBlockWork = 1 << 16;
+constexpr int kWarpDmax = 64;
+constexpr int kWarpWords = 256;   // per-warp region: 256-slot hash or 8192-bit bitmap
+constexpr int64_t kWarpWork = 4096;
+constexpr int kBlockDmax = 2048;
+constexpr int kBlockWords = 8192;  // CTA region: 8192-slot hash or 2^18-bit bitmap
+constexpr int64_t kBlockWork = 1 << 18;
 constexpr int32_t kEmpty = -1;
 
 struct Plan {
   int64_t n_btask = 0;        // CTA tasks
-  int64_t *d_bt = nullptr;    // 4 int64 per task: v, part, k0, k1 (k = index into d_icol)
+  int64_t *d_bt = nullptr;    // 4 int64 per task: v, part, k0, k1 (k = in-record index)
   int64_t n_wtask = 0;        // warp tasks
   int32_t *d_wt = nullptr;    // v per warp task
   unsigned long long *d_cursor = nullptr;  // [0] CTA cursor, [1] warp cursor
-  int grid = 0;
+  int grid_global = 0, grid_pv = 0;
 };
 
 static unsigned grid_for(int64_t n, int block, int sm_count) {
@@ -51,39 +54,32 @@ static unsigned grid_for(int64_t n, int block, int sm_count) {
   return (unsigned)g;
 }
 
+#define XT_GRID_STRIDE(i, n) \
+  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < (n); i += int64_t(gridDim.x) * blockDim.x)
+
 // ---- plan kernels -----------------------------------------------------------
 
-// w[e] = d+(icol[e]) for every in-edge e (the items that edge streams)
-__global__ void k_inedge_work(const int32_t *__restrict__ icol, int64_t ne, const int64_t *__restrict__ off,
-                              int64_t *__restrict__ w) {
-  for (int64_t e = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; e < ne; e += int64_t(gridDim.x) * blockDim.x) {
-    int32_t u = icol[e];
-    w[e] = off[u + 1] - off[u];
-  }
+__global__ void k_inrec_work(const InRec *__restrict__ rec, int64_t ne, int64_t *__restrict__ w) {
+  XT_GRID_STRIDE(e, ne) w[e] = rec[e].len;
 }
 
-// tail-grouped work: d+(col[e]) per out-edge
+// tail-grouped work (statistics): d+(col[e]) per out-edge
 __global__ void k_outedge_work(const int32_t *__restrict__ col, int64_t ne, const int64_t *__restrict__ off,
                                int64_t *__restrict__ w) {
-  for (int64_t e = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; e < ne; e += int64_t(gridDim.x) * blockDim.x) {
-    int32_t v = col[e];
+  XT_GRID_STRIDE(e, ne) {
+    const int32_t v = col[e];
     w[e] = off[v + 1] - off[v];
   }
 }
 
-struct BinCounts {
-  int64_t btasks;
-  int64_t wtasks;
-};
-
 __device__ __forceinline__ void classify(int64_t v, const int64_t *__restrict__ off, const int64_t *__restrict__ ioff,
                                          const int64_t *__restrict__ P, int64_t &nb, int64_t &nw, int64_t &parts,
                                          int64_t &chunks, int64_t &work) {
-  int64_t dp = off[v + 1] - off[v];
-  int64_t k0 = ioff[v], k1 = ioff[v + 1];
+  const int64_t dp = off[v + 1] - off[v];
+  const int64_t k0 = ioff[v], k1 = ioff[v + 1];
   nb = nw = parts = chunks = 0;
   work = P[k1] - P[k0];
-  if (dp == 0 || k1 == k0 || work == 0) return;
+  if (dp == 0 || work == 0) return;
   if (dp <= kWarpDmax && work <= kWarpWork) {
     nw = 1;
     return;
@@ -96,7 +92,7 @@ __device__ __forceinline__ void classify(int64_t v, const int64_t *__restrict__ 
 __global__ void k_plan_count(int64_t nv, const int64_t *__restrict__ off, const int64_t *__restrict__ ioff,
                              const int64_t *__restrict__ P, int64_t *__restrict__ nb_out,
                              int64_t *__restrict__ nw_out) {
-  for (int64_t v = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; v < nv; v += int64_t(gridDim.x) * blockDim.x) {
+  XT_GRID_STRIDE(v, nv) {
     int64_t nb, nw, parts, chunks, work;
     classify(v, off, ioff, P, nb, nw, parts, chunks, work);
     nb_out[v] = nb;
@@ -107,7 +103,7 @@ __global__ void k_plan_count(int64_t nv, const int64_t *__restrict__ off, const 
 // first k in [lo,hi] with P[k] >= x
 __device__ __forceinline__ int64_t lower_bound_i64(const int64_t *__restrict__ P, int64_t lo, int64_t hi, int64_t x) {
   while (lo < hi) {
-    int64_t mid = lo + (hi - lo) / 2;
+    const int64_t mid = lo + (hi - lo) / 2;
     if (P[mid] < x) lo = mid + 1;
     else hi = mid;
   }
@@ -117,17 +113,16 @@ __device__ __forceinline__ int64_t lower_bound_i64(const int64_t *__restrict__ P
 __global__ void k_plan_fill(int64_t nv, const int64_t *__restrict__ off, const int64_t *__restrict__ ioff,
                             const int64_t *__restrict__ P, const int64_t *__restrict__ nb_pos,
                             const int64_t *__restrict__ nw_pos, int64_t *__restrict__ bt, int32_t *__restrict__ wt) {
-  for (int64_t v = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; v < nv; v += int64_t(gridDim.x) * blockDim.x) {
+  XT_GRID_STRIDE(v, nv) {
     int64_t nb, nw, parts, chunks, work;
     classify(v, off, ioff, P, nb, nw, parts, chunks, work);
     if (nw) wt[nw_pos[v]] = int32_t(v);
     if (!nb) continue;
     const int64_t k0 = ioff[v], k1 = ioff[v + 1], base = P[k0];
-    int64_t t = nb_pos[v];
-    int64_t prev = k0;
+    int64_t t = nb_pos[v], prev = k0;
     for (int64_t c = 0; c < chunks; c++) {
-      int64_t kend = (c + 1 == chunks) ? k1 : lower_bound_i64(P, prev, k1, base + (work * (c + 1)) / chunks);
-      if (kend <= prev) continue;  // empty chunk (a single in-neighbour carries more work)
+      const int64_t kend = (c + 1 == chunks) ? k1 : lower_bound_i64(P, prev, k1, base + (work * (c + 1)) / chunks);
+      if (kend <= prev) continue;  // empty chunk (one in-record carries more work)
       for (int64_t p = 0; p < parts; p++) {
         bt[4 * t + 0] = v;
         bt[4 * t + 1] = p;
@@ -137,8 +132,7 @@ __global__ void k_plan_fill(int64_t nv, const int64_t *__restrict__ off, const i
       }
       prev = kend;
     }
-    // unused slots (empty chunks) become no-op tasks
-    for (; t < nb_pos[v] + nb; t++) {
+    for (; t < nb_pos[v] + nb; t++) {  // slots of empty chunks: no-op tasks
       bt[4 * t + 0] = v;
       bt[4 * t + 1] = 0;
       bt[4 * t + 2] = k1;
@@ -147,95 +141,267 @@ __global__ void k_plan_fill(int64_t nv, const int64_t *__restrict__ off, const i
   }
 }
 
-// ---- count kernel -----------------------------------------------------------
+// ---- membership structures --------------------------------------------------
 
 __device__ __forceinline__ uint32_t hash_slot(int32_t x, int shift) {
   return (uint32_t(x) * 0x9E3779B1u) >> shift;
 }
 
-template <bool PV>
 __device__ __forceinline__ void hash_insert(int32_t *tab, uint32_t mask, int shift, int32_t x) {
   uint32_t h = hash_slot(x, shift);
   while (true) {
-    int32_t old = atomicCAS(&tab[h], kEmpty, x);
+    const int32_t old = atomicCAS(&tab[h], kEmpty, x);
     if (old == kEmpty || old == x) return;
     h = (h + 1) & mask;
   }
 }
 
-// returns the slot holding x, or -1
+// the slot holding x, or -1
 __device__ __forceinline__ int hash_find(const int32_t *tab, uint32_t mask, int shift, int32_t x) {
   uint32_t h = hash_slot(x, shift);
   while (true) {
-    int32_t k = tab[h];
+    const int32_t k = tab[h];
     if (k == x) return int(h);
     if (k == kEmpty) return -1;
     h = (h + 1) & mask;
   }
 }
 
-__device__ __forceinline__ int log2_slots(int64_t d, int min_slots) {
-  int lg = 0;
-  while ((int64_t(1) << lg) < 2 * d || (1 << lg) < min_slots) lg++;
-  return lg;
+// The member set N+(v) (or one part of it) in shared memory.
+struct Members {
+  int32_t *words;   // bitmap words or hash slots
+  int32_t *cnt;     // per-slot hit counters (per-vertex mode, hash only)
+  int32_t lo, hi;   // smallest and largest member
+  uint32_t mask;    // hash: slots - 1
+  int shift;        // hash: 32 - log2(slots)
+  bool bitmap;
+};
+
+// Chooses the structure for members col[r0, r1) that fits `words` words and
+// returns how many words must be cleared.
+template <bool PV>
+__device__ __forceinline__ int members_layout(Members &m, const int32_t *__restrict__ col, int64_t r0, int64_t r1,
+                                              int words) {
+  m.lo = col[r0];
+  m.hi = col[r1 - 1];
+  const int64_t range = int64_t(m.hi) - int64_t(m.lo) + 1;
+  m.bitmap = !PV && range <= int64_t(words) * 32;
+  if (m.bitmap) {
+    m.mask = 0;
+    m.shift = 0;
+    return int((range + 31) >> 5);
+  }
+  int lg = 6;
+  while ((int64_t(1) << lg) < 4 * (r1 - r0)) lg++;  // load factor <= 1/4: an absent key costs ~1.2 probes
+  m.mask = (1u << lg) - 1;
+  m.shift = 32 - lg;
+  return 1 << lg;
 }
 
-// One warp streams the out-lists of in-neighbours icol[k] (k = kbeg, kbeg+kstep, ...
-// in 32-wide batches) through the hash tab. Returns this lane's hit count.
-template <bool PV>
-__device__ __forceinline__ int64_t stream_inlists(const int64_t *__restrict__ off, const int32_t *__restrict__ col,
-                                                  const int32_t *__restrict__ icol, int64_t kbeg, int64_t kend,
-                                                  int64_t kstep, const int32_t *tab, int32_t *cnt, uint32_t mask,
-                                                  int shift, int64_t *__restrict__ pv, int lane) {
-  int64_t hits = 0;
-  for (int64_t kb = kbeg; kb < kend; kb += kstep) {
-    const int64_t k = kb + lane;
-    int32_t u = 0;
-    int64_t s = 0, e = 0;
-    if (k < kend) {
-      u = icol[k];
-      s = off[u];
-      e = off[u + 1];
+__device__ __forceinline__ void members_insert(const Members &m, int32_t x) {
+  if (m.bitmap) {
+    const uint32_t d = uint32_t(x - m.lo);
+    atomicOr(reinterpret_cast<unsigned int *>(&m.words[d >> 5]), 1u << (d & 31));
+  } else {
+    hash_insert(m.words, m.mask, m.shift, x);
+  }
+}
+
+// ---- streaming the in-record suffixes ----------------------------------------
+
+// A warp step: 32 aligned 16-byte groups (one LDG.128 per lane) of one suffix.
+struct Chunk {
+  int4 x;          // four columns of this lane's group
+  int64_t grp;     // group index (columns 4*grp .. 4*grp+3)
+  int64_t s, e;    // the suffix [s, e)
+  int32_t u;       // its owner (per-vertex credit)
+  int32_t serial;  // which suffix of the walk (warp-uniform)
+  bool exists;     // warp-uniform: this step exists
+};
+
+// One warp's walk over the in-records rec[k0, kend), taken in batches of bsz
+// records (lane j < bsz holds record j of a batch). Batches come one after
+// another (a warp task), or from a cursor in shared memory that the warps of
+// a CTA task share, so warps that finish early take more. The next batch is
+// claimed and its records loaded while the current one streams.
+// Control flow is warp-uniform.
+struct RecWalk {
+  const InRec *__restrict__ rec;
+  const int32_t *__restrict__ col;
+  int *cursor;              // shared batch cursor (CTA task) or null
+  int64_t k0, kend;         // the task's records
+  int64_t kb, nkb, seq;     // current / next batch base, next sequential base
+  int bsz, nb, j;
+  int64_t bs, be;           // lane's record of this batch
+  int32_t bu;
+  int4 nrec;                // lane's record of the next batch (prefetched)
+  int64_t cs, ce, g, gend;  // current suffix and group cursor
+  int32_t cu, serial;
+  bool have;
+  int lane;
+
+  __device__ __forceinline__ int64_t claim() {
+    if (!cursor) {
+      const int64_t b = seq;
+      seq += bsz;
+      return b;
     }
-    const int nb = (kend - kb < 32) ? int(kend - kb) : 32;
-    for (int j = 0; j < nb; j++) {
-      const int64_t sj = __shfl_sync(0xffffffffu, s, j);
-      const int64_t ej = __shfl_sync(0xffffffffu, e, j);
-      int64_t h = 0;
-      for (int64_t p = sj + lane; p < ej; p += 32) {
-        const int32_t w = col[p];
-        const int slot = hash_find(tab, mask, shift, w);
-        if (slot >= 0) {
-          h++;
-          if (PV) atomicAdd(&cnt[slot], 1);
+    int r = 0;
+    if (lane == 0) r = atomicAdd(cursor, bsz);
+    return k0 + __shfl_sync(0xffffffffu, r, 0);
+  }
+  __device__ __forceinline__ int4 fetch(int64_t base) const {
+    const int64_t k = base + lane;
+    return (lane < bsz && k < kend) ? __ldg(reinterpret_cast<const int4 *>(rec) + k) : make_int4(0, 0, 0, -1);
+  }
+  __device__ __forceinline__ void take(int4 r) {
+    bs = int64_t(uint32_t(r.x)) | (int64_t(r.y) << 32);
+    be = bs + r.z;
+    bu = r.w;
+    nb = (kend - kb < bsz) ? int(kend - kb) : bsz;
+    nkb = claim();
+    nrec = fetch(nkb);
+  }
+  __device__ __forceinline__ void select(int jj) {
+    j = jj;
+    cs = __shfl_sync(0xffffffffu, bs, jj);
+    ce = __shfl_sync(0xffffffffu, be, jj);
+    cu = __shfl_sync(0xffffffffu, bu, jj);
+    g = cs >> 2;
+    gend = (ce + 3) >> 2;
+    if (cs == ce) gend = g;  // empty suffix
+    serial++;
+  }
+  __device__ __forceinline__ void init() {
+    nb = j = 0;
+    bs = be = cs = ce = g = gend = 0;
+    bu = cu = -1;
+    serial = 0;
+    seq = k0;
+    kb = claim();
+    have = kb < kend;
+    if (!have) return;
+    take(fetch(kb));
+    select(0);
+  }
+  __device__ __forceinline__ void advance() {
+    while (have && g >= gend) {
+      if (j + 1 < nb) {
+        select(j + 1);
+      } else {
+        kb = nkb;
+        if (kb >= kend) {
+          have = false;
+          break;
         }
-      }
-      hits += h;
-      if (PV) {
-        int64_t tot = h;
-        for (int o = 16; o; o >>= 1) tot += __shfl_xor_sync(0xffffffffu, tot, o);
-        const int32_t uj = __shfl_sync(0xffffffffu, u, j);
-        if (lane == 0 && tot) atomicAdd(reinterpret_cast<unsigned long long *>(&pv[uj]), (unsigned long long)tot);
+        take(nrec);
+        select(0);
       }
     }
+  }
+  __device__ __forceinline__ Chunk issue() {
+    Chunk c;
+    advance();
+    c.exists = have;
+    c.grp = g + lane;
+    c.s = cs;
+    c.e = ce;
+    c.u = cu;
+    c.serial = serial;
+    c.x = make_int4(0, 0, 0, 0);
+    if (have) {
+      if (c.grp < gend) c.x = __ldg(reinterpret_cast<const int4 *>(col) + c.grp);
+      g += 32;
+    }
+    return c;
+  }
+};
+
+// Probes a chunk; returns this lane's hits and sets `past` when none of the
+// lane's valid columns is <= m.hi (so the rest of the suffix is past it).
+template <bool PV>
+__device__ __forceinline__ int probe_chunk(const Chunk &c, const Members &m, bool &past) {
+  int h = 0;
+  past = true;
+  const int64_t p0 = 4 * c.grp;
+  const int32_t w[4] = {c.x.x, c.x.y, c.x.z, c.x.w};
+#pragma unroll
+  for (int i = 0; i < 4; i++) {
+    const int64_t p = p0 + i;
+    if (p < c.s || p >= c.e) continue;
+    const int32_t x = w[i];
+    if (x <= m.hi) past = false;
+    if (x < m.lo || x > m.hi) continue;
+    if (m.bitmap) {
+      const uint32_t d = uint32_t(x - m.lo);
+      h += (m.words[d >> 5] >> (d & 31)) & 1;
+    } else {
+      const int slot = hash_find(m.words, m.mask, m.shift, x);
+      if (slot >= 0) {
+        h++;
+        if (PV) atomicAdd(&m.cnt[slot], 1);
+      }
+    }
+  }
+  return h;
+}
+
+// Streams the suffixes of in-records [k0, kend) in batches of bsz records
+// (claimed from `cursor` when it is not null) through the member set;
+// returns this lane's hit count.
+template <bool PV>
+__device__ __forceinline__ int64_t stream_suffixes(const InRec *__restrict__ rec, const int32_t *__restrict__ col,
+                                                   int64_t k0, int64_t kend, int bsz, int *cursor, const Members &m,
+                                                   int64_t *__restrict__ pv, int lane) {
+  RecWalk wk;
+  wk.rec = rec;
+  wk.col = col;
+  wk.cursor = cursor;
+  wk.k0 = k0;
+  wk.kend = kend;
+  wk.bsz = bsz;
+  wk.lane = lane;
+  wk.init();
+  int64_t hits = 0;
+  Chunk a = wk.issue();
+  while (a.exists) {
+    Chunk b = wk.issue();  // the next step's loads are in flight during these probes
+    bool past;
+    const int h = probe_chunk<PV>(a, m, past);
+    hits += h;
+    if (PV) {
+      int tot = h;
+      for (int o = 16; o; o >>= 1) tot += __shfl_xor_sync(0xffffffffu, tot, o);
+      if (lane == 0 && tot) atomicAdd(reinterpret_cast<unsigned long long *>(&pv[a.u]), (unsigned long long)tot);
+    }
+    if (__all_sync(0xffffffffu, past) && b.exists && b.serial == a.serial) {
+      // the suffix is sorted: every later column is above max N+(v) too, so
+      // drop the step already in flight and the rest of this suffix
+      wk.g = wk.gend;
+      b = wk.issue();
+    }
+    a = b;
   }
   return hits;
 }
 
+// ---- the count kernel ---------------------------------------------------------
+
 template <bool PV>
-__global__ void __launch_bounds__(kThreads) k_count(const int64_t *__restrict__ off, const int32_t *__restrict__ col,
-                                                    const int64_t *__restrict__ ioff,
-                                                    const int32_t *__restrict__ icol, const int64_t *__restrict__ bt,
-                                                    int64_t n_bt, const int32_t *__restrict__ wt, int64_t n_wt,
-                                                    unsigned long long *__restrict__ cursor,
-                                                    unsigned long long *__restrict__ global,
-                                                    int64_t *__restrict__ pv) {
+__global__ void __launch_bounds__(kThreads, 4) k_count(const int64_t *__restrict__ off, const int32_t *__restrict__ col,
+                                                       const int64_t *__restrict__ ioff,
+                                                       const InRec *__restrict__ rec, const int64_t *__restrict__ bt,
+                                                       int64_t n_bt, const int32_t *__restrict__ wt, int64_t n_wt,
+                                                       unsigned long long *__restrict__ cursor,
+                                                       unsigned long long *__restrict__ global,
+                                                       int64_t *__restrict__ pv) {
   extern __shared__ int32_t smem[];
-  int32_t *btab = smem;                                       // kBlockSlots
-  int32_t *bcnt = smem + kBlockSlots;                         // kBlockSlots (PV only)
-  int32_t *wtab_all = smem + (PV ? 2 : 1) * kBlockSlots;      // kWarps * kWarpSlots
-  int32_t *wcnt_all = wtab_all + kWarps * kWarpSlots;         // (PV only)
+  int32_t *bwords = smem;                                   // kBlockWords
+  int32_t *bcnt = smem + kBlockWords;                       // kBlockWords (PV only)
+  int32_t *wwords_all = smem + (PV ? 2 : 1) * kBlockWords;  // kWarps * kWarpWords
+  int32_t *wcnt_all = wwords_all + kWarps * kWarpWords;     // (PV only)
   __shared__ int64_t s_task;
+  __shared__ int s_batch;  // next in-record batch of the current CTA task
   __shared__ unsigned long long s_red[kWarps];
 
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -243,24 +409,31 @@ __global__ void __launch_bounds__(kThreads) k_count(const int64_t *__restrict__ 
 
   // ---- CTA tasks ----
   while (true) {
-    if (tid == 0) s_task = (int64_t)atomicAdd(&cursor[0], 1ull);
+    if (tid == 0) {
+      s_task = int64_t(atomicAdd(&cursor[0], 1ull));
+      s_batch = 0;
+    }
     __syncthreads();
     const int64_t t = s_task;
     if (t >= n_bt) break;
     const int64_t v = bt[4 * t], part = bt[4 * t + 1], k0 = bt[4 * t + 2], k1 = bt[4 * t + 3];
     const int64_t r0 = off[v] + part * kBlockDmax;
     const int64_t r1 = min(off[v + 1], r0 + kBlockDmax);
-    const int lg = log2_slots(r1 - r0, 64);
-    const uint32_t mask = (1u << lg) - 1;
-    const int shift = 32 - lg;
-    for (int i = tid; i <= int(mask); i += kThreads) {
-      btab[i] = kEmpty;
+    Members m;
+    m.words = bwords;
+    m.cnt = bcnt;
+    const int nclear = members_layout<PV>(m, col, r0, r1, kBlockWords);
+    for (int i = tid; i < nclear; i += kThreads) {
+      bwords[i] = m.bitmap ? 0 : kEmpty;
       if (PV) bcnt[i] = 0;
     }
     __syncthreads();
-    for (int64_t p = r0 + tid; p < r1; p += kThreads) hash_insert<PV>(btab, mask, shift, col[p]);
+    for (int64_t p = r0 + tid; p < r1; p += kThreads) members_insert(m, col[p]);
     __syncthreads();
-    int64_t h = stream_inlists<PV>(off, col, icol, k0 + 32 * warp, k1, 32 * kWarps, btab, bcnt, mask, shift, pv, lane);
+    // batches small enough that every warp gets several of them
+    int64_t bsz = (k1 - k0) / (4 * kWarps);
+    bsz = bsz < 1 ? 1 : (bsz > 32 ? 32 : bsz);
+    int64_t h = stream_suffixes<PV>(rec, col, k0, k1, int(bsz), &s_batch, m, pv, lane);
     acc += h;
     if (PV) {
       for (int o = 16; o; o >>= 1) h += __shfl_xor_sync(0xffffffffu, h, o);
@@ -273,42 +446,43 @@ __global__ void __launch_bounds__(kThreads) k_count(const int64_t *__restrict__ 
         for (int w = 0; w < kWarps; w++) tot += s_red[w];
         if (tot) atomicAdd(reinterpret_cast<unsigned long long *>(&pv[v]), tot);
       }
-      for (int i = tid; i <= int(mask); i += kThreads)
-        if (bcnt[i]) atomicAdd(reinterpret_cast<unsigned long long *>(&pv[btab[i]]), (unsigned long long)bcnt[i]);
+      for (int i = tid; i < nclear; i += kThreads)
+        if (bcnt[i]) atomicAdd(reinterpret_cast<unsigned long long *>(&pv[bwords[i]]), (unsigned long long)bcnt[i]);
       __syncthreads();
     }
   }
 
   // ---- warp tasks ----
-  int32_t *wtab = wtab_all + warp * kWarpSlots;
-  int32_t *wcnt = wcnt_all + warp * kWarpSlots;
+  int32_t *wwords = wwords_all + warp * kWarpWords;
+  int32_t *wcnt = wcnt_all + warp * kWarpWords;
   while (true) {
     int64_t t = 0;
-    if (lane == 0) t = (int64_t)atomicAdd(&cursor[1], 1ull);
+    if (lane == 0) t = int64_t(atomicAdd(&cursor[1], 1ull));
     t = __shfl_sync(0xffffffffu, t, 0);
     if (t >= n_wt) break;
     const int32_t v = wt[t];
     const int64_t r0 = off[v], r1 = off[v + 1];
-    const int lg = log2_slots(r1 - r0, kWarpSlots);
-    const uint32_t mask = (1u << lg) - 1;
-    const int shift = 32 - lg;
-    for (int i = lane; i < kWarpSlots; i += 32) {
-      wtab[i] = kEmpty;
+    Members m;
+    m.words = wwords;
+    m.cnt = wcnt;
+    const int nclear = members_layout<PV>(m, col, r0, r1, kWarpWords);
+    for (int i = lane; i < nclear; i += 32) {
+      wwords[i] = m.bitmap ? 0 : kEmpty;
       if (PV) wcnt[i] = 0;
     }
     __syncwarp();
-    for (int64_t p = r0 + lane; p < r1; p += 32) hash_insert<PV>(wtab, mask, shift, col[p]);
+    for (int64_t p = r0 + lane; p < r1; p += 32) members_insert(m, col[p]);
     __syncwarp();
-    int64_t h = stream_inlists<PV>(off, col, icol, ioff[v], ioff[v + 1], 32, wtab, wcnt, mask, shift, pv, lane);
+    int64_t h = stream_suffixes<PV>(rec, col, ioff[v], ioff[v + 1], 32, nullptr, m, pv, lane);
     acc += h;
     if (PV) {
       for (int o = 16; o; o >>= 1) h += __shfl_xor_sync(0xffffffffu, h, o);
       __syncwarp();
       if (lane == 0 && h) atomicAdd(reinterpret_cast<unsigned long long *>(&pv[v]), (unsigned long long)h);
-      for (int i = lane; i < kWarpSlots; i += 32)
-        if (wcnt[i]) atomicAdd(reinterpret_cast<unsigned long long *>(&pv[wtab[i]]), (unsigned long long)wcnt[i]);
-      __syncwarp();
+      for (int i = lane; i < nclear; i += 32)
+        if (wcnt[i]) atomicAdd(reinterpret_cast<unsigned long long *>(&pv[wwords[i]]), (unsigned long long)wcnt[i]);
     }
+    __syncwarp();
   }
 
   // ---- reduce ----
@@ -324,28 +498,31 @@ __global__ void __launch_bounds__(kThreads) k_count(const int64_t *__restrict__ 
 }
 
 static size_t count_smem_bytes(bool pv) {
-  return sizeof(int32_t) * ((pv ? 2 : 1) * kBlockSlots + (pv ? 2 : 1) * kWarps * kWarpSlots);
+  return sizeof(int32_t) * size_t(pv ? 2 : 1) * (kBlockWords + kWarps * kWarpWords);
+}
+
+// per-vertex counts in internal numbering -> input numbering
+__global__ void k_unpermute(const int64_t *__restrict__ in, const int32_t *__restrict__ n2o, int64_t nv,
+                            int64_t *__restrict__ out) {
+  XT_GRID_STRIDE(r, nv) out[n2o[r]] = in[r];
 }
 
 __global__ void k_max_i32(const int32_t *__restrict__ a, int64_t n, unsigned long long *out) {
   unsigned long long m = 0;
-  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x)
-    m = max(m, (unsigned long long)a[i]);
+  XT_GRID_STRIDE(i, n) m = max(m, (unsigned long long)a[i]);
   for (int o = 16; o; o >>= 1) m = max(m, __shfl_xor_sync(0xffffffffu, m, o));
   if ((threadIdx.x & 31) == 0) atomicMax(out, m);
 }
 
 __global__ void k_max_rowlen(const int64_t *__restrict__ off, int64_t nv, unsigned long long *out) {
   unsigned long long m = 0;
-  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < nv; i += int64_t(gridDim.x) * blockDim.x)
-    m = max(m, (unsigned long long)(off[i + 1] - off[i]));
+  XT_GRID_STRIDE(i, nv) m = max(m, (unsigned long long)(off[i + 1] - off[i]));
   for (int o = 16; o; o >>= 1) m = max(m, __shfl_xor_sync(0xffffffffu, m, o));
   if ((threadIdx.x & 31) == 0) atomicMax(out, m);
 }
 
 // ---- host side --------------------------------------------------------------
 
-template <class F>
 static xt_status exclusive_scan(Ctx *c, const int64_t *in, int64_t *out, int64_t n) {
   size_t bytes = 0;
   XT_CUDA(c, cub::DeviceScan::ExclusiveSum(nullptr, bytes, in, out, n, c->stream));
@@ -367,6 +544,10 @@ void free_plan(Graph *g) {
   g->plan = nullptr;
 }
 
+static xt_status d2h(Ctx *c, void *h, const void *d, size_t bytes) {
+  return cuda_status(c, cudaMemcpyAsync(h, d, bytes, cudaMemcpyDeviceToHost, c->stream), "D2H");
+}
+
 xt_status make_plan(Graph *g) {
   Ctx *c = g->ctx;
   free_plan(g);
@@ -385,21 +566,18 @@ xt_status make_plan(Graph *g) {
     if ((s = cuda_status(c, cudaMemsetAsync(stats, 0, 4 * sizeof(unsigned long long), c->stream), "memset")) !=
         XT_OK)
       break;
-    // graph statistics
     k_max_i32<<<counted(c, grid_for(nv, B, c->sm_count)), B, 0, c->stream>>>(g->d_deg, nv, stats + 0);
     k_max_rowlen<<<counted(c, grid_for(nv, B, c->sm_count)), B, 0, c->stream>>>(g->d_off, nv, stats + 1);
     k_max_rowlen<<<counted(c, grid_for(nv, B, c->sm_count)), B, 0, c->stream>>>(g->d_ioff, nv, stats + 2);
-    // tail-grouped work (statistics only)
+    // tail-grouped work, for the statistics only
     k_outedge_work<<<counted(c, grid_for(ne, B, c->sm_count)), B, 0, c->stream>>>(g->d_col, ne, g->d_off, w);
     if ((s = cuda_status(c, cudaMemsetAsync(w + ne, 0, sizeof(int64_t), c->stream), "memset")) != XT_OK) break;
-    if ((s = exclusive_scan<int64_t>(c, w, P, ne + 1)) != XT_OK) break;
+    if ((s = exclusive_scan(c, w, P, ne + 1)) != XT_OK) break;
     int64_t tail_work = 0;
-    if ((s = cuda_status(c, cudaMemcpyAsync(&tail_work, P + ne, sizeof(int64_t), cudaMemcpyDeviceToHost, c->stream),
-                         "memcpy")) != XT_OK)
-      break;
-    // head-grouped work prefix over in-edges
-    k_inedge_work<<<counted(c, grid_for(ne, B, c->sm_count)), B, 0, c->stream>>>(g->d_icol, ne, g->d_off, w);
-    if ((s = exclusive_scan<int64_t>(c, w, P, ne + 1)) != XT_OK) break;
+    if ((s = d2h(c, &tail_work, P + ne, sizeof(int64_t))) != XT_OK) break;
+    // suffix lengths, prefix-summed in head order
+    k_inrec_work<<<counted(c, grid_for(ne, B, c->sm_count)), B, 0, c->stream>>>(g->d_irec, ne, w);
+    if ((s = exclusive_scan(c, w, P, ne + 1)) != XT_OK) break;
     if ((s = dalloc_n(c, &nb, size_t(nv + 1))) != XT_OK) break;
     if ((s = dalloc_n(c, &nw, size_t(nv + 1))) != XT_OK) break;
     if ((s = dalloc_n(c, &nbp, size_t(nv + 1))) != XT_OK) break;
@@ -407,23 +585,14 @@ xt_status make_plan(Graph *g) {
     k_plan_count<<<counted(c, grid_for(nv, B, c->sm_count)), B, 0, c->stream>>>(nv, g->d_off, g->d_ioff, P, nb, nw);
     if ((s = cuda_status(c, cudaMemsetAsync(nb + nv, 0, sizeof(int64_t), c->stream), "memset")) != XT_OK) break;
     if ((s = cuda_status(c, cudaMemsetAsync(nw + nv, 0, sizeof(int64_t), c->stream), "memset")) != XT_OK) break;
-    if ((s = exclusive_scan<int64_t>(c, nb, nbp, nv + 1)) != XT_OK) break;
-    if ((s = exclusive_scan<int64_t>(c, nw, nwp, nv + 1)) != XT_OK) break;
-    int64_t h[2] = {0, 0};
+    if ((s = exclusive_scan(c, nb, nbp, nv + 1)) != XT_OK) break;
+    if ((s = exclusive_scan(c, nw, nwp, nv + 1)) != XT_OK) break;
+    int64_t h[3] = {0, 0, 0};
     unsigned long long hs[4] = {0, 0, 0, 0};
-    if ((s = cuda_status(c, cudaMemcpyAsync(&h[0], nbp + nv, sizeof(int64_t), cudaMemcpyDeviceToHost, c->stream),
-                         "memcpy")) != XT_OK)
-      break;
-    if ((s = cuda_status(c, cudaMemcpyAsync(&h[1], nwp + nv, sizeof(int64_t), cudaMemcpyDeviceToHost, c->stream),
-                         "memcpy")) != XT_OK)
-      break;
-    int64_t head_work = 0;
-    if ((s = cuda_status(c, cudaMemcpyAsync(&head_work, P + ne, sizeof(int64_t), cudaMemcpyDeviceToHost, c->stream),
-                         "memcpy")) != XT_OK)
-      break;
-    if ((s = cuda_status(c, cudaMemcpyAsync(hs, stats, sizeof(hs), cudaMemcpyDeviceToHost, c->stream), "memcpy")) !=
-        XT_OK)
-      break;
+    if ((s = d2h(c, &h[0], nbp + nv, sizeof(int64_t))) != XT_OK) break;
+    if ((s = d2h(c, &h[1], nwp + nv, sizeof(int64_t))) != XT_OK) break;
+    if ((s = d2h(c, &h[2], P + ne, sizeof(int64_t))) != XT_OK) break;
+    if ((s = d2h(c, hs, stats, sizeof(hs))) != XT_OK) break;
     if ((s = cuda_status(c, cudaStreamSynchronize(c->stream), "sync")) != XT_OK) break;
     pl->n_btask = h[0];
     pl->n_wtask = h[1];
@@ -431,28 +600,24 @@ xt_status make_plan(Graph *g) {
     g->max_out_degree = int64_t(hs[1]);
     g->max_in_degree = int64_t(hs[2]);
     g->wedge_work = tail_work;
-    g->stream_work = head_work;
+    g->stream_work = h[2];
     if ((s = dalloc_n(c, &pl->d_bt, size_t(4 * (pl->n_btask > 0 ? pl->n_btask : 1)))) != XT_OK) break;
     if ((s = dalloc_n(c, &pl->d_wt, size_t(pl->n_wtask > 0 ? pl->n_wtask : 1))) != XT_OK) break;
-    k_plan_fill<<<counted(c, grid_for(nv, B, c->sm_count)), B, 0, c->stream>>>(nv, g->d_off, g->d_ioff, P, nbp, nwp, pl->d_bt,
-                                                                   pl->d_wt);
+    k_plan_fill<<<counted(c, grid_for(nv, B, c->sm_count)), B, 0, c->stream>>>(nv, g->d_off, g->d_ioff, P, nbp, nwp,
+                                                                               pl->d_bt, pl->d_wt);
     if ((s = cuda_status(c, cudaGetLastError(), "k_plan_fill")) != XT_OK) break;
-    // persistent grid
-    const size_t sm_bytes = count_smem_bytes(true);
-    if ((s = cuda_status(c, cudaFuncSetAttribute(k_count<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                 int(sm_bytes)),
-                         "attr")) != XT_OK)
-      break;
-    if ((s = cuda_status(c, cudaFuncSetAttribute(k_count<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                 int(count_smem_bytes(false))),
-                         "attr")) != XT_OK)
-      break;
-    int occ = 0;
-    if ((s = cuda_status(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_count<false>, kThreads,
-                                                                            count_smem_bytes(false)),
-                         "occupancy")) != XT_OK)
-      break;
-    pl->grid = c->sm_count * (occ > 0 ? occ : 1);
+    // persistent grids: every CTA that fits on the device at once
+    int occ[2] = {0, 0};
+    for (int pvm = 0; pvm < 2 && s == XT_OK; pvm++) {
+      auto fn = pvm ? k_count<true> : k_count<false>;
+      const size_t bytes = count_smem_bytes(pvm != 0);
+      s = cuda_status(c, cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes)), "attr");
+      if (s == XT_OK)
+        s = cuda_status(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ[pvm], fn, kThreads, bytes), "occ");
+    }
+    if (s != XT_OK) break;
+    pl->grid_global = c->sm_count * (occ[0] > 0 ? occ[0] : 1);
+    pl->grid_pv = c->sm_count * (occ[1] > 0 ? occ[1] : 1);
   } while (0);
   dfree(c, w);
   dfree(c, P);
@@ -471,18 +636,28 @@ xt_status count_graph(Graph *g, int64_t *d_global, int64_t *d_pv) {
   Plan *pl = g->plan;
   XT_CUDA(c, cudaMemsetAsync(pl->d_cursor, 0, 2 * sizeof(unsigned long long), c->stream));
   XT_CUDA(c, cudaMemsetAsync(d_global, 0, sizeof(int64_t), c->stream));
-  if (d_pv) XT_CUDA(c, cudaMemsetAsync(d_pv, 0, sizeof(int64_t) * g->nv, c->stream));
-  if (g->ne == 0) return XT_OK;
+  int64_t *pv_int = nullptr;  // per-vertex counts in internal numbering
+  if (d_pv) {
+    if (g->d_perm) XT_TRY(dalloc_n(c, &pv_int, size_t(g->nv)));
+    else pv_int = d_pv;
+    XT_CUDA(c, cudaMemsetAsync(pv_int, 0, sizeof(int64_t) * g->nv, c->stream));
+  }
   unsigned long long *gl = reinterpret_cast<unsigned long long *>(d_global);
-  if (d_pv)
-    k_count<true><<<counted(c, pl->grid), kThreads, count_smem_bytes(true), c->stream>>>(
-        g->d_off, g->d_col, g->d_ioff, g->d_icol, pl->d_bt, pl->n_btask, pl->d_wt, pl->n_wtask, pl->d_cursor, gl,
-        d_pv);
-  else
-    k_count<false><<<counted(c, pl->grid), kThreads, count_smem_bytes(false), c->stream>>>(
-        g->d_off, g->d_col, g->d_ioff, g->d_icol, pl->d_bt, pl->n_btask, pl->d_wt, pl->n_wtask, pl->d_cursor, gl,
-        nullptr);
-  XT_CUDA(c, cudaGetLastError());
+  if (g->ne > 0) {
+    if (d_pv)
+      k_count<true><<<counted(c, pl->grid_pv), kThreads, count_smem_bytes(true), c->stream>>>(
+          g->d_off, g->d_col, g->d_ioff, g->d_irec, pl->d_bt, pl->n_btask, pl->d_wt, pl->n_wtask, pl->d_cursor, gl,
+          pv_int);
+    else
+      k_count<false><<<counted(c, pl->grid_global), kThreads, count_smem_bytes(false), c->stream>>>(
+          g->d_off, g->d_col, g->d_ioff, g->d_irec, pl->d_bt, pl->n_btask, pl->d_wt, pl->n_wtask, pl->d_cursor, gl,
+          nullptr);
+  }
+  if (d_pv && g->d_perm)
+    k_unpermute<<<counted(c, grid_for(g->nv, 256, c->sm_count)), 256, 0, c->stream>>>(pv_int, g->d_perm, g->nv, d_pv);
+  cudaError_t e = cudaGetLastError();
+  if (pv_int && pv_int != d_pv) dfree(c, pv_int);
+  XT_CUDA(c, e);
   return XT_OK;
 }
 

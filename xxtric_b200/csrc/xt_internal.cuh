@@ -11,6 +11,8 @@
 namespace xt {
 
 constexpr int kWarp = 32;
+// int32 column arrays carry this many spare entries past their end
+constexpr size_t kColPad = 8;
 
 // ---- context ---------------------------------------------------------------
 struct Ctx {
@@ -60,17 +62,31 @@ xt_status set_error(Ctx *c, xt_status s, const std::string &msg);
 // ---- oriented graph on the device ------------------------------------------
 struct Plan;  // degree-binned schedule, built once per graph
 
+// In-record of edge u->v, stored with the head v: the columns of N+(u) that
+// rank above v, i.e. the suffix d_col[s, s+len) after v's own position.
+// Every triangle (u,v,w) has its w in exactly this suffix and in N+(v).
+struct __align__(16) InRec {
+  int64_t s;
+  int32_t len;
+  int32_t u;
+};
+
 struct Graph {
   Ctx *ctx = nullptr;
   int64_t nv = 0;
   int64_t n_input = 0;
   int64_t ne = 0;  // |E+|
   int orient = XT_ORIENT_DEGREE;
+  // Vertices are renumbered so that the orientation rank IS the id: under
+  // XT_ORIENT_DEGREE, internal id = position in (degree, input id) order;
+  // under XT_ORIENT_ID the numbering is the input's. Every edge then points
+  // from the lower to the higher internal id and rows ascend by rank.
   int64_t *d_off = nullptr;   // out-CSR offsets, nv+1
-  int32_t *d_col = nullptr;   // out-CSR columns N+(u), ne, rows ascending
-  int64_t *d_ioff = nullptr;  // in-CSR offsets, nv+1
-  int32_t *d_icol = nullptr;  // in-CSR columns N-(v), ne, rows ascending
-  int32_t *d_deg = nullptr;   // undirected degree, nv
+  int32_t *d_col = nullptr;   // out-CSR columns N+(u), ne (+kColPad), rows ascending
+  int64_t *d_ioff = nullptr;  // in-record offsets per head v, nv+1
+  InRec *d_irec = nullptr;    // one record per edge u->v, grouped by v
+  int32_t *d_deg = nullptr;   // undirected degree, input ids, nv
+  int32_t *d_perm = nullptr;  // internal id -> input id (null when identity)
   int64_t max_degree = 0;
   int64_t max_out_degree = 0;
   int64_t max_in_degree = 0;
