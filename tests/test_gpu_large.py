@@ -65,6 +65,7 @@ def test_scale24_properties(ctx):
     # relabel every vertex by a random permutation: same total, permuted counts
     perm = torch.randperm(n, device="cuda", dtype=torch.int64).to(torch.int32)
     ps, pd = perm[s.long()], perm[d.long()]
+    torch.cuda.synchronize()  # produced on torch's stream, read on the library's
     g2 = ctx.graph_from_device_edges(n, len(s), ps, pd, xt.ORIENT_DEGREE)
     t2, pv2 = g2.count(per_vertex=True)
     g2.free()

@@ -27,14 +27,36 @@
 
 namespace xt {
 
-constexpr int kThreads = 256;
+// Tuning constants (compile-time; the XT_* macros let a build override them)
+#ifndef XT_THREADS
+#define XT_THREADS 256
+#endif
+#ifndef XT_BLOCK_WORK_LOG2
+#define XT_BLOCK_WORK_LOG2 20
+#endif
+#ifndef XT_WARP_WORK
+#define XT_WARP_WORK 4096
+#endif
+constexpr int kThreads = XT_THREADS;
 constexpr int kWarps = kThreads / 32;
+#ifndef XT_MIN_BLOCKS
+#define XT_MIN_BLOCKS (1024 / XT_THREADS)
+#endif
+constexpr int kMinBlocks = XT_MIN_BLOCKS;  // CTAs per SM the register budget is sized for
 constexpr int kWarpDmax = 64;
 constexpr int kWarpWords = 256;   // per-warp region: 256-slot hash or 8192-bit bitmap
-constexpr int64_t kWarpWork = 4096;
+constexpr int64_t kWarpWork = XT_WARP_WORK;
 constexpr int kBlockDmax = 2048;
 constexpr int kBlockWords = 8192;  // CTA region: 8192-slot hash or 2^18-bit bitmap
-constexpr int64_t kBlockWork = 1 << 18;
+constexpr int64_t kBlockWorkMin = int64_t(1) << 14;
+constexpr int64_t kBlockWorkMax = int64_t(1) << XT_BLOCK_WORK_LOG2;
+
+// Run-time schedule thresholds (the binning of make_plan).
+struct PlanParams {
+  int64_t warp_work;   // a head with d+(v) <= warp_dmax and at most this much work is a warp task
+  int64_t block_work;  // items per CTA task
+  int32_t warp_dmax;
+};
 constexpr int32_t kEmpty = -1;
 
 struct Plan {
@@ -44,6 +66,7 @@ struct Plan {
   int32_t *d_wt = nullptr;    // v per warp task
   unsigned long long *d_cursor = nullptr;  // [0] CTA cursor, [1] warp cursor
   int grid_global = 0, grid_pv = 0;
+  int64_t block_work = 0, warp_work = 0;   // the thresholds the plan was made with
 };
 
 static unsigned grid_for(int64_t n, int block, int sm_count) {
@@ -73,28 +96,28 @@ __global__ void k_outedge_work(const int32_t *__restrict__ col, int64_t ne, cons
 }
 
 __device__ __forceinline__ void classify(int64_t v, const int64_t *__restrict__ off, const int64_t *__restrict__ ioff,
-                                         const int64_t *__restrict__ P, int64_t &nb, int64_t &nw, int64_t &parts,
-                                         int64_t &chunks, int64_t &work) {
+                                         const int64_t *__restrict__ P, const PlanParams pp, int64_t &nb,
+                                         int64_t &nw, int64_t &parts, int64_t &chunks, int64_t &work) {
   const int64_t dp = off[v + 1] - off[v];
   const int64_t k0 = ioff[v], k1 = ioff[v + 1];
   nb = nw = parts = chunks = 0;
   work = P[k1] - P[k0];
   if (dp == 0 || work == 0) return;
-  if (dp <= kWarpDmax && work <= kWarpWork) {
+  if (dp <= pp.warp_dmax && work <= pp.warp_work) {
     nw = 1;
     return;
   }
   parts = (dp + kBlockDmax - 1) / kBlockDmax;
-  chunks = (work + kBlockWork - 1) / kBlockWork;
+  chunks = (work + pp.block_work - 1) / pp.block_work;
   nb = parts * chunks;
 }
 
 __global__ void k_plan_count(int64_t nv, const int64_t *__restrict__ off, const int64_t *__restrict__ ioff,
-                             const int64_t *__restrict__ P, int64_t *__restrict__ nb_out,
+                             const int64_t *__restrict__ P, const PlanParams pp, int64_t *__restrict__ nb_out,
                              int64_t *__restrict__ nw_out) {
   XT_GRID_STRIDE(v, nv) {
     int64_t nb, nw, parts, chunks, work;
-    classify(v, off, ioff, P, nb, nw, parts, chunks, work);
+    classify(v, off, ioff, P, pp, nb, nw, parts, chunks, work);
     nb_out[v] = nb;
     nw_out[v] = nw;
   }
@@ -111,11 +134,11 @@ __device__ __forceinline__ int64_t lower_bound_i64(const int64_t *__restrict__ P
 }
 
 __global__ void k_plan_fill(int64_t nv, const int64_t *__restrict__ off, const int64_t *__restrict__ ioff,
-                            const int64_t *__restrict__ P, const int64_t *__restrict__ nb_pos,
+                            const int64_t *__restrict__ P, const PlanParams pp, const int64_t *__restrict__ nb_pos,
                             const int64_t *__restrict__ nw_pos, int64_t *__restrict__ bt, int32_t *__restrict__ wt) {
   XT_GRID_STRIDE(v, nv) {
     int64_t nb, nw, parts, chunks, work;
-    classify(v, off, ioff, P, nb, nw, parts, chunks, work);
+    classify(v, off, ioff, P, pp, nb, nw, parts, chunks, work);
     if (nw) wt[nw_pos[v]] = int32_t(v);
     if (!nb) continue;
     const int64_t k0 = ioff[v], k1 = ioff[v + 1], base = P[k0];
@@ -209,14 +232,44 @@ __device__ __forceinline__ void members_insert(const Members &m, int32_t x) {
 
 // ---- streaming the in-record suffixes ----------------------------------------
 
-// A warp step: 32 aligned 16-byte groups (one LDG.128 per lane) of one suffix.
+// A warp step: kStepGroups x 32 aligned 16-byte groups (kStepGroups LDG.128
+// per lane) taken from the flattened groups of a batch of suffixes, so a
+// step spans as many suffixes as it needs and every lane has groups while
+// the batch lasts.
+#ifndef XT_STEP_GROUPS
+#define XT_STEP_GROUPS 2
+#endif
+constexpr int kStepGroups = XT_STEP_GROUPS;
+
 struct Chunk {
-  int4 x;          // four columns of this lane's group
-  int64_t grp;     // group index (columns 4*grp .. 4*grp+3)
-  int64_t s, e;    // the suffix [s, e)
-  int32_t u;       // its owner (per-vertex credit)
-  int32_t serial;  // which suffix of the walk (warp-uniform)
-  bool exists;     // warp-uniform: this step exists
+  int4 x[kStepGroups];     // four columns per group
+  uint32_t vm[kStepGroups];  // which of the four are inside the suffix (bit i: column i)
+  int32_t rj[kStepGroups];   // the suffix's slot in the batch (per-vertex credit)
+  bool exists;               // warp-uniform: this step exists
+};
+
+// bits i in [0,4) with pos + i in [lo, hi), where lo - pos <= 3 whenever
+// lo > pos (a suffix starts inside its first group)
+__device__ __forceinline__ uint32_t valid_mask(uint32_t pos, uint32_t lo, uint32_t hi) {
+  const uint32_t a = lo > pos ? lo - pos : 0u;
+  uint32_t b = hi > pos ? hi - pos : 0u;
+  b = b > 4u ? 4u : b;
+  return ((1u << b) - 1u) & ~((1u << a) - 1u);
+}
+
+// Per-warp shared-memory view of the current batch.
+// Flattened positions are 4 x flattened group + column in group; a batch
+// holds at most 32 suffixes of fewer than kMaxOutDegree columns each, so
+// positions fit in 32 bits.
+constexpr int64_t kMaxOutDegree = int64_t(1) << 27;
+
+struct BatchView {
+  uint32_t start[33];  // first flattened group of each suffix; start[32] = total
+  int64_t gbase[32];   // first global group index of each suffix, minus its start
+  uint32_t lopos[32];  // the suffix's first flattened position
+  uint32_t hipos[32];  // one past its last
+  int32_t u[32];       // the suffix's owner
+  int32_t hits[32];    // per-vertex mode: hits per suffix in this batch
 };
 
 // One warp's walk over the in-records rec[k0, kend), taken in batches of bsz
@@ -224,119 +277,152 @@ struct Chunk {
 // another (a warp task), or from a cursor in shared memory that the warps of
 // a CTA task share, so warps that finish early take more. The next batch is
 // claimed and its records loaded while the current one streams.
-// Control flow is warp-uniform.
-struct RecWalk {
-  const InRec *__restrict__ rec;
+template <bool PV>
+struct FlatWalk {
+  const InRec *__restrict__ rec;  // the task's records: rec[0, kend)
   const int32_t *__restrict__ col;
-  int *cursor;              // shared batch cursor (CTA task) or null
-  int64_t k0, kend;         // the task's records
-  int64_t kb, nkb, seq;     // current / next batch base, next sequential base
-  int bsz, nb, j;
-  int64_t bs, be;           // lane's record of this batch
-  int32_t bu;
-  int4 nrec;                // lane's record of the next batch (prefetched)
-  int64_t cs, ce, g, gend;  // current suffix and group cursor
-  int32_t cu, serial;
+  int64_t *__restrict__ pv;
+  BatchView *bv;
+  int *cursor;                // shared batch cursor (CTA task) or null
+  int32_t kend;               // records in the task
+  int32_t kb, nkb, seq;       // current / next batch base, next sequential base
+  int bsz, nb;
+  int4 nrec;                  // lane's record of the next batch (prefetched)
+  uint32_t total, F;          // groups in the batch, next step's first group (uniform)
+  int r;                      // this lane's suffix cursor (monotone within a batch)
+  // this lane's copy of suffix r's layout: flattened groups end at c_end,
+  // global group = flattened + c_gb, valid flattened positions [c_lo, c_hi)
+  uint32_t c_end, c_lo, c_hi;
+  int64_t c_gb;
   bool have;
   int lane;
 
-  __device__ __forceinline__ int64_t claim() {
+  __device__ __forceinline__ void load_suffix() {
+    c_end = bv->start[r + 1];
+    c_gb = bv->gbase[r];
+    c_lo = bv->lopos[r];
+    c_hi = bv->hipos[r];
+  }
+
+  __device__ __forceinline__ int32_t claim() {
     if (!cursor) {
-      const int64_t b = seq;
+      const int32_t b = seq;
       seq += bsz;
       return b;
     }
-    int r = 0;
-    if (lane == 0) r = atomicAdd(cursor, bsz);
-    return k0 + __shfl_sync(0xffffffffu, r, 0);
+    int c = 0;
+    if (lane == 0) c = atomicAdd(cursor, bsz);
+    return __shfl_sync(0xffffffffu, c, 0);
   }
-  __device__ __forceinline__ int4 fetch(int64_t base) const {
-    const int64_t k = base + lane;
+  __device__ __forceinline__ int4 fetch(int32_t base) const {
+    const int32_t k = base + lane;
     return (lane < bsz && k < kend) ? __ldg(reinterpret_cast<const int4 *>(rec) + k) : make_int4(0, 0, 0, -1);
   }
-  __device__ __forceinline__ void take(int4 r) {
-    bs = int64_t(uint32_t(r.x)) | (int64_t(r.y) << 32);
-    be = bs + r.z;
-    bu = r.w;
-    nb = (kend - kb < bsz) ? int(kend - kb) : bsz;
+  // per-vertex mode: credit the finished batch's suffix owners
+  __device__ __forceinline__ void flush() {
+    if (PV && nb > 0) {
+      __syncwarp();
+      if (lane < nb && bv->hits[lane])
+        atomicAdd(reinterpret_cast<unsigned long long *>(&pv[bv->u[lane]]), (unsigned long long)bv->hits[lane]);
+    }
+  }
+  // lays the batch whose records are in lane registers r4 out in shared memory
+  __device__ __forceinline__ void take(int4 r4) {
+    flush();
+    const int64_t s = int64_t(uint32_t(r4.x)) | (int64_t(r4.y) << 32);
+    const uint32_t len = uint32_t(r4.z);
+    const int64_t g0 = s >> 2;
+    const uint32_t ng = (len > 0) ? uint32_t(((s + len + 3) >> 2) - g0) : 0u;
+    uint32_t incl = ng;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += t;
+    }
+    total = __shfl_sync(0xffffffffu, incl, 31);
+    __syncwarp();  // every lane is done reading the previous batch
+    const uint32_t st = incl - ng;
+    bv->start[lane] = st;
+    if (lane == 31) bv->start[32] = incl;
+    bv->gbase[lane] = g0 - int64_t(st);
+    bv->lopos[lane] = 4u * st + uint32_t(s & 3);
+    bv->hipos[lane] = 4u * st + uint32_t(s & 3) + len;
+    if (PV) {
+      bv->u[lane] = r4.w;
+      bv->hits[lane] = 0;
+    }
+    __syncwarp();
+    nb = (kend - kb < bsz) ? (kend - kb) : bsz;
+    F = 0;
+    r = 0;
+    load_suffix();
     nkb = claim();
     nrec = fetch(nkb);
   }
-  __device__ __forceinline__ void select(int jj) {
-    j = jj;
-    cs = __shfl_sync(0xffffffffu, bs, jj);
-    ce = __shfl_sync(0xffffffffu, be, jj);
-    cu = __shfl_sync(0xffffffffu, bu, jj);
-    g = cs >> 2;
-    gend = (ce + 3) >> 2;
-    if (cs == ce) gend = g;  // empty suffix
-    serial++;
-  }
   __device__ __forceinline__ void init() {
-    nb = j = 0;
-    bs = be = cs = ce = g = gend = 0;
-    bu = cu = -1;
-    serial = 0;
-    seq = k0;
+    nb = 0;
+    seq = 0;
     kb = claim();
     have = kb < kend;
-    if (!have) return;
-    take(fetch(kb));
-    select(0);
-  }
-  __device__ __forceinline__ void advance() {
-    while (have && g >= gend) {
-      if (j + 1 < nb) {
-        select(j + 1);
-      } else {
-        kb = nkb;
-        if (kb >= kend) {
-          have = false;
-          break;
-        }
-        take(nrec);
-        select(0);
-      }
-    }
+    if (have) take(fetch(kb));
   }
   __device__ __forceinline__ Chunk issue() {
     Chunk c;
-    advance();
-    c.exists = have;
-    c.grp = g + lane;
-    c.s = cs;
-    c.e = ce;
-    c.u = cu;
-    c.serial = serial;
-    c.x = make_int4(0, 0, 0, 0);
-    if (have) {
-      if (c.grp < gend) c.x = __ldg(reinterpret_cast<const int4 *>(col) + c.grp);
-      g += 32;
+    while (have && F >= total) {  // batch exhausted: move to the next one
+      kb = nkb;
+      if (kb >= kend) {
+        flush();
+        have = false;
+        break;
+      }
+      take(nrec);
     }
+    c.exists = have;
+#pragma unroll
+    for (int q = 0; q < kStepGroups; q++) {
+      c.x[q] = make_int4(0, 0, 0, 0);
+      c.vm[q] = 0;  // lanes past the batch probe nothing
+      c.rj[q] = 0;
+    }
+    if (!have) return c;
+    // this lane's kStepGroups consecutive groups: usually one suffix, so the
+    // layout read from shared memory is reused from the previous group
+#pragma unroll
+    for (int q = 0; q < kStepGroups; q++) {
+      const uint32_t f = F + uint32_t(kStepGroups * lane + q);
+      if (f < total) {
+        if (f >= c_end) {
+          do r++;
+          while (bv->start[r + 1] <= f);
+          load_suffix();
+        }
+        c.x[q] = __ldg(reinterpret_cast<const int4 *>(col) + (int64_t(f) + c_gb));
+        c.vm[q] = valid_mask(4u * f, c_lo, c_hi);
+        c.rj[q] = r;
+      }
+    }
+    F += 32 * kStepGroups;
     return c;
   }
 };
 
-// Probes a chunk; returns this lane's hits and sets `past` when none of the
-// lane's valid columns is <= m.hi (so the rest of the suffix is past it).
-template <bool PV>
-__device__ __forceinline__ int probe_chunk(const Chunk &c, const Members &m, bool &past) {
+// Probes one group; returns the hits. A candidate outside
+// [min N+(v), max N+(v)] is rejected by one unsigned compare.
+template <bool PV, bool BITMAP>
+__device__ __forceinline__ int probe_group(int4 x4, uint32_t vm, const Members &m) {
   int h = 0;
-  past = true;
-  const int64_t p0 = 4 * c.grp;
-  const int32_t w[4] = {c.x.x, c.x.y, c.x.z, c.x.w};
+  const int32_t w[4] = {x4.x, x4.y, x4.z, x4.w};
+  const uint32_t span = uint32_t(m.hi - m.lo);
 #pragma unroll
   for (int i = 0; i < 4; i++) {
-    const int64_t p = p0 + i;
-    if (p < c.s || p >= c.e) continue;
-    const int32_t x = w[i];
-    if (x <= m.hi) past = false;
-    if (x < m.lo || x > m.hi) continue;
-    if (m.bitmap) {
-      const uint32_t d = uint32_t(x - m.lo);
-      h += (m.words[d >> 5] >> (d & 31)) & 1;
-    } else {
-      const int slot = hash_find(m.words, m.mask, m.shift, x);
+    const uint32_t d = uint32_t(w[i] - m.lo);
+    const bool ok = ((vm >> i) & 1u) && d <= span;
+    if (BITMAP) {
+      // branch-free: an invalid candidate reads word 0 and is masked out
+      const uint32_t word = uint32_t(m.words[ok ? (d >> 5) : 0u]);
+      h += int((word >> (d & 31)) & uint32_t(ok));
+    } else if (ok) {
+      const int slot = hash_find(m.words, m.mask, m.shift, w[i]);
       if (slot >= 0) {
         h++;
         if (PV) atomicAdd(&m.cnt[slot], 1);
@@ -349,46 +435,59 @@ __device__ __forceinline__ int probe_chunk(const Chunk &c, const Members &m, boo
 // Streams the suffixes of in-records [k0, kend) in batches of bsz records
 // (claimed from `cursor` when it is not null) through the member set;
 // returns this lane's hit count.
-template <bool PV>
-__device__ __forceinline__ int64_t stream_suffixes(const InRec *__restrict__ rec, const int32_t *__restrict__ col,
-                                                   int64_t k0, int64_t kend, int bsz, int *cursor, const Members &m,
-                                                   int64_t *__restrict__ pv, int lane) {
-  RecWalk wk;
-  wk.rec = rec;
+template <bool PV, bool BITMAP>
+__device__ __forceinline__ int64_t stream_kind(const InRec *__restrict__ rec, const int32_t *__restrict__ col,
+                                               int64_t k0, int64_t kend, int bsz, int *cursor, const Members &m,
+                                               BatchView *bv, int64_t *__restrict__ pv, int lane) {
+  FlatWalk<PV> wk;
+  wk.rec = rec + k0;
   wk.col = col;
+  wk.pv = pv;
+  wk.bv = bv;
   wk.cursor = cursor;
-  wk.k0 = k0;
-  wk.kend = kend;
+  wk.kend = int32_t(kend - k0);
   wk.bsz = bsz;
   wk.lane = lane;
   wk.init();
   int64_t hits = 0;
   Chunk a = wk.issue();
   while (a.exists) {
-    Chunk b = wk.issue();  // the next step's loads are in flight during these probes
-    bool past;
-    const int h = probe_chunk<PV>(a, m, past);
-    hits += h;
+    Chunk b;
     if (PV) {
-      int tot = h;
-      for (int o = 16; o; o >>= 1) tot += __shfl_xor_sync(0xffffffffu, tot, o);
-      if (lane == 0 && tot) atomicAdd(reinterpret_cast<unsigned long long *>(&pv[a.u]), (unsigned long long)tot);
-    }
-    if (__all_sync(0xffffffffu, past) && b.exists && b.serial == a.serial) {
-      // the suffix is sorted: every later column is above max N+(v) too, so
-      // drop the step already in flight and the rest of this suffix
-      wk.g = wk.gend;
+      // credit a's suffixes before the next issue may lay a new batch (and
+      // flush the credits) over their slots
+#pragma unroll
+      for (int q = 0; q < kStepGroups; q++) {
+        const int h = probe_group<PV, BITMAP>(a.x[q], a.vm[q], m);
+        if (h) atomicAdd(&bv->hits[a.rj[q]], h);
+        hits += h;
+      }
       b = wk.issue();
+    } else {
+      b = wk.issue();  // the next step's loads are in flight during these probes
+      int h = 0;
+#pragma unroll
+      for (int q = 0; q < kStepGroups; q++) h += probe_group<PV, BITMAP>(a.x[q], a.vm[q], m);
+      hits += h;
     }
     a = b;
   }
   return hits;
 }
 
+template <bool PV>
+__device__ __forceinline__ int64_t stream_suffixes(const InRec *__restrict__ rec, const int32_t *__restrict__ col,
+                                                   int64_t k0, int64_t kend, int bsz, int *cursor, const Members &m,
+                                                   BatchView *bv, int64_t *__restrict__ pv, int lane) {
+  // the membership kind is fixed per task: one specialised loop each
+  if (m.bitmap) return stream_kind<PV, true>(rec, col, k0, kend, bsz, cursor, m, bv, pv, lane);
+  return stream_kind<PV, false>(rec, col, k0, kend, bsz, cursor, m, bv, pv, lane);
+}
+
 // ---- the count kernel ---------------------------------------------------------
 
 template <bool PV>
-__global__ void __launch_bounds__(kThreads, 4) k_count(const int64_t *__restrict__ off, const int32_t *__restrict__ col,
+__global__ void __launch_bounds__(kThreads, kMinBlocks) k_count(const int64_t *__restrict__ off, const int32_t *__restrict__ col,
                                                        const int64_t *__restrict__ ioff,
                                                        const InRec *__restrict__ rec, const int64_t *__restrict__ bt,
                                                        int64_t n_bt, const int32_t *__restrict__ wt, int64_t n_wt,
@@ -403,6 +502,7 @@ __global__ void __launch_bounds__(kThreads, 4) k_count(const int64_t *__restrict
   __shared__ int64_t s_task;
   __shared__ int s_batch;  // next in-record batch of the current CTA task
   __shared__ unsigned long long s_red[kWarps];
+  __shared__ BatchView s_bv[kWarps];
 
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   int64_t acc = 0;
@@ -433,7 +533,7 @@ __global__ void __launch_bounds__(kThreads, 4) k_count(const int64_t *__restrict
     // batches small enough that every warp gets several of them
     int64_t bsz = (k1 - k0) / (4 * kWarps);
     bsz = bsz < 1 ? 1 : (bsz > 32 ? 32 : bsz);
-    int64_t h = stream_suffixes<PV>(rec, col, k0, k1, int(bsz), &s_batch, m, pv, lane);
+    int64_t h = stream_suffixes<PV>(rec, col, k0, k1, int(bsz), &s_batch, m, &s_bv[warp], pv, lane);
     acc += h;
     if (PV) {
       for (int o = 16; o; o >>= 1) h += __shfl_xor_sync(0xffffffffu, h, o);
@@ -473,7 +573,7 @@ __global__ void __launch_bounds__(kThreads, 4) k_count(const int64_t *__restrict
     __syncwarp();
     for (int64_t p = r0 + lane; p < r1; p += 32) members_insert(m, col[p]);
     __syncwarp();
-    int64_t h = stream_suffixes<PV>(rec, col, ioff[v], ioff[v + 1], 32, nullptr, m, pv, lane);
+    int64_t h = stream_suffixes<PV>(rec, col, ioff[v], ioff[v + 1], 32, nullptr, m, &s_bv[warp], pv, lane);
     acc += h;
     if (PV) {
       for (int o = 16; o; o >>= 1) h += __shfl_xor_sync(0xffffffffu, h, o);
@@ -578,11 +678,40 @@ xt_status make_plan(Graph *g) {
     // suffix lengths, prefix-summed in head order
     k_inrec_work<<<counted(c, grid_for(ne, B, c->sm_count)), B, 0, c->stream>>>(g->d_irec, ne, w);
     if ((s = exclusive_scan(c, w, P, ne + 1)) != XT_OK) break;
+    // persistent grids: every CTA that fits on the device at once
+    int occ[2] = {0, 0};
+    for (int pvm = 0; pvm < 2 && s == XT_OK; pvm++) {
+      auto fn = pvm ? k_count<true> : k_count<false>;
+      const size_t bytes = count_smem_bytes(pvm != 0);
+      s = cuda_status(c, cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes)), "attr");
+      if (s == XT_OK)
+        s = cuda_status(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ[pvm], fn, kThreads, bytes), "occ");
+    }
+    if (s != XT_OK) break;
+    pl->grid_global = c->sm_count * (occ[0] > 0 ? occ[0] : 1);
+    pl->grid_pv = c->sm_count * (occ[1] > 0 ? occ[1] : 1);
+    // CTA task size: large tasks amortise the member-set build and the task
+    // barrier, but every CTA should still get about 16 of them
+    int64_t total_work = 0;
+    if ((s = d2h(c, &total_work, P + ne, sizeof(int64_t))) != XT_OK) break;
+    if ((s = cuda_status(c, cudaStreamSynchronize(c->stream), "sync")) != XT_OK) break;
+    PlanParams pp;
+    pp.warp_dmax = kWarpDmax;
+    pp.warp_work = g->tune_warp_work > 0 ? g->tune_warp_work : kWarpWork;
+    if (g->tune_block_work > 0) {
+      pp.block_work = g->tune_block_work;
+    } else {
+      pp.block_work = kBlockWorkMin;
+      while (pp.block_work < kBlockWorkMax && pp.block_work * 16 * pl->grid_global < total_work) pp.block_work *= 2;
+    }
+    pl->block_work = pp.block_work;
+    pl->warp_work = pp.warp_work;
     if ((s = dalloc_n(c, &nb, size_t(nv + 1))) != XT_OK) break;
     if ((s = dalloc_n(c, &nw, size_t(nv + 1))) != XT_OK) break;
     if ((s = dalloc_n(c, &nbp, size_t(nv + 1))) != XT_OK) break;
     if ((s = dalloc_n(c, &nwp, size_t(nv + 1))) != XT_OK) break;
-    k_plan_count<<<counted(c, grid_for(nv, B, c->sm_count)), B, 0, c->stream>>>(nv, g->d_off, g->d_ioff, P, nb, nw);
+    k_plan_count<<<counted(c, grid_for(nv, B, c->sm_count)), B, 0, c->stream>>>(nv, g->d_off, g->d_ioff, P, pp, nb,
+                                                                                nw);
     if ((s = cuda_status(c, cudaMemsetAsync(nb + nv, 0, sizeof(int64_t), c->stream), "memset")) != XT_OK) break;
     if ((s = cuda_status(c, cudaMemsetAsync(nw + nv, 0, sizeof(int64_t), c->stream), "memset")) != XT_OK) break;
     if ((s = exclusive_scan(c, nb, nbp, nv + 1)) != XT_OK) break;
@@ -601,23 +730,15 @@ xt_status make_plan(Graph *g) {
     g->max_in_degree = int64_t(hs[2]);
     g->wedge_work = tail_work;
     g->stream_work = h[2];
+    if (g->max_out_degree >= kMaxOutDegree) {
+      s = set_error(c, XT_ERR_OVERFLOW, "an oriented out-degree of 2^27 or more is not supported");
+      break;
+    }
     if ((s = dalloc_n(c, &pl->d_bt, size_t(4 * (pl->n_btask > 0 ? pl->n_btask : 1)))) != XT_OK) break;
     if ((s = dalloc_n(c, &pl->d_wt, size_t(pl->n_wtask > 0 ? pl->n_wtask : 1))) != XT_OK) break;
-    k_plan_fill<<<counted(c, grid_for(nv, B, c->sm_count)), B, 0, c->stream>>>(nv, g->d_off, g->d_ioff, P, nbp, nwp,
-                                                                               pl->d_bt, pl->d_wt);
+    k_plan_fill<<<counted(c, grid_for(nv, B, c->sm_count)), B, 0, c->stream>>>(nv, g->d_off, g->d_ioff, P, pp, nbp,
+                                                                               nwp, pl->d_bt, pl->d_wt);
     if ((s = cuda_status(c, cudaGetLastError(), "k_plan_fill")) != XT_OK) break;
-    // persistent grids: every CTA that fits on the device at once
-    int occ[2] = {0, 0};
-    for (int pvm = 0; pvm < 2 && s == XT_OK; pvm++) {
-      auto fn = pvm ? k_count<true> : k_count<false>;
-      const size_t bytes = count_smem_bytes(pvm != 0);
-      s = cuda_status(c, cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes)), "attr");
-      if (s == XT_OK)
-        s = cuda_status(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ[pvm], fn, kThreads, bytes), "occ");
-    }
-    if (s != XT_OK) break;
-    pl->grid_global = c->sm_count * (occ[0] > 0 ? occ[0] : 1);
-    pl->grid_pv = c->sm_count * (occ[1] > 0 ? occ[1] : 1);
   } while (0);
   dfree(c, w);
   dfree(c, P);

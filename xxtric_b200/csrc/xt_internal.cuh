@@ -90,6 +90,8 @@ struct Graph {
   int64_t max_degree = 0;
   int64_t max_out_degree = 0;
   int64_t max_in_degree = 0;
+  int64_t tune_block_work = 0;  // schedule overrides (0: choose automatically)
+  int64_t tune_warp_work = 0;
   int64_t wedge_work = 0;   // sum over oriented (u,v) of d+(v)
   int64_t stream_work = 0;  // sum over oriented (u,v) of d+(u) = sum_u d+(u)^2
   Plan *plan = nullptr;
