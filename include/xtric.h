@@ -130,6 +130,21 @@ xt_status xt_count_async(xt_graph *g, int64_t *d_global, int64_t *d_per_vertex);
 xt_status xt_count_device(int64_t nv, const int64_t *d_indices, const int64_t *d_edge_list, int64_t *d_count,
                           int accumulate, void *cuda_stream);
 
+/* No counterpart in the reference. The count of the same device CSR as
+ * xt_count_device (int64 offsets, int64 tails; rows sorted, deduped,
+ * symmetric), for callers that cannot allocate device memory while they run:
+ * it calls no cudaMalloc, cudaFree or other allocating routine. Its scratch is
+ * one fixed 64 MiB array inside the library, present on every GPU that loads
+ * the library until the process exits; it holds 8 bytes per vertex, so
+ * nv must not exceed 8,389,088 (else XT_ERR_OVERFLOW). The first call on a
+ * device sets up the array's address (make it before any stream capture).
+ * Calls that overlap on one device race on the shared array: serialise them.
+ * Orientation is by vertex id. Overwrites *d_count, or adds to it when
+ * accumulate != 0; XT_ERR_INVALID when a row lacks a back edge (input not
+ * symmetric). Synchronises the given stream before returning. */
+xt_status xt_count_device_static(int64_t nv, const int64_t *d_indices, const int64_t *d_edge_list,
+                                 int64_t *d_count, int accumulate, void *cuda_stream);
+
 /* ---- synthetic inputs on the device --------------------------------------
  * Deterministic counter-based generators (same bits for the same seed on any
  * GPU and in the CPU oracle). Outputs are device int32 arrays of ne rows. */

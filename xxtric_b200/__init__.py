@@ -81,6 +81,7 @@ _proto("xt_graph_free", _int, _vp)
 _proto("xt_count", _int, _vp, _vp, _vp)
 _proto("xt_count_async", _int, _vp, _vp, _vp)
 _proto("xt_count_device", _int, _i64, _vp, _vp, _vp, _int, _vp)
+_proto("xt_count_device_static", _int, _i64, _vp, _vp, _vp, _int, _vp)
 _proto("xt_gen_rmat", _int, _vp, _int, _i64, _u64, _int, _int, _int, _int, _int, _vp, _vp)
 _proto("xt_gen_chunglu", _int, _vp, _i64, _vp, _i64, _u64, _int, _vp, _vp)
 _proto("xt_chunglu_cdf", _i64, _i64, _dbl, _dbl, _dbl, _vp)
@@ -93,6 +94,7 @@ EXPORTED = ["xt_strerror", "xt_last_error", "xt_open", "xt_close", "xt_set_strea
             "xt_launch_count", "xt_synchronize", "xt_graph_get_perm",
             "xt_graph_from_csr", "xt_graph_from_edges", "xt_graph_from_device_edges", "xt_graph_get_info",
             "xt_graph_get_csr", "xt_graph_free", "xt_count", "xt_count_async", "xt_count_device",
+            "xt_count_device_static",
             "xt_gen_rmat", "xt_gen_chunglu", "xt_chunglu_cdf", "xt_gen_er", "xt_vite_read", "xt_vite_write",
             "xt_rgg_generate"]
 
@@ -322,6 +324,15 @@ def count_device(nv: int, d_indices, d_edge_list, d_count, accumulate: bool = Fa
     """single_gpu_count replacement on the reference's device CSR layout (int64 offsets and tails)."""
     s = _L.xt_count_device(nv, _ptr(d_indices), _ptr(d_edge_list), _ptr(d_count), int(accumulate), stream)
     _check(s, "xt_count_device")
+
+
+def count_device_static(nv: int, d_indices, d_edge_list, d_count, accumulate: bool = False,
+                        stream: int = 0) -> None:
+    """Like count_device, for callers that must not allocate device memory: all
+    scratch lives in a fixed array inside the library (8 bytes per vertex, at
+    most 8,389,088 vertices); calls on one device must not overlap."""
+    s = _L.xt_count_device_static(nv, _ptr(d_indices), _ptr(d_edge_list), _ptr(d_count), int(accumulate), stream)
+    _check(s, "xt_count_device_static")
 
 
 class TriangleCountingSingle:

@@ -24,7 +24,7 @@ BUILD = os.path.join(ROOT, "_build")
 LIB = os.path.join(PKG, "libxtb200.so")
 CLI = os.path.join(PKG, "xtric")
 
-CUDA_SOURCES = ["csrc/capi.cu", "csrc/build.cu", "csrc/count.cu", "csrc/gen.cu"]
+CUDA_SOURCES = ["csrc/capi.cu", "csrc/build.cu", "csrc/count.cu", "csrc/gen.cu", "csrc/count_static.cu"]
 HOST_SOURCES = ["host/host_io.cpp"]
 CLI_SOURCES = ["host/xtric_main.cpp"]
 HEADERS = ["csrc/xt_internal.cuh", "../include/xtric.h", "host/xtric_host.hpp"]
