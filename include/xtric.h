@@ -145,6 +145,53 @@ xt_status xt_count_device(int64_t nv, const int64_t *d_indices, const int64_t *d
 xt_status xt_count_device_static(int64_t nv, const int64_t *d_indices, const int64_t *d_edge_list,
                                  int64_t *d_count, int accumulate, void *cuda_stream);
 
+/* ---- batching form ---------------------------------------------------------
+ * No counterpart in the reference, which counts one graph per run. Many
+ * independent graphs become one graph object: graph g has the vertices
+ * [vertex_offsets[g], vertex_offsets[g+1]) and the edge rows
+ * [edge_offsets[g], edge_offsets[g+1]) of src/dst, whose ids are LOCAL to
+ * their graph (0 .. n_g - 1). One build serves all graphs and one count
+ * launch covers them all; xt_count_groups returns every graph's own count,
+ * identical to counting that graph alone. */
+xt_status xt_graph_from_batch(xt_ctx *ctx, int64_t n_graphs, const int64_t *vertex_offsets,
+                              const int64_t *edge_offsets, const int32_t *src, const int32_t *dst, int orient,
+                              xt_graph **out);
+/* the same with src/dst in device memory (offset tables on the host) */
+xt_status xt_graph_from_device_batch(xt_ctx *ctx, int64_t n_graphs, const int64_t *vertex_offsets,
+                                     const int64_t *edge_offsets, const int32_t *d_src, const int32_t *d_dst,
+                                     int orient, xt_graph **out);
+/* graphs in a batch (0 for a single graph) */
+int64_t xt_graph_groups(const xt_graph *g);
+/* total and per-graph counts (host buffer of xt_graph_groups entries, nullable) */
+xt_status xt_count_groups(xt_graph *g, int64_t *total, int64_t *per_group);
+xt_status xt_count_groups_async(xt_graph *g, int64_t *d_total, int64_t *d_per_group);
+/* Capture the graph's count (its memsets and its one persistent launch) into
+ * a CUDA graph once; xt_count_groups then replays it. */
+xt_status xt_graph_capture(xt_graph *g);
+/* Schedule thresholds (0 = automatic): items per CTA task, the work limit of
+ * a warp task, and the largest member id range kept as a bitmap (beyond it a
+ * hash). Re-plans (and re-captures a captured graph). */
+xt_status xt_graph_set_tuning(xt_graph *g, int64_t block_work, int64_t warp_work, int64_t bitmap_bits);
+/* Autotuner: a coordinate search of the three thresholds, timing `reps`
+ * counts each, keeping the fastest; with cache_path it first looks the
+ * (GPU, graph class) key up in that text file and appends new results.
+ * A JSON report of the trials goes to report (nullable). */
+xt_status xt_graph_autotune(xt_graph *g, int reps, const char *cache_path, char *report, int64_t report_len);
+
+/* The batch workload of this repository's benchmarks: for graph i of
+ * n_graphs, kind (0 = unit-square random geometric graph, 1 = Erdos-Renyi
+ * G(n, m)), vertex count (log-uniform in [256, 65536)), mean degree
+ * (log-uniform in [8, 64)) and its own seed, all derived from seed. */
+xt_status xt_batch_spec(int64_t n_graphs, uint64_t seed, int32_t *kind, int64_t *n, double *mean_deg,
+                        uint64_t *graph_seed);
+/* Generates those graphs on the device: local-id edge rows (random geometric:
+ * every pair u < v within distance sqrt(mean_deg / (pi n)); Erdos-Renyi:
+ * round(n mean_deg / 2) uniform pairs), edge_offsets (host, n_graphs + 1)
+ * filled, the arrays allocated by the library (release with xt_device_free). */
+xt_status xt_gen_batch(xt_ctx *ctx, int64_t n_graphs, const int32_t *kind, const int64_t *n, const double *mean_deg,
+                       const uint64_t *graph_seed, int64_t *edge_offsets, int32_t **d_src, int32_t **d_dst);
+xt_status xt_device_free(xt_ctx *ctx, void *p);
+
 /* ---- synthetic inputs on the device --------------------------------------
  * Deterministic counter-based generators (same bits for the same seed on any
  * GPU and in the CPU oracle). Outputs are device int32 arrays of ne rows. */

@@ -53,6 +53,9 @@ def lib() -> ctypes.CDLL:
             ("xo_rgg_edges", c.c_int64, [c.c_int64, c.c_uint64, c.c_double, c.c_int64, _i64p, _i64p]),
             ("xo_ref_rgg", c.c_int64, [c.c_int64, c.c_int, c.c_double, c.c_int64, _i64p, _i64p]),
             ("xo_seed_seq1", c.c_uint32, [c.c_uint32]),
+            ("xo_batch_spec", None, [c.c_int64, c.c_uint64, np.ctypeslib.ndpointer(np.int32, flags="C"), _i64p,
+                                     np.ctypeslib.ndpointer(np.float64, flags="C"), _u64p]),
+            ("xo_batch_graph", c.c_int64, [c.c_int32, c.c_int64, c.c_double, c.c_uint64, c.c_int64, _i64p, _i64p]),
         ]:
             f = getattr(L, name)
             f.restype = res
@@ -131,6 +134,27 @@ def rgg_edges(n: int, seed: int, r2: float):
         src = np.empty(cap, np.int64)
         dst = np.empty(cap, np.int64)
         m = int(lib().xo_rgg_edges(n, seed, r2, cap, src, dst))
+        if m >= 0:
+            return src[:m].copy(), dst[:m].copy()
+        cap = -m
+
+
+def batch_spec(n_graphs: int, seed: int) -> dict:
+    kind = np.zeros(n_graphs, np.int32)
+    n = np.zeros(n_graphs, np.int64)
+    deg = np.zeros(n_graphs, np.float64)
+    gseed = np.zeros(n_graphs, np.uint64)
+    lib().xo_batch_spec(n_graphs, seed, kind, n, deg, gseed)
+    return {"kind": kind, "n": n, "mean_deg": deg, "graph_seed": gseed}
+
+
+def batch_graph(kind: int, n: int, mean_deg: float, gseed: int):
+    """One graph of the batch workload: (src, dst) local ids."""
+    cap = max(1024, int(n * mean_deg))
+    while True:
+        src = np.empty(cap, np.int64)
+        dst = np.empty(cap, np.int64)
+        m = int(lib().xo_batch_graph(int(kind), int(n), float(mean_deg), int(gseed), cap, src, dst))
         if m >= 0:
             return src[:m].copy(), dst[:m].copy()
         cap = -m

@@ -544,3 +544,38 @@ int64_t xo_ref_rgg(int64_t nv, int P, double radius, int64_t cap, int64_t *off, 
   free(E);
   return total;
 }
+
+/* ======================================================================== */
+/* the batch workload (twin of xt_batch_spec / xt_gen_batch)                */
+/* ======================================================================== */
+
+#define XO_STREAM_BATCH 5
+
+void xo_batch_spec(int64_t ng, uint64_t seed, int32_t *kind, int64_t *n, double *mean_deg, uint64_t *gseed) {
+  for (int64_t i = 0; i < ng; i++) {
+    const uint64_t r0 = xo_rand(seed, XO_STREAM_BATCH, 4u * (uint64_t)i);
+    const uint64_t r1 = xo_rand(seed, XO_STREAM_BATCH, 4u * (uint64_t)i + 1u);
+    const uint64_t r2 = xo_rand(seed, XO_STREAM_BATCH, 4u * (uint64_t)i + 2u);
+    const uint64_t r3 = xo_rand(seed, XO_STREAM_BATCH, 4u * (uint64_t)i + 3u);
+    kind[i] = (int32_t)(i & 1);
+    const uint64_t oct = r0 >> 61, base = (uint64_t)256 << oct;
+    n[i] = (int64_t)(base + xo_mulhi(r1, base));
+    const uint64_t doct = xo_mulhi(r2, 3u);
+    mean_deg[i] = (double)((uint64_t)8 << doct) * (1.0 + (double)(r3 >> 11) * (1.0 / 9007199254740992.0));
+    gseed[i] = xo_mix64(seed ^ (0x9e3779b97f4a7c15ULL * (uint64_t)(i + 1)));
+  }
+}
+
+/* one graph of the batch: returns its edge count (u,v local ids) or
+ * -(needed) when cap is too small */
+int64_t xo_batch_graph(int32_t kind, int64_t n, double mean_deg, uint64_t gseed, int64_t cap, int64_t *src,
+                       int64_t *dst) {
+  if (kind == 1) {
+    const int64_t m = (int64_t)llround((double)n * mean_deg / 2.0);
+    if (m > cap) return -m;
+    xo_er_edges(n, gseed, 0, m, src, dst);
+    return m;
+  }
+  const double r2 = mean_deg / (3.14159265358979323846 * (double)n);
+  return xo_rgg_edges(n, gseed, r2, cap, src, dst);
+}

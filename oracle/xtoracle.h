@@ -84,6 +84,13 @@ int64_t xo_ref_rgg(int64_t nv, int P, double radius, int64_t cap, int64_t *off, 
 /* std::seed_seq({s}).generate() of one 32-bit word (utils.hpp:37-44) */
 uint32_t xo_seed_seq1(uint32_t s);
 
+/* the batch workload: per-graph kind (0 geometric, 1 Erdos-Renyi), size,
+ * mean degree and seed; and one graph's edges (local ids; returns the count
+ * or -(needed) when cap is too small) */
+void xo_batch_spec(int64_t ng, uint64_t seed, int32_t *kind, int64_t *n, double *mean_deg, uint64_t *gseed);
+int64_t xo_batch_graph(int32_t kind, int64_t n, double mean_deg, uint64_t gseed, int64_t cap, int64_t *src,
+                       int64_t *dst);
+
 #ifdef __cplusplus
 }
 #endif

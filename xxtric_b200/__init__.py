@@ -82,6 +82,17 @@ _proto("xt_count", _int, _vp, _vp, _vp)
 _proto("xt_count_async", _int, _vp, _vp, _vp)
 _proto("xt_count_device", _int, _i64, _vp, _vp, _vp, _int, _vp)
 _proto("xt_count_device_static", _int, _i64, _vp, _vp, _vp, _int, _vp)
+_proto("xt_graph_from_batch", _int, _vp, _i64, _vp, _vp, _vp, _vp, _int, _P(_vp))
+_proto("xt_graph_from_device_batch", _int, _vp, _i64, _vp, _vp, _vp, _vp, _int, _P(_vp))
+_proto("xt_graph_groups", _i64, _vp)
+_proto("xt_count_groups", _int, _vp, _vp, _vp)
+_proto("xt_count_groups_async", _int, _vp, _vp, _vp)
+_proto("xt_graph_capture", _int, _vp)
+_proto("xt_graph_set_tuning", _int, _vp, _i64, _i64, _i64)
+_proto("xt_graph_autotune", _int, _vp, _int, ctypes.c_char_p, _vp, _i64)
+_proto("xt_batch_spec", _int, _i64, _u64, _vp, _vp, _vp, _vp)
+_proto("xt_gen_batch", _int, _vp, _i64, _vp, _vp, _vp, _vp, _vp, _P(_vp), _P(_vp))
+_proto("xt_device_free", _int, _vp, _vp)
 _proto("xt_gen_rmat", _int, _vp, _int, _i64, _u64, _int, _int, _int, _int, _int, _vp, _vp)
 _proto("xt_gen_chunglu", _int, _vp, _i64, _vp, _i64, _u64, _int, _vp, _vp)
 _proto("xt_chunglu_cdf", _i64, _i64, _dbl, _dbl, _dbl, _vp)
@@ -94,7 +105,9 @@ EXPORTED = ["xt_strerror", "xt_last_error", "xt_open", "xt_close", "xt_set_strea
             "xt_launch_count", "xt_synchronize", "xt_graph_get_perm",
             "xt_graph_from_csr", "xt_graph_from_edges", "xt_graph_from_device_edges", "xt_graph_get_info",
             "xt_graph_get_csr", "xt_graph_free", "xt_count", "xt_count_async", "xt_count_device",
-            "xt_count_device_static",
+            "xt_count_device_static", "xt_graph_from_batch", "xt_graph_from_device_batch", "xt_graph_groups",
+            "xt_count_groups", "xt_count_groups_async", "xt_graph_capture", "xt_graph_set_tuning",
+            "xt_graph_autotune", "xt_batch_spec", "xt_gen_batch", "xt_device_free",
             "xt_gen_rmat", "xt_gen_chunglu", "xt_chunglu_cdf", "xt_gen_er", "xt_vite_read", "xt_vite_write",
             "xt_rgg_generate"]
 
@@ -159,6 +172,36 @@ def generate_rgg(nv: int, nprocs: int = 1, radius: float = 0.0, random_edge_pct:
     _check(_L.xt_rgg_generate(nv, nprocs, radius, random_edge_pct, seed, ne.value, ctypes.byref(ne), _ptr(off),
                               _ptr(tails)), "generate_rgg")
     return off, tails
+
+
+def batch_spec(n_graphs: int, seed: int) -> dict:
+    """The batch workload's per-graph parameters (xt_batch_spec)."""
+    kind = np.zeros(n_graphs, np.int32)
+    n = np.zeros(n_graphs, np.int64)
+    deg = np.zeros(n_graphs, np.float64)
+    gseed = np.zeros(n_graphs, np.uint64)
+    _check(_L.xt_batch_spec(n_graphs, seed, _ptr(kind), _ptr(n), _ptr(deg), _ptr(gseed)), "xt_batch_spec")
+    return {"kind": kind, "n": n, "mean_deg": deg, "graph_seed": gseed}
+
+
+class DeviceArray:
+    """A library-owned device array (released with the context's allocator);
+    torch.as_tensor(arr, device='cuda') views it without a copy."""
+
+    def __init__(self, ctx: "Context", ptr: int, n: int, typestr: str, itemsize: int):
+        self.ctx, self.ptr, self.n, self.typestr, self.itemsize = ctx, ptr, n, typestr, itemsize
+
+    @property
+    def __cuda_array_interface__(self):
+        return {"shape": (self.n,), "typestr": self.typestr, "data": (self.ptr, False), "version": 3}
+
+    def data_ptr(self) -> int:
+        return self.ptr
+
+    def free(self) -> None:
+        if self.ptr and self.ctx._h:
+            _check(_L.xt_device_free(self.ctx._h, self.ptr), "xt_device_free", self.ctx)
+        self.ptr = 0
 
 
 def chunglu_cdf(n: int, gamma: float = 2.1, mean_deg: float = 64.0, max_deg: float = 131072.0):
@@ -244,6 +287,39 @@ class Context:
     def synchronize(self) -> None:
         _check(_L.xt_synchronize(self._h), "xt_synchronize", self)
 
+    # -- batching form --
+    def gen_batch(self, spec: dict):
+        """Generate the batch's graphs on the device: (edge_offsets, src, dst)
+        with local ids; src/dst are DeviceArray (free them when done)."""
+        ng = len(spec["n"])
+        kind = np.ascontiguousarray(spec["kind"], np.int32)
+        n = np.ascontiguousarray(spec["n"], np.int64)
+        deg = np.ascontiguousarray(spec["mean_deg"], np.float64)
+        seed = np.ascontiguousarray(spec["graph_seed"], np.uint64)
+        eoff = np.zeros(ng + 1, np.int64)
+        ps, pd = _vp(), _vp()
+        _check(_L.xt_gen_batch(self._h, ng, _ptr(kind), _ptr(n), _ptr(deg), _ptr(seed), _ptr(eoff),
+                               ctypes.byref(ps), ctypes.byref(pd)), "xt_gen_batch", self)
+        ne = int(eoff[-1])
+        return eoff, DeviceArray(self, ps.value or 0, ne, "<i4", 4), DeviceArray(self, pd.value or 0, ne, "<i4", 4)
+
+    def graph_from_batch(self, vertex_offsets, edge_offsets, src, dst, orient: int = ORIENT_DEGREE,
+                         device: bool = False) -> "DeviceGraph":
+        """Many graphs as one (local ids per graph); device=True when src/dst are device arrays."""
+        voff = np.ascontiguousarray(vertex_offsets, np.int64)
+        eoff = np.ascontiguousarray(edge_offsets, np.int64)
+        h = _vp()
+        if device:
+            s = _L.xt_graph_from_device_batch(self._h, len(voff) - 1, _ptr(voff), _ptr(eoff), _ptr(src), _ptr(dst),
+                                              orient, ctypes.byref(h))
+        else:
+            s_ = np.ascontiguousarray(src, np.int32)
+            d_ = np.ascontiguousarray(dst, np.int32)
+            s = _L.xt_graph_from_batch(self._h, len(voff) - 1, _ptr(voff), _ptr(eoff), _ptr(s_), _ptr(d_), orient,
+                                       ctypes.byref(h))
+        _check(s, "xt_graph_from_batch", self)
+        return DeviceGraph(self, h.value)
+
     # -- generators (device int32 outputs: torch tensors or raw pointers). They
     # run on the context stream; sync=True waits for them, so the outputs can
     # be read from any other stream right away.
@@ -306,6 +382,35 @@ class DeviceGraph:
 
     def count_async(self, d_global, d_per_vertex=None) -> None:
         _check(_L.xt_count_async(self._h, _ptr(d_global), _ptr(d_per_vertex)), "xt_count_async", self.ctx)
+
+    @property
+    def groups(self) -> int:
+        return int(_L.xt_graph_groups(self._h))
+
+    def count_groups(self):
+        """(total, per-graph counts) of a batch."""
+        t = _i64(0)
+        per = np.zeros(max(self.groups, 0), np.int64)
+        _check(_L.xt_count_groups(self._h, ctypes.byref(t), _ptr(per) if len(per) else None), "xt_count_groups",
+               self.ctx)
+        return t.value, per
+
+    def count_groups_async(self, d_total, d_per_group=None) -> None:
+        _check(_L.xt_count_groups_async(self._h, _ptr(d_total), _ptr(d_per_group)), "xt_count_groups_async",
+               self.ctx)
+
+    def capture(self) -> None:
+        _check(_L.xt_graph_capture(self._h), "xt_graph_capture", self.ctx)
+
+    def set_tuning(self, block_work: int = 0, warp_work: int = 0, bitmap_bits: int = 0) -> None:
+        _check(_L.xt_graph_set_tuning(self._h, block_work, warp_work, bitmap_bits), "xt_graph_set_tuning", self.ctx)
+
+    def autotune(self, reps: int = 3, cache_path: Optional[str] = None) -> dict:
+        import json
+        buf = ctypes.create_string_buffer(1 << 16)
+        _check(_L.xt_graph_autotune(self._h, reps, cache_path.encode() if cache_path else None, buf, len(buf)),
+               "xt_graph_autotune", self.ctx)
+        return json.loads(buf.value.decode() or "{}")
 
     def free(self) -> None:
         if self._h:

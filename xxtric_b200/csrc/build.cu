@@ -432,6 +432,10 @@ xt_status build_from_csr(Ctx *c, int64_t nv, const int64_t *d_off, const int64_t
 
 void free_graph_device(Graph *g) {
   if (!g->ctx) return;
+  if (g->exec) cudaGraphExecDestroy(g->exec);
+  g->exec = nullptr;
+  dfree(g->ctx, g->d_res);
+  g->d_res = nullptr;
   free_plan(g);
   dfree(g->ctx, g->d_off);
   dfree(g->ctx, g->d_col);
@@ -439,12 +443,14 @@ void free_graph_device(Graph *g) {
   dfree(g->ctx, g->d_irec);
   dfree(g->ctx, g->d_deg);
   dfree(g->ctx, g->d_perm);
+  dfree(g->ctx, g->d_group);
   g->d_off = nullptr;
   g->d_col = nullptr;
   g->d_ioff = nullptr;
   g->d_irec = nullptr;
   g->d_deg = nullptr;
   g->d_perm = nullptr;
+  g->d_group = nullptr;
 }
 
 }  // namespace xt

@@ -67,6 +67,7 @@ struct Plan {
   unsigned long long *d_cursor = nullptr;  // [0] CTA cursor, [1] warp cursor
   int grid_global = 0, grid_pv = 0;
   int64_t block_work = 0, warp_work = 0;   // the thresholds the plan was made with
+  int64_t bitmap_bits = 0;
 };
 
 static unsigned grid_for(int64_t n, int block, int sm_count) {
@@ -200,15 +201,16 @@ struct Members {
   bool bitmap;
 };
 
-// Chooses the structure for members col[r0, r1) that fits `words` words and
+// Chooses the structure for members col[r0, r1) that fits `words` words (a
+// bitmap only while the members' id range is at most bitmap_bits) and
 // returns how many words must be cleared.
 template <bool PV>
 __device__ __forceinline__ int members_layout(Members &m, const int32_t *__restrict__ col, int64_t r0, int64_t r1,
-                                              int words) {
+                                              int words, int64_t bitmap_bits) {
   m.lo = col[r0];
   m.hi = col[r1 - 1];
   const int64_t range = int64_t(m.hi) - int64_t(m.lo) + 1;
-  m.bitmap = !PV && range <= int64_t(words) * 32;
+  m.bitmap = !PV && range <= int64_t(words) * 32 && range <= bitmap_bits;
   if (m.bitmap) {
     m.mask = 0;
     m.shift = 0;
@@ -486,14 +488,40 @@ __device__ __forceinline__ int64_t stream_suffixes(const InRec *__restrict__ rec
 
 // ---- the count kernel ---------------------------------------------------------
 
+struct CountArgs {
+  const int64_t *off;
+  const int32_t *col;
+  const int64_t *ioff;
+  const InRec *rec;
+  const int64_t *bt;  // CTA tasks
+  int64_t n_bt;
+  const int32_t *wt;  // warp tasks
+  int64_t n_wt;
+  unsigned long long *cursor;     // [0] CTA cursor, [1] warp cursor
+  unsigned long long *global;     // the total
+  int64_t *pv;                    // per-vertex counts (per-vertex mode)
+  const int32_t *group;           // head -> group (a graph of a batch), or null
+  unsigned long long *group_out;  // per-group counts when group != null
+  int64_t bitmap_bits;            // largest member id range kept as a bitmap
+};
+
+// adds a warp's hits of one task to the task head's group
+__device__ __forceinline__ void credit_group(const CountArgs &a, int64_t v, int64_t h, int lane) {
+  for (int o = 16; o; o >>= 1) h += __shfl_xor_sync(0xffffffffu, h, o);
+  if (lane == 0 && h) atomicAdd(&a.group_out[a.group[v]], (unsigned long long)h);
+}
+
 template <bool PV>
-__global__ void __launch_bounds__(kThreads, kMinBlocks) k_count(const int64_t *__restrict__ off, const int32_t *__restrict__ col,
-                                                       const int64_t *__restrict__ ioff,
-                                                       const InRec *__restrict__ rec, const int64_t *__restrict__ bt,
-                                                       int64_t n_bt, const int32_t *__restrict__ wt, int64_t n_wt,
-                                                       unsigned long long *__restrict__ cursor,
-                                                       unsigned long long *__restrict__ global,
-                                                       int64_t *__restrict__ pv) {
+__global__ void __launch_bounds__(kThreads, kMinBlocks) k_count(const CountArgs a) {
+  const int64_t *__restrict__ off = a.off;
+  const int32_t *__restrict__ col = a.col;
+  const int64_t *__restrict__ ioff = a.ioff;
+  const InRec *__restrict__ rec = a.rec;
+  const int64_t *__restrict__ bt = a.bt;
+  const int32_t *__restrict__ wt = a.wt;
+  const int64_t n_bt = a.n_bt, n_wt = a.n_wt;
+  unsigned long long *__restrict__ cursor = a.cursor;
+  int64_t *__restrict__ pv = a.pv;
   extern __shared__ int32_t smem[];
   int32_t *bwords = smem;                                   // kBlockWords
   int32_t *bcnt = smem + kBlockWords;                       // kBlockWords (PV only)
@@ -522,7 +550,7 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) k_count(const int64_t *_
     Members m;
     m.words = bwords;
     m.cnt = bcnt;
-    const int nclear = members_layout<PV>(m, col, r0, r1, kBlockWords);
+    const int nclear = members_layout<PV>(m, col, r0, r1, kBlockWords, a.bitmap_bits);
     for (int i = tid; i < nclear; i += kThreads) {
       bwords[i] = m.bitmap ? 0 : kEmpty;
       if (PV) bcnt[i] = 0;
@@ -535,6 +563,7 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) k_count(const int64_t *_
     bsz = bsz < 1 ? 1 : (bsz > 32 ? 32 : bsz);
     int64_t h = stream_suffixes<PV>(rec, col, k0, k1, int(bsz), &s_batch, m, &s_bv[warp], pv, lane);
     acc += h;
+    if (a.group) credit_group(a, v, h, lane);
     if (PV) {
       for (int o = 16; o; o >>= 1) h += __shfl_xor_sync(0xffffffffu, h, o);
       if (lane == 0) s_red[warp] = (unsigned long long)h;
@@ -565,7 +594,7 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) k_count(const int64_t *_
     Members m;
     m.words = wwords;
     m.cnt = wcnt;
-    const int nclear = members_layout<PV>(m, col, r0, r1, kWarpWords);
+    const int nclear = members_layout<PV>(m, col, r0, r1, kWarpWords, a.bitmap_bits);
     for (int i = lane; i < nclear; i += 32) {
       wwords[i] = m.bitmap ? 0 : kEmpty;
       if (PV) wcnt[i] = 0;
@@ -575,6 +604,7 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) k_count(const int64_t *_
     __syncwarp();
     int64_t h = stream_suffixes<PV>(rec, col, ioff[v], ioff[v + 1], 32, nullptr, m, &s_bv[warp], pv, lane);
     acc += h;
+    if (a.group) credit_group(a, v, h, lane);
     if (PV) {
       for (int o = 16; o; o >>= 1) h += __shfl_xor_sync(0xffffffffu, h, o);
       __syncwarp();
@@ -593,7 +623,7 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) k_count(const int64_t *_
   if (tid == 0) {
     unsigned long long tot = 0;
     for (int w = 0; w < kWarps; w++) tot += s_red[w];
-    atomicAdd(global, tot);
+    atomicAdd(a.global, tot);
   }
 }
 
@@ -706,6 +736,7 @@ xt_status make_plan(Graph *g) {
     }
     pl->block_work = pp.block_work;
     pl->warp_work = pp.warp_work;
+    pl->bitmap_bits = g->tune_bitmap_bits > 0 ? g->tune_bitmap_bits : int64_t(kBlockWords) * 32;
     if ((s = dalloc_n(c, &nb, size_t(nv + 1))) != XT_OK) break;
     if ((s = dalloc_n(c, &nw, size_t(nv + 1))) != XT_OK) break;
     if ((s = dalloc_n(c, &nbp, size_t(nv + 1))) != XT_OK) break;
@@ -751,28 +782,42 @@ xt_status make_plan(Graph *g) {
   return s;
 }
 
-xt_status count_graph(Graph *g, int64_t *d_global, int64_t *d_pv) {
+xt_status count_graph(Graph *g, int64_t *d_global, int64_t *d_pv, int64_t *d_groups) {
   Ctx *c = g->ctx;
   if (!g->plan) XT_TRY(make_plan(g));
   Plan *pl = g->plan;
   XT_CUDA(c, cudaMemsetAsync(pl->d_cursor, 0, 2 * sizeof(unsigned long long), c->stream));
   XT_CUDA(c, cudaMemsetAsync(d_global, 0, sizeof(int64_t), c->stream));
+  if (d_groups) {
+    if (!g->d_group) return set_error(c, XT_ERR_INVALID, "per-group counts need a graph built as a batch");
+    XT_CUDA(c, cudaMemsetAsync(d_groups, 0, sizeof(int64_t) * g->n_groups, c->stream));
+  }
   int64_t *pv_int = nullptr;  // per-vertex counts in internal numbering
   if (d_pv) {
     if (g->d_perm) XT_TRY(dalloc_n(c, &pv_int, size_t(g->nv)));
     else pv_int = d_pv;
     XT_CUDA(c, cudaMemsetAsync(pv_int, 0, sizeof(int64_t) * g->nv, c->stream));
   }
-  unsigned long long *gl = reinterpret_cast<unsigned long long *>(d_global);
+  CountArgs a;
+  a.off = g->d_off;
+  a.col = g->d_col;
+  a.ioff = g->d_ioff;
+  a.rec = g->d_irec;
+  a.bt = pl->d_bt;
+  a.n_bt = pl->n_btask;
+  a.wt = pl->d_wt;
+  a.n_wt = pl->n_wtask;
+  a.cursor = pl->d_cursor;
+  a.global = reinterpret_cast<unsigned long long *>(d_global);
+  a.pv = pv_int;
+  a.group = d_groups ? g->d_group : nullptr;
+  a.group_out = reinterpret_cast<unsigned long long *>(d_groups);
+  a.bitmap_bits = pl->bitmap_bits;
   if (g->ne > 0) {
     if (d_pv)
-      k_count<true><<<counted(c, pl->grid_pv), kThreads, count_smem_bytes(true), c->stream>>>(
-          g->d_off, g->d_col, g->d_ioff, g->d_irec, pl->d_bt, pl->n_btask, pl->d_wt, pl->n_wtask, pl->d_cursor, gl,
-          pv_int);
+      k_count<true><<<counted(c, pl->grid_pv), kThreads, count_smem_bytes(true), c->stream>>>(a);
     else
-      k_count<false><<<counted(c, pl->grid_global), kThreads, count_smem_bytes(false), c->stream>>>(
-          g->d_off, g->d_col, g->d_ioff, g->d_irec, pl->d_bt, pl->n_btask, pl->d_wt, pl->n_wtask, pl->d_cursor, gl,
-          nullptr);
+      k_count<false><<<counted(c, pl->grid_global), kThreads, count_smem_bytes(false), c->stream>>>(a);
   }
   if (d_pv && g->d_perm)
     k_unpermute<<<counted(c, grid_for(g->nv, 256, c->sm_count)), 256, 0, c->stream>>>(pv_int, g->d_perm, g->nv, d_pv);

@@ -92,6 +92,14 @@ struct Graph {
   int64_t max_in_degree = 0;
   int64_t tune_block_work = 0;  // schedule overrides (0: choose automatically)
   int64_t tune_warp_work = 0;
+  int64_t tune_bitmap_bits = 0;
+  int32_t *d_group = nullptr;   // internal id -> group (graph of a batch), or null
+  int64_t n_groups = 0;
+  // a captured count (CUDA graph) writing the total and the per-group
+  // counts into d_res[0] and d_res[1..n_groups]
+  cudaGraphExec_t exec = nullptr;
+  int64_t exec_kernels = 0;  // library kernels inside `exec`, counted per replay
+  int64_t *d_res = nullptr;
   int64_t wedge_work = 0;   // sum over oriented (u,v) of d+(v)
   int64_t stream_work = 0;  // sum over oriented (u,v) of d+(u) = sum_u d+(u)^2
   Plan *plan = nullptr;
@@ -113,7 +121,8 @@ void free_plan(Graph *g);
 
 // Launches the count on the graph's context stream. d_global: one int64
 // (overwritten); d_pv: nv int64 (nullable, overwritten).
-xt_status count_graph(Graph *g, int64_t *d_global, int64_t *d_pv);
+// d_groups: n_groups int64 per-group counts (graphs built as a batch), nullable.
+xt_status count_graph(Graph *g, int64_t *d_global, int64_t *d_pv, int64_t *d_groups = nullptr);
 
 }  // namespace xt
 
