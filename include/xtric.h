@@ -172,6 +172,12 @@ xt_status xt_graph_capture(xt_graph *g);
  * a warp task, and the largest member id range kept as a bitmap (beyond it a
  * hash). Re-plans (and re-captures a captured graph). */
 xt_status xt_graph_set_tuning(xt_graph *g, int64_t block_work, int64_t warp_work, int64_t bitmap_bits);
+/* Tier limits: heads with at most lane_work candidates are counted one per
+ * lane (binary search in the row), heads with at most warp_work candidates
+ * and at most 256 members one per warp, the rest by CTA tasks. Negative =
+ * automatic (the lane tier is on only for graphs of 2^30 or more
+ * candidates), 0 = tier off. Re-plans (and re-captures a captured graph). */
+xt_status xt_graph_set_tiers(xt_graph *g, int64_t lane_work, int64_t warp_work);
 /* Autotuner: a coordinate search of the three thresholds, timing `reps`
  * counts each, keeping the fastest; with cache_path it first looks the
  * (GPU, graph class) key up in that text file and appends new results.

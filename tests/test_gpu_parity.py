@@ -247,3 +247,43 @@ def test_mirror_class(ctx):
     assert tc.count() == GOLDEN["rmat10"]["triangles"]
     assert tc.count() == GOLDEN["rmat10"]["triangles"]  # counting twice is idempotent
     tc.clear()
+
+
+# (lane_work, warp_work): every head on one tier, and the automatic choice
+TIERS = [(1 << 40, 0), (0, 1 << 40), (0, 0), (64, 4096), (-1, -1)]
+
+
+@pytest.mark.parametrize("kind", ["rmat", "chunglu"])
+def test_each_tier_alone_vs_oracle(ctx, torch_cuda, kind):
+    # Lane tasks (binary search in the row), warp tasks and CTA tasks each
+    # count the whole graph alone, then mixed; totals, per-vertex counts and
+    # a captured replay after a re-plan all equal the oracle's.
+    torch = torch_cuda
+    if kind == "rmat":
+        n, m = 1 << 14, 16 << 14
+        s = torch.empty(m, dtype=torch.int32, device="cuda")
+        d = torch.empty_like(s)
+        ctx.gen_rmat(14, m, 3, s, d)
+    else:
+        n = 1 << 15
+        cdf, m = xt.chunglu_cdf(n, 2.1, 24.0, 8192.0)
+        s = torch.empty(m, dtype=torch.int32, device="cuda")
+        d = torch.empty_like(s)
+        ctx.gen_chunglu(cdf, m, 5, s, d)
+    off, tails = oracle.canon_csr(n, s.cpu().numpy().astype(np.int64), d.cpu().numpy().astype(np.int64))
+    expect, opv = oracle.count_merge(off, tails, per_vertex=True)
+    for orient in ORIENTS:
+        g = ctx.graph_from_device_edges(n, m, s, d, orient)
+        try:
+            for lane_work, warp_work in TIERS:
+                g.set_tiers(lane_work, warp_work)
+                t, pv = g.count(per_vertex=True)
+                assert t == expect, (orient, lane_work, warp_work)
+                assert (pv == opv).all(), (orient, lane_work, warp_work)
+            g.set_tiers(1 << 40, 0)
+            g.capture()
+            assert g.count_groups()[0] == expect  # the captured replay
+            g.set_tiers(0, 1 << 40)  # re-plans and re-captures
+            assert g.count_groups()[0] == expect
+        finally:
+            g.free()

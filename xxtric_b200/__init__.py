@@ -89,6 +89,7 @@ _proto("xt_count_groups", _int, _vp, _vp, _vp)
 _proto("xt_count_groups_async", _int, _vp, _vp, _vp)
 _proto("xt_graph_capture", _int, _vp)
 _proto("xt_graph_set_tuning", _int, _vp, _i64, _i64, _i64)
+_proto("xt_graph_set_tiers", _int, _vp, _i64, _i64)
 _proto("xt_graph_autotune", _int, _vp, _int, ctypes.c_char_p, _vp, _i64)
 _proto("xt_batch_spec", _int, _i64, _u64, _vp, _vp, _vp, _vp)
 _proto("xt_gen_batch", _int, _vp, _i64, _vp, _vp, _vp, _vp, _vp, _P(_vp), _P(_vp))
@@ -106,7 +107,7 @@ EXPORTED = ["xt_strerror", "xt_last_error", "xt_open", "xt_close", "xt_set_strea
             "xt_graph_from_csr", "xt_graph_from_edges", "xt_graph_from_device_edges", "xt_graph_get_info",
             "xt_graph_get_csr", "xt_graph_free", "xt_count", "xt_count_async", "xt_count_device",
             "xt_count_device_static", "xt_graph_from_batch", "xt_graph_from_device_batch", "xt_graph_groups",
-            "xt_count_groups", "xt_count_groups_async", "xt_graph_capture", "xt_graph_set_tuning",
+            "xt_count_groups", "xt_count_groups_async", "xt_graph_capture", "xt_graph_set_tuning", "xt_graph_set_tiers",
             "xt_graph_autotune", "xt_batch_spec", "xt_gen_batch", "xt_device_free",
             "xt_gen_rmat", "xt_gen_chunglu", "xt_chunglu_cdf", "xt_gen_er", "xt_vite_read", "xt_vite_write",
             "xt_rgg_generate"]
@@ -404,6 +405,13 @@ class DeviceGraph:
 
     def set_tuning(self, block_work: int = 0, warp_work: int = 0, bitmap_bits: int = 0) -> None:
         _check(_L.xt_graph_set_tuning(self._h, block_work, warp_work, bitmap_bits), "xt_graph_set_tuning", self.ctx)
+
+    def set_tiers(self, lane_work: int = -1, warp_work: int = -1) -> None:
+        """Tier limits of the schedule: heads with at most lane_work candidates
+        go one per lane, then heads with at most warp_work candidates (and at
+        most 256 members) one per warp, the rest to CTA tasks. -1 = automatic,
+        0 = tier off."""
+        _check(_L.xt_graph_set_tiers(self._h, lane_work, warp_work), "xt_graph_set_tiers", self.ctx)
 
     def autotune(self, reps: int = 3, cache_path: Optional[str] = None) -> dict:
         import json

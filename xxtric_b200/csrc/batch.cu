@@ -438,6 +438,15 @@ xt_status run_count_res(Graph *g) {
   return count_graph(g, g->d_res, nullptr, g->n_groups > 0 ? g->d_res + 1 : nullptr);
 }
 
+xt_status set_tiers(Graph *g, int64_t lane_work, int64_t warp_work) {
+  const bool was_captured = g->exec != nullptr;
+  g->tier_lane_work = lane_work >= 0 ? lane_work : -1;
+  g->tier_warp_work = warp_work >= 0 ? warp_work : -1;
+  XT_TRY(make_plan(g));
+  if (was_captured) XT_TRY(capture_count(g));
+  return XT_OK;
+}
+
 xt_status set_tuning(Graph *g, int64_t block_work, int64_t warp_work, int64_t bitmap_bits) {
   const bool was_captured = g->exec != nullptr;
   g->tune_block_work = block_work > 0 ? block_work : 0;
@@ -485,8 +494,9 @@ static std::string tune_key(const Graph *g) {
     }
     return b;
   };
-  char buf[256];
-  snprintf(buf, sizeof buf, "%s|sm%d|orient%d|nv2^%d|ne2^%d|work2^%d|groups%lld", p.name, p.multiProcessorCount,
+  char buf[512];
+  // the schedule revision keeps timings of an older kernel from being reused
+  snprintf(buf, sizeof buf, "sched3|%s|sm%d|orient%d|nv2^%d|ne2^%d|work2^%d|groups%lld", p.name, p.multiProcessorCount,
            g->orient, lg(g->nv), lg(g->ne), lg(g->stream_work), (long long)g->n_groups);
   for (char *q = buf; *q; q++)
     if (*q == ' ') *q = '_';
@@ -685,6 +695,12 @@ xt_status xt_graph_set_tuning(xt_graph *gr, int64_t block_work, int64_t warp_wor
   if (!gr) return XT_ERR_INVALID;
   cudaSetDevice(gr->g.ctx->device);
   return set_tuning(&gr->g, block_work, warp_work, bitmap_bits);
+}
+
+xt_status xt_graph_set_tiers(xt_graph *gr, int64_t lane_work, int64_t warp_work) {
+  if (!gr) return XT_ERR_INVALID;
+  cudaSetDevice(gr->g.ctx->device);
+  return set_tiers(&gr->g, lane_work, warp_work);
 }
 
 xt_status xt_graph_autotune(xt_graph *gr, int reps, const char *cache_path, char *report, int64_t report_len) {

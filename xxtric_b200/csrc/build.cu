@@ -155,9 +155,32 @@ __global__ void k_degree_from_off(const int64_t *__restrict__ off, int64_t nv, i
   XT_GRID_STRIDE(i, nv) deg[i] = int32_t(off[i + 1] - off[i]);
 }
 
-// (head << pb | position) for every out-CSR position
-__global__ void k_in_keys(const int32_t *__restrict__ col, int64_t m, int pb, uint64_t *__restrict__ ik) {
-  XT_GRID_STRIDE(p, m) ik[p] = (uint64_t(uint32_t(col[p])) << pb) | uint64_t(p);
+// Suffix-length class, longest first: 127 - c where c is the length itself
+// below 32 and four classes per octave above, so records of one head sort
+// into runs of similar length.
+__device__ __forceinline__ uint32_t len_class_desc(int64_t len) {
+  uint32_t c;
+  if (len < 32) {
+    c = uint32_t(len);
+  } else {
+    const int lg = 63 - __clzll(len);
+    c = 32u + 4u * uint32_t(lg - 5) + uint32_t((len >> (lg - 2)) & 3);
+  }
+  return 127u - (c < 127u ? c : 127u);
+}
+
+// (head << (lb + pb) | length class << pb | position) for every out-CSR
+// position; lb (0..7) bits of the class fit beside the head and position
+__global__ void k_in_keys(const int32_t *__restrict__ col, const int32_t *__restrict__ rowof,
+                          const int64_t *__restrict__ off, int64_t m, int pb, int lb, uint64_t *__restrict__ ik) {
+  XT_GRID_STRIDE(p, m) {
+    uint64_t k = (uint64_t(uint32_t(col[p])) << (pb + lb)) | uint64_t(p);
+    if (lb > 0) {
+      const int64_t len = off[rowof[p] + 1] - p - 1;
+      k |= uint64_t(len_class_desc(len) >> (7 - lb)) << pb;
+    }
+    ik[p] = k;
+  }
 }
 
 // sorted in-keys -> in-records (suffix of N+(u) after the head)
@@ -286,7 +309,7 @@ static xt_status orient_and_finish(Ctx *c, uint64_t *uniq, uint64_t *scratch, in
   XT_TRY(dalloc_n(c, &g->d_col, size_t(m) + kColPad));
   XT_CUDA(c, cudaMemsetAsync(g->d_col + m, 0xff, sizeof(int32_t) * kColPad, c->stream));
   XT_TRY(keys_to_csr(c, okeys, m, nv, b, g->d_off, g->d_col));
-  // in-records grouped by head, in increasing out-position
+  // in-records grouped by head, longest suffix first
   XT_TRY(dalloc_n(c, &g->d_ioff, size_t(nv + 1)));
   XT_TRY(dalloc_n(c, &g->d_irec, size_t(m > 0 ? m : 1)));
   if (m == 0) {
@@ -294,6 +317,7 @@ static xt_status orient_and_finish(Ctx *c, uint64_t *uniq, uint64_t *scratch, in
     return XT_OK;
   }
   const int pb = bits_for(m);
+  const int lb = (b + pb + 7 <= 64) ? 7 : (b + pb < 64 ? 64 - b - pb : 0);
   uint64_t *ik = (okeys == scratch) ? uniq : scratch;  // the buffer no longer needed
   uint64_t *ik2 = nullptr;
   int32_t *rowof = nullptr;
@@ -301,11 +325,12 @@ static xt_status orient_and_finish(Ctx *c, uint64_t *uniq, uint64_t *scratch, in
   if (s == XT_OK) s = dalloc_n(c, &rowof, size_t(m));
   if (s == XT_OK) {
     k_csr_rows<<<counted(c, grid_for(nv * 32, B, c->sm_count)), B, 0, c->stream>>>(g->d_off, nv, m, rowof, nullptr);
-    k_in_keys<<<counted(c, grid_for(m, B, c->sm_count)), B, 0, c->stream>>>(g->d_col, m, pb, ik);
+    k_in_keys<<<counted(c, grid_for(m, B, c->sm_count)), B, 0, c->stream>>>(g->d_col, rowof, g->d_off, m, pb, lb,
+                                                                            ik);
     s = cuda_status(c, cudaGetLastError(), "in-keys");
   }
-  if (s == XT_OK) s = sort_keys(c, ik, ik2, m, b + pb);
-  if (s == XT_OK) s = keys_to_csr(c, ik2, m, nv, pb, g->d_ioff, nullptr);
+  if (s == XT_OK) s = sort_keys(c, ik, ik2, m, b + lb + pb);
+  if (s == XT_OK) s = keys_to_csr(c, ik2, m, nv, lb + pb, g->d_ioff, nullptr);
   if (s == XT_OK) {
     k_in_records<<<counted(c, grid_for(m, B, c->sm_count)), B, 0, c->stream>>>(ik2, m, pb, rowof, g->d_off,
                                                                                g->d_irec);

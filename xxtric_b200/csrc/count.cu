@@ -6,21 +6,26 @@
 // binary-searches adj(v) for w (xxtric.hpp:150-207, check_edgelist
 // xxtric.hpp:516-545). Here it is found from the MIDDLE corner v:
 //   1. N+(v) is loaded once into shared memory as a membership structure:
-//      a bitmap over [min N+(v), max N+(v)] when that range is small enough,
-//      else an open-addressing hash table (load factor <= 1/4);
+//      a bitmap over the words spanning [min N+(v), max N+(v)] when that range
+//      is small enough, else an open-addressing hash table (load factor <= 1/4);
 //   2. for every in-edge u->v, the suffix of N+(u) after v (the reference's
-//      n > m range) is streamed through it. A candidate below min N+(v) is
-//      skipped and one above max N+(v) ends that suffix (the reference's
+//      n > m range) is streamed through it; candidates outside
+//      [min N+(v), max N+(v)] fail the test at once (the reference's
 //      edge_above_min / edge_within_max prunes, xxtric.hpp:576-588).
 // Items streamed: sum over u of C(d+(u), 2), each tested in shared memory.
 //
 // Schedule (make_plan): per head v, work(v) = total suffix length.
-//   warp bin : d+(v) <= kWarpDmax and work(v) <= kWarpWork -> one warp per v
-//   block bin: otherwise -> CTA tasks over chunks of v's in-records of about
-//              kBlockWork items; N+(v) beyond kBlockDmax members is split
+//   lane tier: work(v) <= tiny_work -> one lane per head, members
+//              binary-searched in the row itself
+//   warp tier: d+(v) <= kWarpDmax and work(v) <= warp_work -> one warp per
+//              head, member set in the warp's slice of shared memory
+//   CTA tier : otherwise -> CTA tasks over chunks of v's in-records of about
+//              block_work items; N+(v) beyond kBlockDmax members is split
 //              into parts, one task per (part, chunk)
 // One persistent kernel drains the CTA tasks first (the large ones), then the
-// warp tasks, each from its own global atomic cursor.
+// warp tasks, then the lane tasks, each from its own global atomic cursor.
+// Inside a task, lanes walk whole suffixes in aligned 32-byte pairs (see
+// stream_kind).
 #include <cub/cub.cuh>
 
 #include "xt_internal.cuh"
@@ -40,31 +45,59 @@ namespace xt {
 constexpr int kThreads = XT_THREADS;
 constexpr int kWarps = kThreads / 32;
 #ifndef XT_MIN_BLOCKS
-#define XT_MIN_BLOCKS (1024 / XT_THREADS)
+#define XT_MIN_BLOCKS 3
 #endif
-constexpr int kMinBlocks = XT_MIN_BLOCKS;  // CTAs per SM the register budget is sized for
-constexpr int kWarpDmax = 64;
-constexpr int kWarpWords = 256;   // per-warp region: 256-slot hash or 8192-bit bitmap
+// CTAs per SM the register budget is sized for: 3 x 256 threads leave ~80
+// registers a thread, and fewer tasks in flight keep more of their suffixes in L2
+constexpr int kMinBlocks = XT_MIN_BLOCKS;
+constexpr int kBlockWords = 8192;  // CTA region: 8192-slot hash or 2^18-bit bitmap
+// warp tasks run after the CTA tasks and split the CTA region among the warps
+constexpr int kWarpWords = kBlockWords / kWarps;  // 1024: a 1024-slot hash or a 32K-bit bitmap
+constexpr int kWarpDmax = kWarpWords / 4;         // hash load factor <= 1/4
 constexpr int64_t kWarpWork = XT_WARP_WORK;
 constexpr int kBlockDmax = 2048;
-constexpr int kBlockWords = 8192;  // CTA region: 8192-slot hash or 2^18-bit bitmap
 constexpr int64_t kBlockWorkMin = int64_t(1) << 14;
 constexpr int64_t kBlockWorkMax = int64_t(1) << XT_BLOCK_WORK_LOG2;
 
 // Run-time schedule thresholds (the binning of make_plan).
 struct PlanParams {
-  int64_t warp_work;   // a head with d+(v) <= warp_dmax and at most this much work is a warp task
+  int64_t tiny_work;   // a head with at most this much work is a lane task
+  int64_t warp_work;   // ... else one with d+(v) <= warp_dmax and at most this much work is a warp task
   int64_t block_work;  // items per CTA task
   int32_t warp_dmax;
+  int32_t batches_per_warp;  // CTA task: record batches per warp, at least
+  int32_t lane_pairs;        // CTA task: pairs per lane on an average record, at least
 };
+#ifndef XT_BATCHES_PER_WARP
+#define XT_BATCHES_PER_WARP 4
+#endif
+#ifndef XT_LANE_PAIRS
+#define XT_LANE_PAIRS 2
+#endif
+#ifndef XT_TINY_WORK
+#define XT_TINY_WORK 64
+#endif
 constexpr int32_t kEmpty = -1;
 
+// A warp or CTA task: the in-records [k0, k0 + nrec) of head v streamed
+// through the members col[r0, r0 + nmem), 2^lg_s lanes per record.
+struct __align__(16) Task {
+  int64_t k0;
+  int64_t r0;
+  int32_t v;
+  int32_t nrec;
+  int32_t nmem;
+  int32_t lg_s;
+};
+
 struct Plan {
-  int64_t n_btask = 0;        // CTA tasks
-  int64_t *d_bt = nullptr;    // 4 int64 per task: v, part, k0, k1 (k = in-record index)
-  int64_t n_wtask = 0;        // warp tasks
-  int32_t *d_wt = nullptr;    // v per warp task
-  unsigned long long *d_cursor = nullptr;  // [0] CTA cursor, [1] warp cursor
+  int64_t n_btask = 0;         // CTA tasks
+  Task *d_bt = nullptr;
+  int64_t n_wtask = 0;         // warp tasks
+  Task *d_wt = nullptr;
+  int64_t n_ttask = 0;         // lane tasks: one head per lane
+  int32_t *d_tt = nullptr;
+  unsigned long long *d_cursor = nullptr;  // [0] CTA, [1] warp, [2] lane task cursors
   int grid_global = 0, grid_pv = 0;
   int64_t block_work = 0, warp_work = 0;   // the thresholds the plan was made with
   int64_t bitmap_bits = 0;
@@ -96,14 +129,19 @@ __global__ void k_outedge_work(const int32_t *__restrict__ col, int64_t ne, cons
   }
 }
 
+// tasks of head v: nb CTA tasks (parts x chunks), nw warp tasks, nt lane tasks (0 or 1 each)
 __device__ __forceinline__ void classify(int64_t v, const int64_t *__restrict__ off, const int64_t *__restrict__ ioff,
                                          const int64_t *__restrict__ P, const PlanParams pp, int64_t &nb,
-                                         int64_t &nw, int64_t &parts, int64_t &chunks, int64_t &work) {
+                                         int64_t &nw, int64_t &nt, int64_t &parts, int64_t &chunks, int64_t &work) {
   const int64_t dp = off[v + 1] - off[v];
   const int64_t k0 = ioff[v], k1 = ioff[v + 1];
-  nb = nw = parts = chunks = 0;
+  nb = nw = nt = parts = chunks = 0;
   work = P[k1] - P[k0];
   if (dp == 0 || work == 0) return;
+  if (work <= pp.tiny_work) {
+    nt = 1;
+    return;
+  }
   if (dp <= pp.warp_dmax && work <= pp.warp_work) {
     nw = 1;
     return;
@@ -115,12 +153,13 @@ __device__ __forceinline__ void classify(int64_t v, const int64_t *__restrict__ 
 
 __global__ void k_plan_count(int64_t nv, const int64_t *__restrict__ off, const int64_t *__restrict__ ioff,
                              const int64_t *__restrict__ P, const PlanParams pp, int64_t *__restrict__ nb_out,
-                             int64_t *__restrict__ nw_out) {
+                             int64_t *__restrict__ nw_out, int64_t *__restrict__ nt_out) {
   XT_GRID_STRIDE(v, nv) {
-    int64_t nb, nw, parts, chunks, work;
-    classify(v, off, ioff, P, pp, nb, nw, parts, chunks, work);
+    int64_t nb, nw, nt, parts, chunks, work;
+    classify(v, off, ioff, P, pp, nb, nw, nt, parts, chunks, work);
     nb_out[v] = nb;
     nw_out[v] = nw;
+    nt_out[v] = nt;
   }
 }
 
@@ -134,34 +173,61 @@ __device__ __forceinline__ int64_t lower_bound_i64(const int64_t *__restrict__ P
   return lo;
 }
 
+// log2 of the lanes per record for a task of R records and W items run by
+// `warps` warps: batches small enough that every warp gets batches_per_warp
+// of them, but no more lanes on a record than leave each lane_pairs pairs
+// of 8 columns
+__device__ __forceinline__ int32_t lanes_log2(int64_t R, int64_t W, int warps, const PlanParams &pp) {
+  const int64_t per = R / (int64_t(pp.batches_per_warp) * warps);
+  int lg_b = 0;
+  while (lg_b < 5 && (int64_t(2) << lg_b) <= per) lg_b++;
+  int lg_s = 5 - lg_b;
+  const int64_t pairs = W / (8 * R) + 1;
+  while (lg_s > 0 && (pairs >> lg_s) < pp.lane_pairs) lg_s--;
+  return lg_s;
+}
+
+__device__ __forceinline__ Task make_task(int64_t v, int64_t k0, int64_t k1, int64_t r0, int64_t r1, int32_t lg_s) {
+  Task t;
+  t.k0 = k0;
+  t.r0 = r0;
+  t.v = int32_t(v);
+  t.nrec = int32_t(k1 - k0);
+  t.nmem = int32_t(r1 - r0);
+  t.lg_s = lg_s;
+  return t;
+}
+
 __global__ void k_plan_fill(int64_t nv, const int64_t *__restrict__ off, const int64_t *__restrict__ ioff,
                             const int64_t *__restrict__ P, const PlanParams pp, const int64_t *__restrict__ nb_pos,
-                            const int64_t *__restrict__ nw_pos, int64_t *__restrict__ bt, int32_t *__restrict__ wt) {
+                            const int64_t *__restrict__ nw_pos, const int64_t *__restrict__ nt_pos,
+                            Task *__restrict__ bt, Task *__restrict__ wt, int32_t *__restrict__ tt) {
   XT_GRID_STRIDE(v, nv) {
-    int64_t nb, nw, parts, chunks, work;
-    classify(v, off, ioff, P, pp, nb, nw, parts, chunks, work);
-    if (nw) wt[nw_pos[v]] = int32_t(v);
+    int64_t nb, nw, nt, parts, chunks, work;
+    classify(v, off, ioff, P, pp, nb, nw, nt, parts, chunks, work);
+    const int64_t k0 = ioff[v], k1 = ioff[v + 1];
+    if (nt) tt[nt_pos[v]] = int32_t(v);
+    if (nw) {
+      // a few records spread over the whole warp
+      int32_t lg_s = 5;
+      while (lg_s > 0 && (int64_t(32) >> lg_s) < k1 - k0) lg_s--;
+      wt[nw_pos[v]] = make_task(v, k0, k1, off[v], off[v + 1], lg_s);
+    }
     if (!nb) continue;
-    const int64_t k0 = ioff[v], k1 = ioff[v + 1], base = P[k0];
+    const int64_t base = P[k0];
     int64_t t = nb_pos[v], prev = k0;
     for (int64_t c = 0; c < chunks; c++) {
       const int64_t kend = (c + 1 == chunks) ? k1 : lower_bound_i64(P, prev, k1, base + (work * (c + 1)) / chunks);
       if (kend <= prev) continue;  // empty chunk (one in-record carries more work)
+      const int32_t lg_s = lanes_log2(kend - prev, P[kend] - P[prev], kWarps, pp);
       for (int64_t p = 0; p < parts; p++) {
-        bt[4 * t + 0] = v;
-        bt[4 * t + 1] = p;
-        bt[4 * t + 2] = prev;
-        bt[4 * t + 3] = kend;
-        t++;
+        const int64_t r0 = off[v] + p * kBlockDmax;
+        const int64_t r1 = min(off[v + 1], r0 + kBlockDmax);
+        bt[t++] = make_task(v, prev, kend, r0, r1, lg_s);
       }
       prev = kend;
     }
-    for (; t < nb_pos[v] + nb; t++) {  // slots of empty chunks: no-op tasks
-      bt[4 * t + 0] = v;
-      bt[4 * t + 1] = 0;
-      bt[4 * t + 2] = k1;
-      bt[4 * t + 3] = k1;
-    }
+    for (; t < nb_pos[v] + nb; t++) bt[t] = make_task(v, k1, k1, off[v], off[v] + 1, 0);  // empty chunks: no-ops
   }
 }
 
@@ -196,28 +262,33 @@ struct Members {
   int32_t *words;   // bitmap words or hash slots
   int32_t *cnt;     // per-slot hit counters (per-vertex mode, hash only)
   int32_t lo, hi;   // smallest and largest member
+  uint32_t base;    // bitmap: x is bit (x & 31) of words[(x >> 5) - base]
+  uint32_t nwords;  // bitmap: words in use; words[nwords] is a zero guard word
   uint32_t mask;    // hash: slots - 1
   int shift;        // hash: 32 - log2(slots)
   bool bitmap;
 };
 
-// Chooses the structure for members col[r0, r1) that fits `words` words (a
-// bitmap only while the members' id range is at most bitmap_bits) and
-// returns how many words must be cleared.
+// Chooses the structure for members mem[0, n) (ascending) that fits `words`
+// words (a bitmap only while the members' id range is at most bitmap_bits)
+// and returns how many words must be cleared.
 template <bool PV>
-__device__ __forceinline__ int members_layout(Members &m, const int32_t *__restrict__ col, int64_t r0, int64_t r1,
-                                              int words, int64_t bitmap_bits) {
-  m.lo = col[r0];
-  m.hi = col[r1 - 1];
+__device__ __forceinline__ int members_layout(Members &m, const int32_t *mem, int n, int words, int64_t bitmap_bits) {
+  m.lo = mem[0];
+  m.hi = mem[n - 1];
   const int64_t range = int64_t(m.hi) - int64_t(m.lo) + 1;
-  m.bitmap = !PV && range <= int64_t(words) * 32 && range <= bitmap_bits;
+  const int64_t nw = int64_t(m.hi >> 5) - int64_t(m.lo >> 5) + 1;
+  m.bitmap = !PV && nw + 1 <= int64_t(words) && range <= bitmap_bits;
   if (m.bitmap) {
+    m.base = uint32_t(m.lo >> 5);
+    m.nwords = uint32_t(nw);
     m.mask = 0;
     m.shift = 0;
-    return int((range + 31) >> 5);
+    return int(nw + 1);
   }
+  m.base = m.nwords = 0;
   int lg = 6;
-  while ((int64_t(1) << lg) < 4 * (r1 - r0)) lg++;  // load factor <= 1/4: an absent key costs ~1.2 probes
+  while ((1 << lg) < 4 * n) lg++;  // load factor <= 1/4: an absent key costs ~1.2 probes
   m.mask = (1u << lg) - 1;
   m.shift = 32 - lg;
   return 1 << lg;
@@ -225,88 +296,116 @@ __device__ __forceinline__ int members_layout(Members &m, const int32_t *__restr
 
 __device__ __forceinline__ void members_insert(const Members &m, int32_t x) {
   if (m.bitmap) {
-    const uint32_t d = uint32_t(x - m.lo);
-    atomicOr(reinterpret_cast<unsigned int *>(&m.words[d >> 5]), 1u << (d & 31));
+    atomicOr(reinterpret_cast<unsigned int *>(&m.words[uint32_t(x >> 5) - m.base]), 1u << (x & 31));
   } else {
     hash_insert(m.words, m.mask, m.shift, x);
   }
 }
 
 // ---- streaming the in-record suffixes ----------------------------------------
-
-// A warp step: kStepGroups x 32 aligned 16-byte groups (kStepGroups LDG.128
-// per lane) taken from the flattened groups of a batch of suffixes, so a
-// step spans as many suffixes as it needs and every lane has groups while
-// the batch lasts.
-#ifndef XT_STEP_GROUPS
-#define XT_STEP_GROUPS 2
+//
+// A pair is an aligned 32-byte block of 8 columns (two 16-byte loads). A
+// batch holds 32/S records; the S lanes of record j take its pairs k, k+S,
+// k+2S, ... so every lane streams a contiguous run of one suffix with no
+// per-column bookkeeping. Records of a head are stored longest first, so the
+// lanes of a batch run for about as many steps each. Columns outside the
+// suffix (the head side of the first pair, the next row after the last)
+// are replaced by a sentinel that no membership test accepts; the test is
+// needed only on a batch's first step and once any lane reaches its last
+// pair.
+#ifndef XT_PF_DEPTH
+#define XT_PF_DEPTH 1
 #endif
-constexpr int kStepGroups = XT_STEP_GROUPS;
+constexpr int32_t kSentinel = -2;  // negative: below every member, and not kEmpty
+// positions inside one suffix are int32: out-degrees stay below this
+constexpr int64_t kMaxOutDegree = int64_t(1) << 30;
 
-struct Chunk {
-  int4 x[kStepGroups];     // four columns per group
-  uint32_t vm[kStepGroups];  // which of the four are inside the suffix (bit i: column i)
-  int32_t rj[kStepGroups];   // the suffix's slot in the batch (per-vertex credit)
-  bool exists;               // warp-uniform: this step exists
-};
-
-// bits i in [0,4) with pos + i in [lo, hi), where lo - pos <= 3 whenever
-// lo > pos (a suffix starts inside its first group)
-__device__ __forceinline__ uint32_t valid_mask(uint32_t pos, uint32_t lo, uint32_t hi) {
-  const uint32_t a = lo > pos ? lo - pos : 0u;
-  uint32_t b = hi > pos ? hi - pos : 0u;
-  b = b > 4u ? 4u : b;
-  return ((1u << b) - 1u) & ~((1u << a) - 1u);
+// One 256-bit load per lane (sm_100 vector width; the column array is
+// 256-byte aligned, so every pair is 32-byte aligned): one L1 wavefront per
+// line touched instead of one per 16-byte half.
+__device__ __forceinline__ void load_pair(const int32_t *__restrict__ col, int64_t P, int4 &a, int4 &b) {
+  const int32_t *p = col + 8 * P;
+  asm volatile("ld.global.nc.v8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+               : "=r"(a.x), "=r"(a.y), "=r"(a.z), "=r"(a.w), "=r"(b.x), "=r"(b.y), "=r"(b.z), "=r"(b.w)
+               : "l"(p));
 }
 
-// Per-warp shared-memory view of the current batch.
-// Flattened positions are 4 x flattened group + column in group; a batch
-// holds at most 32 suffixes of fewer than kMaxOutDegree columns each, so
-// positions fit in 32 bits.
-constexpr int64_t kMaxOutDegree = int64_t(1) << 27;
+// Asks L2 to fetch [p, p + bytes) (16-byte aligned, a multiple of 16 bytes)
+// without waiting for it: the suffixes of the next batch are on their way to
+// L2 while this batch streams.
+#ifndef XT_L2_PREFETCH
+#define XT_L2_PREFETCH 1
+#endif
+__device__ __forceinline__ void prefetch_l2(const void *p, uint32_t bytes) {
+  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
+}
 
-struct BatchView {
-  uint32_t start[33];  // first flattened group of each suffix; start[32] = total
-  int64_t gbase[32];   // first global group index of each suffix, minus its start
-  uint32_t lopos[32];  // the suffix's first flattened position
-  uint32_t hipos[32];  // one past its last
-  int32_t u[32];       // the suffix's owner
-  int32_t hits[32];    // per-vertex mode: hits per suffix in this batch
-};
-
-// One warp's walk over the in-records rec[k0, kend), taken in batches of bsz
-// records (lane j < bsz holds record j of a batch). Batches come one after
-// another (a warp task), or from a cursor in shared memory that the warps of
-// a CTA task share, so warps that finish early take more. The next batch is
-// claimed and its records loaded while the current one streams.
-template <bool PV>
-struct FlatWalk {
-  const InRec *__restrict__ rec;  // the task's records: rec[0, kend)
-  const int32_t *__restrict__ col;
-  int64_t *__restrict__ pv;
-  BatchView *bv;
-  int *cursor;                // shared batch cursor (CTA task) or null
-  int32_t kend;               // records in the task
-  int32_t kb, nkb, seq;       // current / next batch base, next sequential base
-  int bsz, nb;
-  int4 nrec;                  // lane's record of the next batch (prefetched)
-  uint32_t total, F;          // groups in the batch, next step's first group (uniform)
-  int r;                      // this lane's suffix cursor (monotone within a batch)
-  // this lane's copy of suffix r's layout: flattened groups end at c_end,
-  // global group = flattened + c_gb, valid flattened positions [c_lo, c_hi)
-  uint32_t c_end, c_lo, c_hi;
-  int64_t c_gb;
-  bool have;
-  int lane;
-
-  __device__ __forceinline__ void load_suffix() {
-    c_end = bv->start[r + 1];
-    c_gb = bv->gbase[r];
-    c_lo = bv->lopos[r];
-    c_hi = bv->hipos[r];
+// the pairs of a record's suffix, and L2 prefetch of them by the record's lane k
+__device__ __forceinline__ void prefetch_suffix(const int32_t *__restrict__ col, int4 r4, int k, int S) {
+  if (!XT_L2_PREFETCH || r4.z <= 0) return;
+  const int64_t s = int64_t(uint32_t(r4.x)) | (int64_t(r4.y) << 32);
+  const int64_t p0 = s >> 3, np = ((s & 7) + r4.z + 7) >> 3;
+  // lane k takes pieces k, k+S, ... of up to 4 KiB (128 pairs)
+  for (int64_t q = int64_t(k) * 128; q < np; q += int64_t(S) * 128) {
+    const int64_t n = np - q < 128 ? np - q : 128;
+    prefetch_l2(reinterpret_cast<const int4 *>(col) + 2 * (p0 + q), uint32_t(n * 32));
   }
+}
 
-  __device__ __forceinline__ int32_t claim() {
+// keeps the columns i with lo <= i < hi
+__device__ __forceinline__ void mask_pair(int4 &a, int4 &b, int32_t lo, int32_t hi) {
+  int32_t *x = reinterpret_cast<int32_t *>(&a);
+  int32_t *y = reinterpret_cast<int32_t *>(&b);
+#pragma unroll
+  for (int i = 0; i < 4; i++) {
+    if (uint32_t(i - lo) >= uint32_t(hi - lo)) x[i] = kSentinel;
+    if (uint32_t(i + 4 - lo) >= uint32_t(hi - lo)) y[i] = kSentinel;
+  }
+}
+
+// bitmap membership: bit (w & 31) of word (w >> 5) - base; every w outside
+// the bitmap's words lands on the zero guard word
+__device__ __forceinline__ uint32_t bitmap_test(const Members &m, int32_t w) {
+  uint32_t i = uint32_t(w >> 5) - m.base;
+  i = i < m.nwords ? i : m.nwords;
+  const uint32_t x = uint32_t(m.words[i]);
+  return __funnelshift_r(x, x, uint32_t(w)) & 1u;
+}
+
+template <bool PV>
+__device__ __forceinline__ int hash_test(const Members &m, int32_t w) {
+  if (uint32_t(w - m.lo) > uint32_t(m.hi - m.lo)) return 0;  // sentinels too
+  const int slot = hash_find(m.words, m.mask, m.shift, w);
+  if (slot < 0) return 0;
+  if (PV) atomicAdd(&m.cnt[slot], 1);
+  return 1;
+}
+
+template <bool PV, bool BITMAP>
+__device__ __forceinline__ int probe_pair(const int4 a, const int4 b, const Members &m) {
+  if (BITMAP) {
+    return int((bitmap_test(m, a.x) + bitmap_test(m, a.y)) + (bitmap_test(m, a.z) + bitmap_test(m, a.w)) +
+               (bitmap_test(m, b.x) + bitmap_test(m, b.y)) + (bitmap_test(m, b.z) + bitmap_test(m, b.w)));
+  }
+  return hash_test<PV>(m, a.x) + hash_test<PV>(m, a.y) + hash_test<PV>(m, a.z) + hash_test<PV>(m, a.w) +
+         hash_test<PV>(m, b.x) + hash_test<PV>(m, b.y) + hash_test<PV>(m, b.z) + hash_test<PV>(m, b.w);
+}
+
+// Streams the suffixes of in-records [k0, kend) through the member set with
+// 2^lg_s lanes per record, in batches claimed from `cursor` (shared by the
+// warps of a CTA task) or taken in order (cursor null); returns this lane's
+// hits. Per-vertex mode credits each record's hits to its owner u.
+template <bool PV, bool BITMAP>
+__device__ __forceinline__ int64_t stream_kind(const InRec *__restrict__ rec, const int32_t *__restrict__ col,
+                                               int64_t k0, int64_t kend, int lg_s, int *cursor, const Members &m,
+                                               int64_t *__restrict__ pv, int lane) {
+  const int S = 1 << lg_s;
+  const int bsz = 32 >> lg_s;
+  const int j = lane >> lg_s, k = lane & (S - 1);
+  const int32_t nrec = int32_t(kend - k0);
+  rec += k0;
+  int32_t seq = 0;
+  auto claim = [&]() -> int32_t {
     if (!cursor) {
       const int32_t b = seq;
       seq += bsz;
@@ -315,175 +414,83 @@ struct FlatWalk {
     int c = 0;
     if (lane == 0) c = atomicAdd(cursor, bsz);
     return __shfl_sync(0xffffffffu, c, 0);
-  }
-  __device__ __forceinline__ int4 fetch(int32_t base) const {
-    const int32_t k = base + lane;
-    return (lane < bsz && k < kend) ? __ldg(reinterpret_cast<const int4 *>(rec) + k) : make_int4(0, 0, 0, -1);
-  }
-  // per-vertex mode: credit the finished batch's suffix owners
-  __device__ __forceinline__ void flush() {
-    if (PV && nb > 0) {
-      __syncwarp();
-      if (lane < nb && bv->hits[lane])
-        atomicAdd(reinterpret_cast<unsigned long long *>(&pv[bv->u[lane]]), (unsigned long long)bv->hits[lane]);
-    }
-  }
-  // lays the batch whose records are in lane registers r4 out in shared memory
-  __device__ __forceinline__ void take(int4 r4) {
-    flush();
-    const int64_t s = int64_t(uint32_t(r4.x)) | (int64_t(r4.y) << 32);
-    const uint32_t len = uint32_t(r4.z);
-    const int64_t g0 = s >> 2;
-    const uint32_t ng = (len > 0) ? uint32_t(((s + len + 3) >> 2) - g0) : 0u;
-    uint32_t incl = ng;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      const uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
-      if (lane >= o) incl += t;
-    }
-    total = __shfl_sync(0xffffffffu, incl, 31);
-    __syncwarp();  // every lane is done reading the previous batch
-    const uint32_t st = incl - ng;
-    bv->start[lane] = st;
-    if (lane == 31) bv->start[32] = incl;
-    bv->gbase[lane] = g0 - int64_t(st);
-    bv->lopos[lane] = 4u * st + uint32_t(s & 3);
-    bv->hipos[lane] = 4u * st + uint32_t(s & 3) + len;
-    if (PV) {
-      bv->u[lane] = r4.w;
-      bv->hits[lane] = 0;
-    }
-    __syncwarp();
-    nb = (kend - kb < bsz) ? (kend - kb) : bsz;
-    F = 0;
-    r = 0;
-    load_suffix();
-    nkb = claim();
-    nrec = fetch(nkb);
-  }
-  __device__ __forceinline__ void init() {
-    nb = 0;
-    seq = 0;
-    kb = claim();
-    have = kb < kend;
-    if (have) take(fetch(kb));
-  }
-  __device__ __forceinline__ Chunk issue() {
-    Chunk c;
-    while (have && F >= total) {  // batch exhausted: move to the next one
-      kb = nkb;
-      if (kb >= kend) {
-        flush();
-        have = false;
-        break;
-      }
-      take(nrec);
-    }
-    c.exists = have;
-#pragma unroll
-    for (int q = 0; q < kStepGroups; q++) {
-      c.x[q] = make_int4(0, 0, 0, 0);
-      c.vm[q] = 0;  // lanes past the batch probe nothing
-      c.rj[q] = 0;
-    }
-    if (!have) return c;
-    // this lane's kStepGroups consecutive groups: usually one suffix, so the
-    // layout read from shared memory is reused from the previous group
-#pragma unroll
-    for (int q = 0; q < kStepGroups; q++) {
-      const uint32_t f = F + uint32_t(kStepGroups * lane + q);
-      if (f < total) {
-        if (f >= c_end) {
-          do r++;
-          while (bv->start[r + 1] <= f);
-          load_suffix();
-        }
-        c.x[q] = __ldg(reinterpret_cast<const int4 *>(col) + (int64_t(f) + c_gb));
-        c.vm[q] = valid_mask(4u * f, c_lo, c_hi);
-        c.rj[q] = r;
-      }
-    }
-    F += 32 * kStepGroups;
-    return c;
-  }
-};
-
-// Probes one group; returns the hits. A candidate outside
-// [min N+(v), max N+(v)] is rejected by one unsigned compare.
-template <bool PV, bool BITMAP>
-__device__ __forceinline__ int probe_group(int4 x4, uint32_t vm, const Members &m) {
-  int h = 0;
-  const int32_t w[4] = {x4.x, x4.y, x4.z, x4.w};
-  const uint32_t span = uint32_t(m.hi - m.lo);
-#pragma unroll
-  for (int i = 0; i < 4; i++) {
-    const uint32_t d = uint32_t(w[i] - m.lo);
-    const bool ok = ((vm >> i) & 1u) && d <= span;
-    if (BITMAP) {
-      // branch-free: an invalid candidate reads word 0 and is masked out
-      const uint32_t word = uint32_t(m.words[ok ? (d >> 5) : 0u]);
-      h += int((word >> (d & 31)) & uint32_t(ok));
-    } else if (ok) {
-      const int slot = hash_find(m.words, m.mask, m.shift, w[i]);
-      if (slot >= 0) {
-        h++;
-        if (PV) atomicAdd(&m.cnt[slot], 1);
-      }
-    }
-  }
-  return h;
-}
-
-// Streams the suffixes of in-records [k0, kend) in batches of bsz records
-// (claimed from `cursor` when it is not null) through the member set;
-// returns this lane's hit count.
-template <bool PV, bool BITMAP>
-__device__ __forceinline__ int64_t stream_kind(const InRec *__restrict__ rec, const int32_t *__restrict__ col,
-                                               int64_t k0, int64_t kend, int bsz, int *cursor, const Members &m,
-                                               BatchView *bv, int64_t *__restrict__ pv, int lane) {
-  FlatWalk<PV> wk;
-  wk.rec = rec + k0;
-  wk.col = col;
-  wk.pv = pv;
-  wk.bv = bv;
-  wk.cursor = cursor;
-  wk.kend = int32_t(kend - k0);
-  wk.bsz = bsz;
-  wk.lane = lane;
-  wk.init();
+  };
+  auto fetch = [&](int32_t base) -> int4 {
+    const int32_t r = base + j;
+    return r < nrec ? __ldg(reinterpret_cast<const int4 *>(rec) + r) : make_int4(0, 0, 0, -1);
+  };
+  // records are loaded two batches ahead and their suffixes sent to L2 one
+  // batch ahead
+  int32_t kb = claim();
+  int4 r4 = fetch(kb);
+  int32_t nkb = claim();
+  int4 n4 = fetch(nkb);
+  prefetch_suffix(col, r4, k, S);
   int64_t hits = 0;
-  Chunk a = wk.issue();
-  while (a.exists) {
-    Chunk b;
-    if (PV) {
-      // credit a's suffixes before the next issue may lay a new batch (and
-      // flush the credits) over their slots
-#pragma unroll
-      for (int q = 0; q < kStepGroups; q++) {
-        const int h = probe_group<PV, BITMAP>(a.x[q], a.vm[q], m);
-        if (h) atomicAdd(&bv->hits[a.rj[q]], h);
-        hits += h;
+  while (kb < nrec) {  // warp-uniform
+    const int32_t nnkb = claim();
+    const int4 nn4 = fetch(nnkb);
+    prefetch_suffix(col, n4, k, S);
+    const int64_t s = int64_t(uint32_t(r4.x)) | (int64_t(r4.y) << 32);
+    const int32_t sr = int32_t(s & 7);  // suffix [sr, er) relative to its first pair
+    const int32_t er = sr + r4.z;
+    const int32_t np = r4.z > 0 ? (er + 7) >> 3 : 0;
+    const int32_t cnt = np > k ? ((np - k + S - 1) >> lg_s) : 0;  // this lane's pairs
+    const int32_t steps = int32_t(__reduce_max_sync(0xffffffffu, uint32_t(cnt)));
+    // steps from `clean` on may hold a lane's last pair (or none)
+    const int32_t clean = int32_t(__reduce_min_sync(0xffffffffu, uint32_t(cnt))) - 1;
+    int64_t P = (s >> 3) + k;
+    int32_t q = 8 * k;  // this lane's pair, relative to the suffix's first pair
+    int4 xa = make_int4(0, 0, 0, 0), xb = xa;
+    if (cnt > 0) load_pair(col, P, xa, xb);
+    int h = 0;
+#if XT_PF_DEPTH >= 2
+    int4 ya = xa, yb = xa;
+    if (cnt > 1) load_pair(col, P + S, ya, yb);
+#pragma unroll 2
+#endif
+    for (int32_t it = 0; it < steps; it++) {
+      int4 a = xa, b = xb;
+      const int32_t cq = q;
+      P += S;
+      q += 8 * S;
+#if XT_PF_DEPTH >= 2
+      xa = ya;
+      xb = yb;
+      if (it + 2 < cnt) load_pair(col, P + S, ya, yb);  // two steps ahead
+#else
+      if (it + 1 < cnt) load_pair(col, P, xa, xb);  // next step's pair in flight during the probes
+#endif
+      if (it == 0 || it >= clean) {
+        const bool act = it < cnt;
+        mask_pair(a, b, act ? sr - cq : 0, act ? er - cq : 0);
       }
-      b = wk.issue();
-    } else {
-      b = wk.issue();  // the next step's loads are in flight during these probes
-      int h = 0;
-#pragma unroll
-      for (int q = 0; q < kStepGroups; q++) h += probe_group<PV, BITMAP>(a.x[q], a.vm[q], m);
-      hits += h;
+      h += probe_pair<PV, BITMAP>(a, b, m);
     }
-    a = b;
+    if (PV) {
+      int hr = h;
+#pragma unroll
+      for (int o = 16; o; o >>= 1)
+        if (o < S) hr += __shfl_down_sync(0xffffffffu, hr, o, S);
+      if (k == 0 && hr && r4.w >= 0)
+        atomicAdd(reinterpret_cast<unsigned long long *>(&pv[r4.w]), (unsigned long long)hr);
+    }
+    hits += h;
+    kb = nkb;
+    r4 = n4;
+    nkb = nnkb;
+    n4 = nn4;
   }
   return hits;
 }
 
 template <bool PV>
 __device__ __forceinline__ int64_t stream_suffixes(const InRec *__restrict__ rec, const int32_t *__restrict__ col,
-                                                   int64_t k0, int64_t kend, int bsz, int *cursor, const Members &m,
-                                                   BatchView *bv, int64_t *__restrict__ pv, int lane) {
+                                                   int64_t k0, int64_t kend, int lg_s, int *cursor, const Members &m,
+                                                   int64_t *__restrict__ pv, int lane) {
   // the membership kind is fixed per task: one specialised loop each
-  if (m.bitmap) return stream_kind<PV, true>(rec, col, k0, kend, bsz, cursor, m, bv, pv, lane);
-  return stream_kind<PV, false>(rec, col, k0, kend, bsz, cursor, m, bv, pv, lane);
+  if (m.bitmap) return stream_kind<PV, true>(rec, col, k0, kend, lg_s, cursor, m, pv, lane);
+  return stream_kind<PV, false>(rec, col, k0, kend, lg_s, cursor, m, pv, lane);
 }
 
 // ---- the count kernel ---------------------------------------------------------
@@ -493,11 +500,13 @@ struct CountArgs {
   const int32_t *col;
   const int64_t *ioff;
   const InRec *rec;
-  const int64_t *bt;  // CTA tasks
+  const Task *bt;  // CTA tasks
   int64_t n_bt;
-  const int32_t *wt;  // warp tasks
+  const Task *wt;  // warp tasks
   int64_t n_wt;
-  unsigned long long *cursor;     // [0] CTA cursor, [1] warp cursor
+  const int32_t *tt;  // lane tasks (heads)
+  int64_t n_tt;
+  unsigned long long *cursor;     // [0] CTA, [1] warp, [2] lane task cursors
   unsigned long long *global;     // the total
   int64_t *pv;                    // per-vertex counts (per-vertex mode)
   const int32_t *group;           // head -> group (a graph of a batch), or null
@@ -511,59 +520,115 @@ __device__ __forceinline__ void credit_group(const CountArgs &a, int64_t v, int6
   if (lane == 0 && h) atomicAdd(&a.group_out[a.group[v]], (unsigned long long)h);
 }
 
+__device__ __forceinline__ void cp_async16(void *smem_dst, const void *gsrc) {
+  const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(smem_dst));
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(gsrc) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
+// Task staging: the next task's descriptor is claimed and its members copied
+// into shared memory (cp.async) and its in-records sent to L2 while the
+// current task streams, so a task starts without a round trip to memory.
+constexpr int kStageCta = kBlockDmax + 8;   // members, from r0 rounded down to 4 columns
+constexpr int kStageWarp = kWarpDmax + 8;
+constexpr int kStageInts = (kStageCta > kWarps * kStageWarp) ? kStageCta : kWarps * kStageWarp;
+
+// the next task from `cursor` (warp-uniform); nrec = -1 when none is left
+__device__ __forceinline__ Task claim_task(unsigned long long *cursor, const Task *__restrict__ tasks, int64_t n,
+                                           int lane) {
+  unsigned long long i = 0;
+  if (lane == 0) i = atomicAdd(cursor, 1ull);
+  i = __shfl_sync(0xffffffffu, i, 0);
+  if (int64_t(i) >= n) {
+    Task t;
+    t.k0 = t.r0 = 0;
+    t.v = t.nmem = t.lg_s = 0;
+    t.nrec = -1;
+    return t;
+  }
+  return tasks[i];
+}
+
+// one warp: copies the task's members into stage and prefetches its records
+// to L2; returns where the members start in stage
+__device__ __forceinline__ int stage_task(int32_t *stage, const int32_t *__restrict__ col,
+                                          const InRec *__restrict__ rec, const Task &t, int lane) {
+  if (t.nrec < 0) return 0;
+  const int64_t a0 = t.r0 & ~int64_t(3);
+  const int nchunk = int((t.r0 + t.nmem - a0 + 3) >> 2);  // reads stay inside the column padding
+  for (int i = lane; i < nchunk; i += 32) cp_async16(stage + 4 * i, col + a0 + 4 * i);
+  cp_async_commit();
+  const int64_t bytes = int64_t(t.nrec) * int64_t(sizeof(InRec));
+  for (int64_t q = int64_t(lane) << 16; q < bytes; q += int64_t(32) << 16)
+    prefetch_l2(reinterpret_cast<const char *>(rec + t.k0) + q, uint32_t(bytes - q < 65536 ? bytes - q : 65536));
+  return int(t.r0 - a0);
+}
+
+// clears the first nclear words of the member set (thread t of nt)
+template <bool PV>
+__device__ __forceinline__ void clear_members(const Members &m, int nclear, int t, int nt) {
+  for (int i = t; i < nclear; i += nt) {
+    m.words[i] = m.bitmap ? 0 : kEmpty;
+    if (PV) m.cnt[i] = 0;
+  }
+}
+
 template <bool PV>
 __global__ void __launch_bounds__(kThreads, kMinBlocks) k_count(const CountArgs a) {
   const int64_t *__restrict__ off = a.off;
   const int32_t *__restrict__ col = a.col;
   const int64_t *__restrict__ ioff = a.ioff;
   const InRec *__restrict__ rec = a.rec;
-  const int64_t *__restrict__ bt = a.bt;
-  const int32_t *__restrict__ wt = a.wt;
-  const int64_t n_bt = a.n_bt, n_wt = a.n_wt;
   unsigned long long *__restrict__ cursor = a.cursor;
   int64_t *__restrict__ pv = a.pv;
   extern __shared__ int32_t smem[];
-  int32_t *bwords = smem;                                   // kBlockWords
-  int32_t *bcnt = smem + kBlockWords;                       // kBlockWords (PV only)
-  int32_t *wwords_all = smem + (PV ? 2 : 1) * kBlockWords;  // kWarps * kWarpWords
-  int32_t *wcnt_all = wwords_all + kWarps * kWarpWords;     // (PV only)
-  __shared__ int64_t s_task;
+  int32_t *bwords = smem;               // kBlockWords
+  int32_t *bcnt = smem + kBlockWords;   // kBlockWords (per-vertex mode only)
+  __shared__ __align__(16) int32_t s_stage[kStageInts];
+  __shared__ Task s_task[2];
+  __shared__ int s_soff[2];
   __shared__ int s_batch;  // next in-record batch of the current CTA task
   __shared__ unsigned long long s_red[kWarps];
-  __shared__ BatchView s_bv[kWarps];
 
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   int64_t acc = 0;
 
   // ---- CTA tasks ----
-  while (true) {
-    if (tid == 0) {
-      s_task = int64_t(atomicAdd(&cursor[0], 1ull));
-      s_batch = 0;
+  if (warp == 0) {
+    const Task t0 = claim_task(&cursor[0], a.bt, a.n_bt, lane);
+    const int so = stage_task(s_stage, col, rec, t0, lane);
+    if (lane == 0) {
+      s_task[0] = t0;
+      s_soff[0] = so;
     }
+  }
+  for (int cur = 0;; cur ^= 1) {
+    if (warp == 0) cp_async_wait_all();
+    if (tid == 0) s_batch = 0;
     __syncthreads();
-    const int64_t t = s_task;
-    if (t >= n_bt) break;
-    const int64_t v = bt[4 * t], part = bt[4 * t + 1], k0 = bt[4 * t + 2], k1 = bt[4 * t + 3];
-    const int64_t r0 = off[v] + part * kBlockDmax;
-    const int64_t r1 = min(off[v + 1], r0 + kBlockDmax);
+    const Task t = s_task[cur];
+    if (t.nrec < 0) break;
+    const int32_t *mem = s_stage + s_soff[cur];
     Members m;
     m.words = bwords;
     m.cnt = bcnt;
-    const int nclear = members_layout<PV>(m, col, r0, r1, kBlockWords, a.bitmap_bits);
-    for (int i = tid; i < nclear; i += kThreads) {
-      bwords[i] = m.bitmap ? 0 : kEmpty;
-      if (PV) bcnt[i] = 0;
+    const int nclear = members_layout<PV>(m, mem, t.nmem, kBlockWords, a.bitmap_bits);
+    clear_members<PV>(m, nclear, tid, kThreads);
+    __syncthreads();
+    for (int i = tid; i < t.nmem; i += kThreads) members_insert(m, mem[i]);
+    __syncthreads();
+    if (warp == 0) {  // stage is free again: bring in the next task
+      const Task tn = claim_task(&cursor[0], a.bt, a.n_bt, lane);
+      const int so = stage_task(s_stage, col, rec, tn, lane);
+      if (lane == 0) {
+        s_task[cur ^ 1] = tn;
+        s_soff[cur ^ 1] = so;
+      }
     }
-    __syncthreads();
-    for (int64_t p = r0 + tid; p < r1; p += kThreads) members_insert(m, col[p]);
-    __syncthreads();
-    // batches small enough that every warp gets several of them
-    int64_t bsz = (k1 - k0) / (4 * kWarps);
-    bsz = bsz < 1 ? 1 : (bsz > 32 ? 32 : bsz);
-    int64_t h = stream_suffixes<PV>(rec, col, k0, k1, int(bsz), &s_batch, m, &s_bv[warp], pv, lane);
+    int64_t h = stream_suffixes<PV>(rec, col, t.k0, t.k0 + t.nrec, t.lg_s, &s_batch, m, pv, lane);
     acc += h;
-    if (a.group) credit_group(a, v, h, lane);
+    if (a.group) credit_group(a, t.v, h, lane);
     if (PV) {
       for (int o = 16; o; o >>= 1) h += __shfl_xor_sync(0xffffffffu, h, o);
       if (lane == 0) s_red[warp] = (unsigned long long)h;
@@ -573,46 +638,91 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) k_count(const CountArgs 
       if (tid == 0) {
         unsigned long long tot = 0;
         for (int w = 0; w < kWarps; w++) tot += s_red[w];
-        if (tot) atomicAdd(reinterpret_cast<unsigned long long *>(&pv[v]), tot);
+        if (tot) atomicAdd(reinterpret_cast<unsigned long long *>(&pv[t.v]), tot);
       }
       for (int i = tid; i < nclear; i += kThreads)
-        if (bcnt[i]) atomicAdd(reinterpret_cast<unsigned long long *>(&pv[bwords[i]]), (unsigned long long)bcnt[i]);
+          if (bcnt[i]) atomicAdd(reinterpret_cast<unsigned long long *>(&pv[bwords[i]]), (unsigned long long)bcnt[i]);
       __syncthreads();
     }
   }
 
-  // ---- warp tasks ----
-  int32_t *wwords = wwords_all + warp * kWarpWords;
-  int32_t *wcnt = wcnt_all + warp * kWarpWords;
-  while (true) {
-    int64_t t = 0;
-    if (lane == 0) t = int64_t(atomicAdd(&cursor[1], 1ull));
-    t = __shfl_sync(0xffffffffu, t, 0);
-    if (t >= n_wt) break;
-    const int32_t v = wt[t];
-    const int64_t r0 = off[v], r1 = off[v + 1];
-    Members m;
-    m.words = wwords;
-    m.cnt = wcnt;
-    const int nclear = members_layout<PV>(m, col, r0, r1, kWarpWords, a.bitmap_bits);
-    for (int i = lane; i < nclear; i += 32) {
-      wwords[i] = m.bitmap ? 0 : kEmpty;
-      if (PV) wcnt[i] = 0;
-    }
-    __syncwarp();
-    for (int64_t p = r0 + lane; p < r1; p += 32) members_insert(m, col[p]);
-    __syncwarp();
-    int64_t h = stream_suffixes<PV>(rec, col, ioff[v], ioff[v + 1], 32, nullptr, m, &s_bv[warp], pv, lane);
-    acc += h;
-    if (a.group) credit_group(a, v, h, lane);
-    if (PV) {
-      for (int o = 16; o; o >>= 1) h += __shfl_xor_sync(0xffffffffu, h, o);
+  // ---- warp tasks: the CTA region split among the warps ----
+  {
+    int32_t *wstage = s_stage + warp * kStageWarp;
+    Task t = claim_task(&cursor[1], a.wt, a.n_wt, lane);
+    int so = stage_task(wstage, col, rec, t, lane);
+    while (true) {
+      cp_async_wait_all();
       __syncwarp();
-      if (lane == 0 && h) atomicAdd(reinterpret_cast<unsigned long long *>(&pv[v]), (unsigned long long)h);
-      for (int i = lane; i < nclear; i += 32)
-        if (wcnt[i]) atomicAdd(reinterpret_cast<unsigned long long *>(&pv[wwords[i]]), (unsigned long long)wcnt[i]);
+      if (t.nrec < 0) break;
+      const int32_t *mem = wstage + so;
+      Members m;
+      m.words = bwords + warp * kWarpWords;
+      m.cnt = bcnt + warp * kWarpWords;
+      const int nclear = members_layout<PV>(m, mem, t.nmem, kWarpWords, a.bitmap_bits);
+      clear_members<PV>(m, nclear, lane, 32);
+      __syncwarp();
+      for (int i = lane; i < t.nmem; i += 32) members_insert(m, mem[i]);
+      __syncwarp();
+      const Task tn = claim_task(&cursor[1], a.wt, a.n_wt, lane);  // read after the stream
+      int64_t h = stream_suffixes<PV>(rec, col, t.k0, t.k0 + t.nrec, t.lg_s, nullptr, m, pv, lane);
+      acc += h;
+      if (a.group) credit_group(a, t.v, h, lane);
+      if (PV) {
+        for (int o = 16; o; o >>= 1) h += __shfl_xor_sync(0xffffffffu, h, o);
+        __syncwarp();
+        if (lane == 0 && h) atomicAdd(reinterpret_cast<unsigned long long *>(&pv[t.v]), (unsigned long long)h);
+        for (int i = lane; i < nclear; i += 32)
+          if (m.cnt[i])
+            atomicAdd(reinterpret_cast<unsigned long long *>(&pv[m.words[i]]), (unsigned long long)m.cnt[i]);
+      }
+      __syncwarp();
+      so = stage_task(wstage, col, rec, tn, lane);
+      t = tn;
     }
-    __syncwarp();
+  }
+
+  // ---- lane tasks: one small head per lane, members binary-searched ----
+  while (true) {
+    unsigned long long base = 0;
+    if (lane == 0) base = atomicAdd(&cursor[2], 32ull);
+    base = __shfl_sync(0xffffffffu, base, 0);
+    if (int64_t(base) >= a.n_tt) break;
+    const int64_t i = int64_t(base) + lane;
+    if (i >= a.n_tt) continue;
+    const int32_t v = a.tt[i];
+    const int64_t r0 = off[v], r1 = off[v + 1];
+    const int32_t lo = col[r0], hi = col[r1 - 1];
+    int64_t hv = 0;
+    for (int64_t k = ioff[v]; k < ioff[v + 1]; k++) {
+      const InRec r = rec[k];
+      int64_t b = r0;  // members below b are below every remaining candidate
+      int32_t hu = 0;
+      for (int64_t p = r.s; p < r.s + r.len; p++) {
+        const int32_t w = col[p];
+        if (w > hi) break;  // the suffix ascends
+        if (w < lo) continue;
+        int64_t x = b, y = r1;
+        while (x < y) {
+          const int64_t mid = (x + y) >> 1;
+          if (col[mid] < w) x = mid + 1;
+          else y = mid;
+        }
+        b = x;
+        if (col[x] == w) {  // x < r1: w <= hi
+          hu++;
+          if (PV) atomicAdd(reinterpret_cast<unsigned long long *>(&pv[w]), 1ull);
+          b = x + 1;
+        }
+      }
+      hv += hu;
+      if (PV && hu) atomicAdd(reinterpret_cast<unsigned long long *>(&pv[r.u]), (unsigned long long)hu);
+    }
+    acc += hv;
+    if (hv) {
+      if (PV) atomicAdd(reinterpret_cast<unsigned long long *>(&pv[v]), (unsigned long long)hv);
+      if (a.group) atomicAdd(&a.group_out[a.group[v]], (unsigned long long)hv);
+    }
   }
 
   // ---- reduce ----
@@ -627,9 +737,7 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) k_count(const CountArgs 
   }
 }
 
-static size_t count_smem_bytes(bool pv) {
-  return sizeof(int32_t) * size_t(pv ? 2 : 1) * (kBlockWords + kWarps * kWarpWords);
-}
+static size_t count_smem_bytes(bool pv) { return sizeof(int32_t) * size_t(pv ? 2 : 1) * kBlockWords; }
 
 // per-vertex counts in internal numbering -> input numbering
 __global__ void k_unpermute(const int64_t *__restrict__ in, const int32_t *__restrict__ n2o, int64_t nv,
@@ -669,6 +777,7 @@ void free_plan(Graph *g) {
   Ctx *c = g->ctx;
   dfree(c, g->plan->d_bt);
   dfree(c, g->plan->d_wt);
+  dfree(c, g->plan->d_tt);
   dfree(c, g->plan->d_cursor);
   delete g->plan;
   g->plan = nullptr;
@@ -685,11 +794,12 @@ xt_status make_plan(Graph *g) {
   g->plan = pl;
   const int64_t nv = g->nv, ne = g->ne;
   const int B = 256;
-  int64_t *w = nullptr, *P = nullptr, *nb = nullptr, *nw = nullptr, *nbp = nullptr, *nwp = nullptr;
+  int64_t *w = nullptr, *P = nullptr, *nb = nullptr, *nw = nullptr, *nt = nullptr, *nbp = nullptr, *nwp = nullptr,
+          *ntp = nullptr;
   unsigned long long *stats = nullptr;
   xt_status s = XT_OK;
   do {
-    if ((s = dalloc_n(c, &pl->d_cursor, 2)) != XT_OK) break;
+    if ((s = dalloc_n(c, &pl->d_cursor, 3)) != XT_OK) break;
     if ((s = dalloc_n(c, &stats, 4)) != XT_OK) break;
     if ((s = dalloc_n(c, &w, size_t(ne + 1))) != XT_OK) break;
     if ((s = dalloc_n(c, &P, size_t(ne + 1))) != XT_OK) break;
@@ -727,7 +837,14 @@ xt_status make_plan(Graph *g) {
     if ((s = cuda_status(c, cudaStreamSynchronize(c->stream), "sync")) != XT_OK) break;
     PlanParams pp;
     pp.warp_dmax = kWarpDmax;
+    // lane tasks trade latency (a lane's dependent loads set the kernel's
+    // tail) for throughput: only graphs with plenty of other work use them
+    pp.tiny_work = total_work >= (int64_t(1) << 30) ? XT_TINY_WORK : 0;
+    if (g->tier_lane_work >= 0) pp.tiny_work = g->tier_lane_work;
+    pp.batches_per_warp = XT_BATCHES_PER_WARP;
+    pp.lane_pairs = XT_LANE_PAIRS;
     pp.warp_work = g->tune_warp_work > 0 ? g->tune_warp_work : kWarpWork;
+    if (g->tier_warp_work >= 0) pp.warp_work = g->tier_warp_work;
     if (g->tune_block_work > 0) {
       pp.block_work = g->tune_block_work;
     } else {
@@ -741,34 +858,41 @@ xt_status make_plan(Graph *g) {
     if ((s = dalloc_n(c, &nw, size_t(nv + 1))) != XT_OK) break;
     if ((s = dalloc_n(c, &nbp, size_t(nv + 1))) != XT_OK) break;
     if ((s = dalloc_n(c, &nwp, size_t(nv + 1))) != XT_OK) break;
+    if ((s = dalloc_n(c, &nt, size_t(nv + 1))) != XT_OK) break;
+    if ((s = dalloc_n(c, &ntp, size_t(nv + 1))) != XT_OK) break;
     k_plan_count<<<counted(c, grid_for(nv, B, c->sm_count)), B, 0, c->stream>>>(nv, g->d_off, g->d_ioff, P, pp, nb,
-                                                                                nw);
+                                                                                nw, nt);
     if ((s = cuda_status(c, cudaMemsetAsync(nb + nv, 0, sizeof(int64_t), c->stream), "memset")) != XT_OK) break;
     if ((s = cuda_status(c, cudaMemsetAsync(nw + nv, 0, sizeof(int64_t), c->stream), "memset")) != XT_OK) break;
+    if ((s = cuda_status(c, cudaMemsetAsync(nt + nv, 0, sizeof(int64_t), c->stream), "memset")) != XT_OK) break;
     if ((s = exclusive_scan(c, nb, nbp, nv + 1)) != XT_OK) break;
     if ((s = exclusive_scan(c, nw, nwp, nv + 1)) != XT_OK) break;
-    int64_t h[3] = {0, 0, 0};
+    if ((s = exclusive_scan(c, nt, ntp, nv + 1)) != XT_OK) break;
+    int64_t h[4] = {0, 0, 0, 0};
     unsigned long long hs[4] = {0, 0, 0, 0};
     if ((s = d2h(c, &h[0], nbp + nv, sizeof(int64_t))) != XT_OK) break;
     if ((s = d2h(c, &h[1], nwp + nv, sizeof(int64_t))) != XT_OK) break;
     if ((s = d2h(c, &h[2], P + ne, sizeof(int64_t))) != XT_OK) break;
+    if ((s = d2h(c, &h[3], ntp + nv, sizeof(int64_t))) != XT_OK) break;
     if ((s = d2h(c, hs, stats, sizeof(hs))) != XT_OK) break;
     if ((s = cuda_status(c, cudaStreamSynchronize(c->stream), "sync")) != XT_OK) break;
     pl->n_btask = h[0];
     pl->n_wtask = h[1];
+    pl->n_ttask = h[3];
     g->max_degree = int64_t(hs[0]);
     g->max_out_degree = int64_t(hs[1]);
     g->max_in_degree = int64_t(hs[2]);
     g->wedge_work = tail_work;
     g->stream_work = h[2];
     if (g->max_out_degree >= kMaxOutDegree) {
-      s = set_error(c, XT_ERR_OVERFLOW, "an oriented out-degree of 2^27 or more is not supported");
+      s = set_error(c, XT_ERR_OVERFLOW, "an oriented out-degree of 2^30 or more is not supported");
       break;
     }
-    if ((s = dalloc_n(c, &pl->d_bt, size_t(4 * (pl->n_btask > 0 ? pl->n_btask : 1)))) != XT_OK) break;
+    if ((s = dalloc_n(c, &pl->d_bt, size_t(pl->n_btask > 0 ? pl->n_btask : 1))) != XT_OK) break;
     if ((s = dalloc_n(c, &pl->d_wt, size_t(pl->n_wtask > 0 ? pl->n_wtask : 1))) != XT_OK) break;
-    k_plan_fill<<<counted(c, grid_for(nv, B, c->sm_count)), B, 0, c->stream>>>(nv, g->d_off, g->d_ioff, P, pp, nbp,
-                                                                               nwp, pl->d_bt, pl->d_wt);
+    if ((s = dalloc_n(c, &pl->d_tt, size_t(pl->n_ttask > 0 ? pl->n_ttask : 1))) != XT_OK) break;
+    k_plan_fill<<<counted(c, grid_for(nv, B, c->sm_count)), B, 0, c->stream>>>(
+        nv, g->d_off, g->d_ioff, P, pp, nbp, nwp, ntp, pl->d_bt, pl->d_wt, pl->d_tt);
     if ((s = cuda_status(c, cudaGetLastError(), "k_plan_fill")) != XT_OK) break;
   } while (0);
   dfree(c, w);
@@ -777,6 +901,8 @@ xt_status make_plan(Graph *g) {
   dfree(c, nw);
   dfree(c, nbp);
   dfree(c, nwp);
+  dfree(c, nt);
+  dfree(c, ntp);
   dfree(c, stats);
   if (s != XT_OK) free_plan(g);
   return s;
@@ -786,7 +912,10 @@ xt_status count_graph(Graph *g, int64_t *d_global, int64_t *d_pv, int64_t *d_gro
   Ctx *c = g->ctx;
   if (!g->plan) XT_TRY(make_plan(g));
   Plan *pl = g->plan;
-  XT_CUDA(c, cudaMemsetAsync(pl->d_cursor, 0, 2 * sizeof(unsigned long long), c->stream));
+  // pairs of columns are read with 32-byte vector loads
+  if (reinterpret_cast<uintptr_t>(g->d_col) % 32 != 0)
+    return set_error(c, XT_ERR_CUDA, "column array is not 32-byte aligned");
+  XT_CUDA(c, cudaMemsetAsync(pl->d_cursor, 0, 3 * sizeof(unsigned long long), c->stream));
   XT_CUDA(c, cudaMemsetAsync(d_global, 0, sizeof(int64_t), c->stream));
   if (d_groups) {
     if (!g->d_group) return set_error(c, XT_ERR_INVALID, "per-group counts need a graph built as a batch");
@@ -807,6 +936,8 @@ xt_status count_graph(Graph *g, int64_t *d_global, int64_t *d_pv, int64_t *d_gro
   a.n_bt = pl->n_btask;
   a.wt = pl->d_wt;
   a.n_wt = pl->n_wtask;
+  a.tt = pl->d_tt;
+  a.n_tt = pl->n_ttask;
   a.cursor = pl->d_cursor;
   a.global = reinterpret_cast<unsigned long long *>(d_global);
   a.pv = pv_int;

@@ -93,6 +93,8 @@ struct Graph {
   int64_t tune_block_work = 0;  // schedule overrides (0: choose automatically)
   int64_t tune_warp_work = 0;
   int64_t tune_bitmap_bits = 0;
+  int64_t tier_lane_work = -1;  // tier limits (-1: automatic, 0: tier off)
+  int64_t tier_warp_work = -1;
   int32_t *d_group = nullptr;   // internal id -> group (graph of a batch), or null
   int64_t n_groups = 0;
   // a captured count (CUDA graph) writing the total and the per-group
