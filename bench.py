@@ -45,7 +45,10 @@ SCALE = 24
 EDGE_FACTOR = 16
 SEED = 1
 SAMPLE_SCALE = 18
-WORKLOAD = ("R-MAT scale 24, edge factor 16 (a=.57 b=.19 c=.19 d=.05, 10% per-level noise, ids permuted), "
+
+
+def workload_name(scale: int) -> str:
+    return (f"R-MAT scale {scale}, edge factor 16 (a=.57 b=.19 c=.19 d=.05, 10% per-level noise, ids permuted), "
             "symmetrised + deduped + loops dropped, degree-oriented, int32 cols / int64 offsets")
 
 
@@ -210,8 +213,8 @@ def run_reference_arm(args) -> None:
     print(json.dumps(line))
 
 
-def config_dict(world: int, info: dict | None) -> dict:
-    c = {"workload": WORKLOAD, "scale": SCALE, "edge_factor": EDGE_FACTOR, "seed": SEED, "orient": "degree",
+def config_dict(world: int, info: dict | None, scale: int = SCALE) -> dict:
+    c = {"workload": workload_name(scale), "scale": scale, "edge_factor": EDGE_FACTOR, "seed": SEED, "orient": "degree",
          "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
          "l2": "inputs larger than L2 (CSR + transpose > 2 GB), no flush"}
     if info:
@@ -235,11 +238,11 @@ def run_xtric(args) -> None:
     stream = torch.cuda.current_stream()
     ctx = xt.Context(local)
     ctx.set_stream(stream.cuda_stream)
-    n = 1 << SCALE
-    ne = EDGE_FACTOR << SCALE
+    n = 1 << args.scale
+    ne = EDGE_FACTOR << args.scale
     src = torch.empty(ne, dtype=torch.int32, device="cuda")
     dst = torch.empty_like(src)
-    ctx.gen_rmat(SCALE, ne, SEED, src, dst)
+    ctx.gen_rmat(args.scale, ne, SEED, src, dst)
     g = ctx.graph_from_device_edges(n, ne, src, dst, xt.ORIENT_DEGREE)
     info = g.info()
     d_count = torch.zeros(1, dtype=torch.int64, device="cuda")
@@ -308,12 +311,12 @@ def run_xtric(args) -> None:
 
     peaks = measured_peaks()
     achieved = info["alg_bytes"] / t_kernel / 1e9
-    traffic = profiled_traffic("k_count_rmat_s24.md")
+    traffic = profiled_traffic("k_count_rmat_s24.md") if args.scale == SCALE else None
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": 1e3 * t_max / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic",
-        "config": config_dict(world, info), "triangles": counts[0],
+        "config": config_dict(world, info, args.scale), "triangles": counts[0],
         "triangles_per_s": counts[0] * args.steps * world / t_max,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
                      "frac": achieved / peaks["hbm_gbs"], "traffic": traffic,
@@ -466,6 +469,9 @@ def main() -> None:
     ap.add_argument("--impl", choices=["xtric", "reference"], default="xtric")
     ap.add_argument("--workload", choices=["rmat24", "batch"], default="rmat24",
                     help="rmat24: the headline single-graph count; batch: the batching form")
+    ap.add_argument("--scale", type=int, default=SCALE,
+                    help="R-MAT scale of the single-graph workload (24 is the headline; smaller scales are the "
+                         "small cases that profiler captures run on)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)  # timing rule: at least 3 untimed warm-up steps
