@@ -460,6 +460,134 @@ def run_batch(args) -> None:
     print(json.dumps(line))
 
 
+SERVE_WORKLOAD = ("count queries on R-MAT graphs (a=.57 b=.19 c=.19 d=.05, edge factor 16, 10% noise, ids "
+                  "permuted), scale uniform in {10..20} (log-uniform vertex count), Poisson arrivals; host edge "
+                  "lists (int32) copied in per query; degree-oriented")
+SERVE_RATES = (10, 30, 100, 300, 1000, 3000, 10000)
+SERVE_POOL = 48
+
+
+def _pct(xs, q):
+    return float(np.percentile(np.asarray(xs) * 1e3, q)) if len(xs) else None
+
+
+def run_serve(args) -> None:
+    """Serving form: Poisson arrival streams at several rates, served with
+    admission by memory budget and continuous batching (xt_serve_*), against
+    the plain per-query path (build + count per query, one at a time) under
+    the same arrivals. Every served count must equal the query's solo count."""
+    import torch
+
+    import xxtric_b200 as xt
+    from xxtric_b200 import replicas
+
+    rank, world, local = replicas.init(backend="nccl")
+    torch.cuda.set_device(local)
+    rng = np.random.default_rng(SEED + 5)
+    ctx = xt.Context(local)
+    pool = []  # (nv, pinned src, pinned dst)
+    for i in range(SERVE_POOL):
+        scale = int(rng.integers(10, 21))
+        ne = EDGE_FACTOR << scale
+        ds = torch.empty(ne, dtype=torch.int32, device="cuda")
+        dd = torch.empty_like(ds)
+        ctx.gen_rmat(scale, ne, 1000 + i, ds, dd)
+        hs = torch.empty(ne, dtype=torch.int32, pin_memory=True)
+        hd = torch.empty(ne, dtype=torch.int32, pin_memory=True)
+        hs.copy_(ds)
+        hd.copy_(dd)
+        pool.append((1 << scale, hs.numpy(), hd.numpy(), scale))
+    del ds, dd
+    torch.cuda.synchronize()
+
+    def plain_one(i):
+        nv, hs, hd, _ = pool[i]
+        g = ctx.graph_from_edges(nv, hs, hd)
+        t = g.count()
+        g.free()
+        return t
+
+    solo = [plain_one(i) for i in range(SERVE_POOL)]  # also warms the plain path
+    srv = xt.Server(local, budget_bytes=150 << 30, slots=3)
+    for i in range(SERVE_POOL):  # warm the server's slots and pool allocator
+        srv.wait(srv.submit(*pool[i][:3]))
+    st0 = srv.stats()
+    sweep = []
+    exact = True
+    l_plain0 = ctx.launches
+    for lam in SERVE_RATES:
+        n = int(min(600, max(30, 3 * lam)))
+        arr = np.cumsum(rng.exponential(1.0 / lam, n))
+        arr -= arr[0]
+        which = rng.integers(0, SERVE_POOL, n)
+        # served: submit on schedule, results timed by the server (submit -> result)
+        t0 = time.perf_counter()
+        sub = []
+        for k in range(n):
+            d = t0 + arr[k] - time.perf_counter()
+            if d > 0:
+                time.sleep(d)
+            ts = time.perf_counter()
+            sub.append((srv.submit(*pool[which[k]][:3]), ts))
+        lat, done = [], []
+        for k, (tk, ts) in enumerate(sub):
+            c, l = srv.wait(tk)
+            exact &= c == solo[which[k]]
+            lat.append(l)
+            done.append(ts + l)
+        served_s = max(done) - t0
+        bl = srv.batches()[-n:]
+        bl = [b for b in bl if b["take"] >= bl[-1]["take"] - served_s - 1.0]
+        # plain: one query at a time in arrival order, each waiting for the previous
+        t0 = time.perf_counter()
+        plat = []
+        for k in range(n):
+            d = t0 + arr[k] - time.perf_counter()
+            if d > 0:
+                time.sleep(d)
+            exact &= plain_one(which[k]) == solo[which[k]]
+            plat.append(time.perf_counter() - (t0 + arr[k]))
+        plain_s = time.perf_counter() - t0
+        edges = int(sum(len(pool[w][1]) for w in which))
+        sweep.append({"rate_per_s": lam, "queries": n, "edge_rows": edges,
+                      "served": {"p50_ms": _pct(lat, 50), "p99_ms": _pct(lat, 99), "graphs_per_s": n / served_s,
+                                 "batches": len(bl), "graphs_per_batch": float(np.mean([b["graphs"] for b in bl])),
+                                 "build_ms_mean": 1e3 * float(np.mean([b["built"] - b["take"] for b in bl])),
+                                 "count_ms_mean": 1e3 * float(np.mean([b["done"] - b["built"] for b in bl])),
+                                 "batch_ms_max": 1e3 * float(max(b["done"] - b["take"] for b in bl))},
+                      "plain": {"p50_ms": _pct(plat, 50), "p99_ms": _pct(plat, 99), "graphs_per_s": n / plain_s}})
+    st = srv.stats()
+    srv.close()
+    top = sweep[-1]
+    line = {
+        "metric": "graphs/s (served count queries, Poisson arrivals)", "value": top["served"]["graphs_per_s"],
+        "unit": "graphs/s", "n_gpus": world, "steps": len(SERVE_RATES), "warmup": 1,
+        "ms_per_step": 1e3 / top["served"]["graphs_per_s"], "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "int32", "data": "synthetic",
+        "config": {"workload": SERVE_WORKLOAD, "pool_graphs": SERVE_POOL,
+                   "pool_scales": [p[3] for p in pool], "rates_per_s": list(SERVE_RATES),
+                   "budget_bytes": st["budget_bytes"], "slots": 3, "seed": SEED,
+                   "l2": "inputs larger than L2 for the large queries; each query copied in from host memory"},
+        "sweep": sweep,
+        "e2e": {"value": top["served"]["graphs_per_s"], "unit": "graphs/s",
+                "h2d_bytes_per_step": 8 * top["edge_rows"], "d2h_bytes_per_step": 8 * top["queries"],
+                "note": "a step is one rate's stream; the served path is end to end by construction"},
+        "speedup_vs_plain_at_top_rate": top["served"]["graphs_per_s"] / top["plain"]["graphs_per_s"],
+        "counts_equal_solo": bool(exact),
+        "server": {k: st[k] - st0.get(k, 0) if k in ("submitted", "completed", "batches", "launches") else st[k]
+                   for k in ("submitted", "completed", "failed", "rejected", "batches", "max_batch", "budget_peak",
+                             "device_peak", "launches")},
+        "gpu_launches": st["launches"] - st0["launches"],
+        "plain_launches": ctx.launches - l_plain0,
+    }
+    ctx.close()
+    replicas.finish()
+    if rank == 0:
+        print(json.dumps(line))
+    if not exact:
+        raise SystemExit("served counts differ from the solo counts")
+
+
 def main() -> None:
     ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
     ap.add_argument("--gpus", type=int, default=1)
@@ -467,8 +595,9 @@ def main() -> None:
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--impl", choices=["xtric", "reference"], default="xtric")
-    ap.add_argument("--workload", choices=["rmat24", "batch"], default="rmat24",
-                    help="rmat24: the headline single-graph count; batch: the batching form")
+    ap.add_argument("--workload", choices=["rmat24", "batch", "serve"], default="rmat24",
+                    help="rmat24: the headline single-graph count; batch: the batching form; serve: the serving "
+                         "form (Poisson arrival sweep)")
     ap.add_argument("--scale", type=int, default=SCALE,
                     help="R-MAT scale of the single-graph workload (24 is the headline; smaller scales are the "
                          "small cases that profiler captures run on)")
@@ -479,6 +608,8 @@ def main() -> None:
         run_reference_arm(args)
     elif args.workload == "batch":
         run_batch(args)
+    elif args.workload == "serve":
+        run_serve(args)
     else:
         run_xtric(args)
 

@@ -86,6 +86,10 @@ xt_status xt_debug_fail_alloc(xt_ctx *ctx, int64_t k);
 /* number of this library's own kernels launched on the context so far
  * (library sorts and scans from CUB are not included) */
 int64_t xt_launch_count(const xt_ctx *ctx);
+/* device bytes this context's own allocations hold now (live) and at most
+ * since it opened or since the last reset (peak); reset_peak != 0 restarts
+ * the high-water mark at the live figure. No counterpart in the reference. */
+xt_status xt_mem_stats(xt_ctx *ctx, int64_t *live, int64_t *peak, int reset_peak);
 
 /* ---- graph build ---------------------------------------------------------
  * Replaces TriangleCountingSingle(Graph*) (xxtric-gpu.hpp:27-156): host CSR in
@@ -197,6 +201,76 @@ xt_status xt_batch_spec(int64_t n_graphs, uint64_t seed, int32_t *kind, int64_t 
 xt_status xt_gen_batch(xt_ctx *ctx, int64_t n_graphs, const int32_t *kind, const int64_t *n, const double *mean_deg,
                        const uint64_t *graph_seed, int64_t *edge_offsets, int32_t **d_src, int32_t **d_dst);
 xt_status xt_device_free(xt_ctx *ctx, void *p);
+
+/* ---- serving form -----------------------------------------------------------
+ * No counterpart in the reference, which counts one graph per process run.
+ * A server owns `slots` contexts (one CUDA stream and one host worker thread
+ * each) on one device. Count queries (host edge lists, graph-local int32
+ * ids) are admitted against a device-memory budget: each query's build and
+ * count hold at most xt_serve_estimate(nv, ne) bytes, and the queries in
+ * flight never hold more than the budget between them. Whenever a slot is
+ * free it takes every queued query that fits (first come first served, up to
+ * max_batch_graphs / max_batch_edges), builds them on the device as one
+ * batch and counts them in one launch; queries that arrive meanwhile wait
+ * only for the next free slot, and the slots' batches overlap on the device.
+ * Each query's count equals the count of its graph alone (xt_count). */
+typedef struct xt_server xt_server;
+typedef struct {
+  int64_t budget_bytes;     /* device bytes for queries in flight; <= 0: 150 GiB. Capped at the
+                               device's free memory at open, less 2 GiB */
+  int64_t max_batch_graphs; /* queries per batch, at most; <= 0: 4096 */
+  int64_t max_batch_edges;  /* edge rows per batch, at most (a larger query runs alone); <= 0: 2^26 */
+  int32_t slots;            /* batches in flight at once; <= 0: 3 */
+  int32_t orient;           /* xt_orient of every query */
+} xt_serve_config;
+typedef struct {
+  int64_t budget_bytes;     /* the budget in force */
+  int64_t submitted, completed, failed, rejected;
+  int64_t queued;           /* waiting for a slot */
+  int64_t in_flight;        /* admitted, result not yet published */
+  int64_t batches;          /* batches run */
+  int64_t max_batch;        /* most queries in one batch */
+  int64_t budget_used;      /* estimated bytes held by queries in flight now */
+  int64_t budget_peak;      /* ... and at most */
+  int64_t device_peak;      /* measured device bytes the slots' allocations held at most at once */
+  int64_t launches;         /* this library's kernels launched by the server */
+} xt_serve_stats;
+/* device bytes one query of nv vertices and ne edge rows may hold while it
+ * is built and counted (alone or in a batch: batch figures add up) */
+int64_t xt_serve_estimate(int64_t nv, int64_t ne);
+xt_status xt_serve_open(int device, const xt_serve_config *cfg, xt_server **out);
+/* Queues a count of the graph with nv vertices and ne rows (src[i], dst[i])
+ * (ids in [0, nv); rows may repeat or be loops). The buffers are read
+ * while the query runs: keep them unchanged until its result is taken
+ * (pinned host memory copies fastest). XT_ERR_ADMISSION when the query
+ * alone exceeds the budget, XT_ERR_CLOSED after xt_serve_close began. */
+xt_status xt_serve_submit(xt_server *srv, int64_t nv, int64_t ne, const int32_t *src, const int32_t *dst,
+                          int64_t *ticket);
+/* The query's result: XT_ERR_NOT_READY while it runs; otherwise its status
+ * (XT_OK with *count, or the error that failed it, e.g. XT_ERR_INVALID for
+ * an id outside [0, nv)) and the seconds from submit to result
+ * (latency_s, nullable). A result is returned once: the ticket is then
+ * forgotten (XT_ERR_INVALID afterwards). */
+xt_status xt_serve_poll(xt_server *srv, int64_t ticket, int64_t *count, double *latency_s);
+/* xt_serve_poll that blocks up to timeout_ms (< 0: no limit); XT_ERR_TIMEOUT
+ * when the result is still not there */
+xt_status xt_serve_wait(xt_server *srv, int64_t ticket, int64_t timeout_ms, int64_t *count, double *latency_s);
+xt_status xt_serve_get_stats(xt_server *srv, xt_serve_stats *stats);
+/* one batch the server ran: times in ns since xt_serve_open (taken from the
+ * queue, built and planned, results published) */
+typedef struct {
+  int64_t t_take_ns, t_built_ns, t_done_ns;
+  int64_t graphs, edge_rows;
+  int32_t slot;
+  int32_t status; /* xt_status of the batch (per-query retries not shown) */
+} xt_serve_batch;
+/* copies the most recent min(max, n) batch records (the server keeps the
+ * last 65,536) into out, oldest first; returns how many, or -1 */
+int64_t xt_serve_batches(xt_server *srv, xt_serve_batch *out, int64_t max);
+/* Stops admitting, fails the queued queries with XT_ERR_CLOSED, lets the
+ * batches in flight finish, joins the workers and frees everything; results
+ * not yet taken are lost. */
+xt_status xt_serve_close(xt_server *srv);
 
 /* ---- synthetic inputs on the device --------------------------------------
  * Deterministic counter-based generators (same bits for the same seed on any

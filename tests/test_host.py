@@ -41,6 +41,22 @@ def test_no_device_is_reported_not_faked():
     with pytest.raises(xt.XtError) as e:
         xt.Context(0)
     assert e.value.status == xt.XT_ERR_NO_DEVICE
+    with pytest.raises(xt.XtError) as e:
+        xt.Server(0)
+    assert e.value.status == xt.XT_ERR_NO_DEVICE
+
+
+def test_serve_estimate_is_linear_and_covers_the_build():
+    # admission figure: grows with both sizes, adds up over a batch, and is
+    # at least the bytes the builder's largest phase holds (8 B/row copied in,
+    # 8 B/row global ids, 16 B/row keys, 40 B per unique edge in the in-record sort)
+    e = xt.serve_estimate
+    assert e(-1, 0) < 0 and e(1, -1) < 0
+    base = e(0, 0)
+    assert 0 < base <= 8 << 20
+    for nv, ne in [(1 << 10, 16 << 10), (1 << 20, 16 << 20), (3, 0)]:
+        assert e(nv, ne) - base >= 72 * ne
+        assert e(2 * nv, 2 * ne) - base == 2 * (e(nv, ne) - base)
 
 
 @pytest.mark.parametrize("nprocs,radius", [(1, 0.0), (2, 0.0), (4, 0.0), (8, 0.0), (1, 0.03), (2, 0.02)])

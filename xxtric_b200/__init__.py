@@ -90,6 +90,15 @@ _proto("xt_count_groups_async", _int, _vp, _vp, _vp)
 _proto("xt_graph_capture", _int, _vp)
 _proto("xt_graph_set_tuning", _int, _vp, _i64, _i64, _i64)
 _proto("xt_graph_set_tiers", _int, _vp, _i64, _i64)
+_proto("xt_mem_stats", _int, _vp, _P(_i64), _P(_i64), _int)
+_proto("xt_serve_estimate", _i64, _i64, _i64)
+_proto("xt_serve_open", _int, _int, _vp, _P(_vp))
+_proto("xt_serve_submit", _int, _vp, _i64, _i64, _vp, _vp, _P(_i64))
+_proto("xt_serve_poll", _int, _vp, _i64, _P(_i64), _P(_dbl))
+_proto("xt_serve_wait", _int, _vp, _i64, _i64, _P(_i64), _P(_dbl))
+_proto("xt_serve_get_stats", _int, _vp, _vp)
+_proto("xt_serve_close", _int, _vp)
+_proto("xt_serve_batches", _i64, _vp, _vp, _i64)
 _proto("xt_graph_autotune", _int, _vp, _int, ctypes.c_char_p, _vp, _i64)
 _proto("xt_batch_spec", _int, _i64, _u64, _vp, _vp, _vp, _vp)
 _proto("xt_gen_batch", _int, _vp, _i64, _vp, _vp, _vp, _vp, _vp, _P(_vp), _P(_vp))
@@ -108,6 +117,8 @@ EXPORTED = ["xt_strerror", "xt_last_error", "xt_open", "xt_close", "xt_set_strea
             "xt_graph_get_csr", "xt_graph_free", "xt_count", "xt_count_async", "xt_count_device",
             "xt_count_device_static", "xt_graph_from_batch", "xt_graph_from_device_batch", "xt_graph_groups",
             "xt_count_groups", "xt_count_groups_async", "xt_graph_capture", "xt_graph_set_tuning", "xt_graph_set_tiers",
+            "xt_mem_stats", "xt_serve_estimate", "xt_serve_open", "xt_serve_submit", "xt_serve_poll",
+            "xt_serve_wait", "xt_serve_get_stats", "xt_serve_close", "xt_serve_batches",
             "xt_graph_autotune", "xt_batch_spec", "xt_gen_batch", "xt_device_free",
             "xt_gen_rmat", "xt_gen_chunglu", "xt_chunglu_cdf", "xt_gen_er", "xt_vite_read", "xt_vite_write",
             "xt_rgg_generate"]
@@ -259,6 +270,13 @@ class Context:
     def launches(self) -> int:
         """This library's kernels launched on the context so far."""
         return int(_L.xt_launch_count(self._h))
+
+    def mem_stats(self, reset_peak: bool = False) -> tuple[int, int]:
+        """(live, peak) device bytes of this context's own allocations."""
+        live, peak = _i64(0), _i64(0)
+        _check(_L.xt_mem_stats(self._h, ctypes.byref(live), ctypes.byref(peak), int(reset_peak)), "xt_mem_stats",
+               self)
+        return live.value, peak.value
 
     # -- graphs --
     def graph_from_csr(self, offsets: np.ndarray, tails: np.ndarray, canonical: bool = False,
@@ -465,3 +483,109 @@ class TriangleCountingSingle:
         if self.ctx is not None:
             self.ctx.close()
             self.ctx = None
+
+
+# ---------------------------------------------------------------------------
+# serving form
+# ---------------------------------------------------------------------------
+
+class ServeConfig(ctypes.Structure):
+    _fields_ = [("budget_bytes", _i64), ("max_batch_graphs", _i64), ("max_batch_edges", _i64),
+                ("slots", _i32), ("orient", _i32)]
+
+
+class ServeStats(ctypes.Structure):
+    _fields_ = [(k, _i64) for k in ("budget_bytes", "submitted", "completed", "failed", "rejected", "queued",
+                                    "in_flight", "batches", "max_batch", "budget_used", "budget_peak",
+                                    "device_peak", "launches")]
+
+    def as_dict(self) -> dict:
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class ServeBatch(ctypes.Structure):
+    _fields_ = [("t_take_ns", _i64), ("t_built_ns", _i64), ("t_done_ns", _i64), ("graphs", _i64),
+                ("edge_rows", _i64), ("slot", _i32), ("status", _i32)]
+
+
+def serve_estimate(nv: int, ne: int) -> int:
+    """Device bytes one query of nv vertices and ne edge rows may hold (admission figure)."""
+    return int(_L.xt_serve_estimate(nv, ne))
+
+
+class Server:
+    """Count queries admitted under a device-memory budget and batched as slots
+    free up (xt_serve_*). submit() returns a ticket; poll()/wait() return
+    (count, latency seconds) once, raising XtError for a failed query."""
+
+    def __init__(self, device: int = 0, budget_bytes: int = 0, slots: int = 0, orient: int = ORIENT_DEGREE,
+                 max_batch_graphs: int = 0, max_batch_edges: int = 0):
+        cfg = ServeConfig(budget_bytes, max_batch_graphs, max_batch_edges, slots, orient)
+        h = _vp()
+        s = _L.xt_serve_open(device, ctypes.byref(cfg), ctypes.byref(h))
+        if s != XT_OK:
+            raise XtError(s, f"xt_serve_open({device}): {strerror(s)}")
+        self._h = h.value
+        self._keep = {}  # ticket -> the host arrays the query reads until it finishes
+
+    def submit(self, nv: int, src: np.ndarray, dst: np.ndarray) -> int:
+        s_ = np.ascontiguousarray(src, np.int32)
+        d_ = np.ascontiguousarray(dst, np.int32)
+        if len(s_) != len(d_):
+            raise XtError(XT_ERR_INVALID, "src and dst differ in length")
+        t = _i64(0)
+        _check(_L.xt_serve_submit(self._h, nv, len(s_), _ptr(s_), _ptr(d_), ctypes.byref(t)), "xt_serve_submit")
+        self._keep[t.value] = (s_, d_)
+        return t.value
+
+    def _result(self, s: int, ticket: int, c, lat):
+        if s == XT_ERR_NOT_READY:
+            return None
+        self._keep.pop(ticket, None)
+        _check(s, f"query {ticket}")
+        return c.value, lat.value
+
+    def poll(self, ticket: int):
+        """(count, latency_s), or None while the query runs."""
+        c, lat = _i64(0), _dbl(0)
+        return self._result(_L.xt_serve_poll(self._h, ticket, ctypes.byref(c), ctypes.byref(lat)), ticket, c, lat)
+
+    def wait(self, ticket: int, timeout_ms: int = -1):
+        c, lat = _i64(0), _dbl(0)
+        s = _L.xt_serve_wait(self._h, ticket, timeout_ms, ctypes.byref(c), ctypes.byref(lat))
+        if s == XT_ERR_TIMEOUT:
+            raise XtError(s, f"query {ticket}: no result within {timeout_ms} ms")
+        return self._result(s, ticket, c, lat)
+
+    def stats(self) -> dict:
+        st = ServeStats()
+        _check(_L.xt_serve_get_stats(self._h, ctypes.byref(st)), "xt_serve_get_stats")
+        return st.as_dict()
+
+    def batches(self, max_n: int = 65536) -> list[dict]:
+        """The most recent batches: times (s since open), graphs, edge rows, slot, status."""
+        buf = (ServeBatch * max_n)()
+        n = _L.xt_serve_batches(self._h, buf, max_n)
+        if n < 0:
+            raise XtError(XT_ERR_INVALID, "xt_serve_batches")
+        return [{"take": b.t_take_ns * 1e-9, "built": b.t_built_ns * 1e-9, "done": b.t_done_ns * 1e-9,
+                 "graphs": b.graphs, "edge_rows": b.edge_rows, "slot": b.slot, "status": b.status}
+                for b in buf[:n]]
+
+    def close(self) -> None:
+        if self._h:
+            _L.xt_serve_close(self._h)
+            self._h = None
+            self._keep.clear()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -25,7 +25,7 @@ LIB = os.path.join(PKG, "libxtb200.so")
 CLI = os.path.join(PKG, "xtric")
 
 CUDA_SOURCES = ["csrc/capi.cu", "csrc/build.cu", "csrc/count.cu", "csrc/gen.cu", "csrc/count_static.cu",
-                "csrc/batch.cu"]
+                "csrc/batch.cu", "csrc/serve.cu"]
 HOST_SOURCES = ["host/host_io.cpp"]
 CLI_SOURCES = ["host/xtric_main.cpp"]
 HEADERS = ["csrc/xt_internal.cuh", "csrc/xt_rng.cuh", "../include/xtric.h", "host/xtric_host.hpp"]

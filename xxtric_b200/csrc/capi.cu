@@ -38,11 +38,27 @@ xt_status dalloc(Ctx *c, void **p, size_t bytes) {
     return set_error(c, XT_ERR_OOM,
                      "device allocation of " + std::to_string(bytes) + " bytes failed: " + cudaGetErrorString(e));
   }
+  c->live[*p] = bytes;
+  c->bytes_live += int64_t(bytes);
+  if (c->bytes_live > c->bytes_peak) c->bytes_peak = c->bytes_live;
+  if (c->shared_live) {
+    const int64_t v = c->shared_live->fetch_add(int64_t(bytes)) + int64_t(bytes);
+    int64_t pk = c->shared_peak->load();
+    while (v > pk && !c->shared_peak->compare_exchange_weak(pk, v)) {
+    }
+  }
   return XT_OK;
 }
 
 void dfree(Ctx *c, void *p) {
-  if (p) cudaFreeAsync(p, c->stream);
+  if (!p) return;
+  auto it = c->live.find(p);
+  if (it != c->live.end()) {
+    c->bytes_live -= int64_t(it->second);
+    if (c->shared_live) c->shared_live->fetch_sub(int64_t(it->second));
+    c->live.erase(it);
+  }
+  cudaFreeAsync(p, c->stream);
 }
 
 }  // namespace xt
@@ -138,6 +154,15 @@ xt_status xt_debug_fail_alloc(xt_ctx *ctx, int64_t k) {
 }
 
 int64_t xt_launch_count(const xt_ctx *ctx) { return ctx ? ctx->c.launches : -1; }
+
+xt_status xt_mem_stats(xt_ctx *ctx, int64_t *live, int64_t *peak, int reset_peak) {
+  if (!ctx) return XT_ERR_INVALID;
+  Ctx *c = &ctx->c;
+  if (live) *live = c->bytes_live;
+  if (peak) *peak = c->bytes_peak;
+  if (reset_peak) c->bytes_peak = c->bytes_live;
+  return XT_OK;
+}
 
 static xt_status finish_build(xt_ctx *ctx, xt_graph *gr, xt_status s, xt_graph **out) {
   Ctx *c = &ctx->c;

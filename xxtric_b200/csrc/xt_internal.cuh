@@ -4,7 +4,9 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <atomic>
 #include <string>
+#include <unordered_map>
 
 #include "../../include/xtric.h"
 
@@ -26,6 +28,12 @@ struct Ctx {
   // device-side error word reused by kernels that check their own inputs
   int *d_err = nullptr;
   int64_t launches = 0;  // kernels of this library launched on this context
+  // device bytes this context holds (its own allocations) and their high-water mark
+  std::unordered_map<void *, size_t> live;
+  int64_t bytes_live = 0, bytes_peak = 0;
+  // optional totals shared by several contexts (a server's slots): bytes live
+  // in all of them together and the high-water mark of that sum
+  std::atomic<int64_t> *shared_live = nullptr, *shared_peak = nullptr;
 };
 
 // Launch-configuration wrapper that counts the library's own kernel launches.
@@ -116,6 +124,11 @@ xt_status build_from_edges(Ctx *c, int64_t nv, int64_t ne, const int32_t *d_src,
 xt_status build_from_csr(Ctx *c, int64_t nv, const int64_t *d_off, const int64_t *d_tails, bool canonical,
                          int orient, Graph *g);
 void free_graph_device(Graph *g);
+
+// Builds the disjoint union of ng graphs (host offset tables, device edge
+// rows with graph-local ids) as one graph with a per-vertex group map.
+xt_status build_batch(Ctx *c, int64_t ng, const int64_t *h_voff, const int64_t *h_eoff, const int32_t *d_src,
+                      const int32_t *d_dst, int orient, Graph *g);
 
 // Builds (or rebuilds) the per-graph schedule and graph statistics.
 xt_status make_plan(Graph *g);
