@@ -37,8 +37,12 @@ static unsigned grid_for(int64_t n, int block, int sm_count) {
   for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < (n); i += int64_t(gridDim.x) * blockDim.x)
 
 // key = (min << b) | max; self loops keep min == max and are dropped later.
+// With deg != null, every non-loop row also counts one for each end: the
+// degree with repeated rows counted again, which orders the vertices as well
+// as the true degree does (any total order gives the same triangle count).
 __global__ void k_edge_keys(const int32_t *__restrict__ src, const int32_t *__restrict__ dst, int64_t ne,
-                            int64_t nv, int b, uint64_t *__restrict__ keys, int *__restrict__ err) {
+                            int64_t nv, int b, uint64_t *__restrict__ keys, int32_t *__restrict__ deg,
+                            int *__restrict__ err) {
   XT_GRID_STRIDE(i, ne) {
     int64_t s = src[i], d = dst[i];
     if (s < 0 || d < 0 || s >= nv || d >= nv) {
@@ -48,6 +52,10 @@ __global__ void k_edge_keys(const int32_t *__restrict__ src, const int32_t *__re
     }
     uint64_t lo = uint64_t(s < d ? s : d), hi = uint64_t(s < d ? d : s);
     keys[i] = (lo << b) | hi;
+    if (deg && lo != hi) {
+      atomicAdd(&deg[lo], 1);
+      atomicAdd(&deg[hi], 1);
+    }
   }
 }
 
@@ -57,15 +65,6 @@ __global__ void k_unique_flags(const uint64_t *__restrict__ keys, int64_t n, int
     uint64_t k = keys[i];
     bool first = (i == 0) || (keys[i - 1] != k);
     flags[i] = (first && ((k >> b) != (k & mask))) ? 1 : 0;
-  }
-}
-
-__global__ void k_degrees(const uint64_t *__restrict__ uniq, int64_t m, int b, int32_t *__restrict__ deg) {
-  const uint64_t mask = (uint64_t(1) << b) - 1;
-  XT_GRID_STRIDE(i, m) {
-    uint64_t k = uniq[i];
-    atomicAdd(&deg[k >> b], 1);
-    atomicAdd(&deg[k & mask], 1);
   }
 }
 
@@ -84,7 +83,7 @@ __global__ void k_rank_perm(const uint64_t *__restrict__ vk, int64_t nv, int32_t
   }
 }
 
-// unique (lo,hi) in input ids -> (src<<b|dst) in internal ids, src < dst
+// (lo,hi) in input ids -> (src<<b|dst) in internal ids, src <= dst
 __global__ void k_relabel_edges(uint64_t *__restrict__ keys, int64_t m, int b, const int32_t *__restrict__ o2n) {
   const uint64_t mask = (uint64_t(1) << b) - 1;
   XT_GRID_STRIDE(i, m) {
@@ -98,12 +97,13 @@ __global__ void k_relabel_edges(uint64_t *__restrict__ keys, int64_t m, int b, c
 // run's first key adds -start, the one at its last key adds end, so each
 // non-empty row ends with end - start (len must start zeroed). The offsets
 // are then the exclusive scan of the lengths.
-__global__ void k_csr_runs(const uint64_t *__restrict__ keys, int64_t m, int b, int64_t *__restrict__ len,
+template <class K>
+__global__ void k_csr_runs(const K *__restrict__ keys, int64_t m, int b, int64_t *__restrict__ len,
                            int32_t *__restrict__ col) {
-  const uint64_t mask = (uint64_t(1) << b) - 1;
+  const K mask = (K(1) << b) - 1;
   XT_GRID_STRIDE(i, m) {
-    const uint64_t k = keys[i];
-    const uint64_t row = k >> b;
+    const K k = keys[i];
+    const K row = k >> b;
     if (i == 0 || (keys[i - 1] >> b) != row)
       atomicAdd(reinterpret_cast<unsigned long long *>(&len[row]), (unsigned long long)(-i));
     if (i + 1 == m || (keys[i + 1] >> b) != row)
@@ -169,26 +169,29 @@ __device__ __forceinline__ uint32_t len_class_desc(int64_t len) {
   return 127u - (c < 127u ? c : 127u);
 }
 
-// (head << (lb + pb) | length class << pb | position) for every out-CSR
-// position; lb (0..7) bits of the class fit beside the head and position
+// (head << lb | length class) sort key and position value for every
+// out-CSR position: lb (0..7) bits of the class fit beside the head in 31 bits
+template <class V>
 __global__ void k_in_keys(const int32_t *__restrict__ col, const int32_t *__restrict__ rowof,
-                          const int64_t *__restrict__ off, int64_t m, int pb, int lb, uint64_t *__restrict__ ik) {
+                          const int64_t *__restrict__ off, int64_t m, int lb, uint32_t *__restrict__ ik,
+                          V *__restrict__ iv) {
   XT_GRID_STRIDE(p, m) {
-    uint64_t k = (uint64_t(uint32_t(col[p])) << (pb + lb)) | uint64_t(p);
+    uint32_t k = uint32_t(col[p]) << lb;
     if (lb > 0) {
       const int64_t len = off[rowof[p] + 1] - p - 1;
-      k |= uint64_t(len_class_desc(len) >> (7 - lb)) << pb;
+      k |= len_class_desc(len) >> (7 - lb);
     }
     ik[p] = k;
+    iv[p] = V(p);
   }
 }
 
-// sorted in-keys -> in-records (suffix of N+(u) after the head)
-__global__ void k_in_records(const uint64_t *__restrict__ ik, int64_t m, int pb, const int32_t *__restrict__ rowof,
+// positions sorted by (head, class) -> in-records (suffix of N+(u) after the head)
+template <class V>
+__global__ void k_in_records(const V *__restrict__ pos, int64_t m, const int32_t *__restrict__ rowof,
                              const int64_t *__restrict__ off, InRec *__restrict__ rec) {
-  const uint64_t pmask = (uint64_t(1) << pb) - 1;
   XT_GRID_STRIDE(i, m) {
-    const int64_t p = int64_t(ik[i] & pmask);
+    const int64_t p = int64_t(pos[i]);
     const int32_t u = rowof[p];
     InRec r;
     r.s = p + 1;
@@ -236,14 +239,28 @@ static xt_status select_flagged(Ctx *c, const uint64_t *in, const uint8_t *flags
   return XT_OK;
 }
 
+// radix sort of (key, value) pairs on the low end_bit bits of 32-bit keys
+template <class V>
+static xt_status sort_pairs32(Ctx *c, const uint32_t *kin, uint32_t *kout, const V *vin, V *vout, int64_t n,
+                              int end_bit) {
+  size_t bytes = 0;
+  XT_CUDA(c, cub::DeviceRadixSort::SortPairs(nullptr, bytes, kin, kout, vin, vout, n, 0, end_bit, c->stream));
+  void *tmp = nullptr;
+  XT_TRY(dalloc(c, &tmp, bytes));
+  cudaError_t e = cub::DeviceRadixSort::SortPairs(tmp, bytes, kin, kout, vin, vout, n, 0, end_bit, c->stream);
+  dfree(c, tmp);
+  XT_CUDA(c, e);
+  return XT_OK;
+}
+
 // sorted (row << b | col) keys -> off[nv+1] (and col[m] when col != null)
-static xt_status keys_to_csr(Ctx *c, const uint64_t *keys, int64_t m, int64_t nv, int b, int64_t *off,
-                             int32_t *col) {
+template <class K>
+static xt_status keys_to_csr(Ctx *c, const K *keys, int64_t m, int64_t nv, int b, int64_t *off, int32_t *col) {
   int64_t *len = nullptr;
   XT_TRY(dalloc_n(c, &len, size_t(nv + 1)));
   cudaError_t e = cudaMemsetAsync(len, 0, sizeof(int64_t) * (nv + 1), c->stream);
   if (e == cudaSuccess && m > 0) {
-    k_csr_runs<<<counted(c, grid_for(m, 256, c->sm_count)), 256, 0, c->stream>>>(keys, m, b, len, col);
+    k_csr_runs<K><<<counted(c, grid_for(m, 256, c->sm_count)), 256, 0, c->stream>>>(keys, m, b, len, col);
     e = cudaGetLastError();
   }
   size_t bytes = 0;
@@ -270,75 +287,92 @@ static xt_status check_err(Ctx *c, const char *what) {
   return XT_OK;
 }
 
-// uniq: m unique undirected edges (lo << b | hi) in input ids, sorted;
-// scratch: m more keys; deg: undirected degree in input ids (taken over by g).
-static xt_status orient_and_finish(Ctx *c, uint64_t *uniq, uint64_t *scratch, int64_t m, int64_t nv, int b,
-                                   int32_t *deg, int orient, Graph *g) {
+// Degree orientation: ranks the vertices by (deg, id) into g->d_perm
+// (internal -> input id) and relabels n keys (lo << b | hi, input ids) in
+// place to (low rank << b | high rank).
+static xt_status rank_and_relabel(Ctx *c, const int32_t *deg, int64_t nv, int b, uint64_t *keys, int64_t n,
+                                  Graph *g) {
   const int B = 256;
-  g->ne = m;
-  g->d_deg = deg;
-  uint64_t *okeys = uniq;
-  if (orient == XT_ORIENT_DEGREE) {
-    uint64_t *vk = nullptr, *vk2 = nullptr;
-    int32_t *o2n = nullptr;
-    XT_TRY(dalloc_n(c, &vk, size_t(nv)));
-    xt_status s = dalloc_n(c, &vk2, size_t(nv));
-    if (s == XT_OK) s = dalloc_n(c, &o2n, size_t(nv));
-    if (s == XT_OK) s = dalloc_n(c, &g->d_perm, size_t(nv));
-    if (s == XT_OK) {
-      k_rank_keys<<<counted(c, grid_for(nv, B, c->sm_count)), B, 0, c->stream>>>(deg, nv, vk);
-      s = sort_keys(c, vk, vk2, nv, 32 + b);
-    }
-    if (s == XT_OK) {
-      k_rank_perm<<<counted(c, grid_for(nv, B, c->sm_count)), B, 0, c->stream>>>(vk2, nv, g->d_perm, o2n);
-      if (m > 0) k_relabel_edges<<<counted(c, grid_for(m, B, c->sm_count)), B, 0, c->stream>>>(uniq, m, b, o2n);
-      s = cuda_status(c, cudaGetLastError(), "relabel");
-    }
-    if (s == XT_OK && m > 0) {
-      s = sort_keys(c, uniq, scratch, m, 2 * b);
-      okeys = scratch;
-    }
-    dfree(c, vk);
-    dfree(c, vk2);
-    dfree(c, o2n);
-    if (s != XT_OK) return s;
+  uint64_t *vk = nullptr, *vk2 = nullptr;
+  int32_t *o2n = nullptr;
+  xt_status s = dalloc_n(c, &vk, size_t(nv));
+  if (s == XT_OK) s = dalloc_n(c, &vk2, size_t(nv));
+  if (s == XT_OK) s = dalloc_n(c, &o2n, size_t(nv));
+  if (s == XT_OK) s = dalloc_n(c, &g->d_perm, size_t(nv));
+  if (s == XT_OK) {
+    k_rank_keys<<<counted(c, grid_for(nv, B, c->sm_count)), B, 0, c->stream>>>(deg, nv, vk);
+    s = sort_keys(c, vk, vk2, nv, 32 + b);
   }
-  // out-CSR. Columns are read as aligned 16-byte groups: pad so the last
-  // group of the last row stays inside the allocation.
+  if (s == XT_OK) {
+    k_rank_perm<<<counted(c, grid_for(nv, B, c->sm_count)), B, 0, c->stream>>>(vk2, nv, g->d_perm, o2n);
+    if (n > 0) k_relabel_edges<<<counted(c, grid_for(n, B, c->sm_count)), B, 0, c->stream>>>(keys, n, b, o2n);
+    s = cuda_status(c, cudaGetLastError(), "relabel");
+  }
+  dfree(c, vk);
+  dfree(c, vk2);
+  dfree(c, o2n);
+  return s;
+}
+
+// In-records grouped by head (d_ioff, d_irec), longest suffix first, from the
+// out-CSR. keys/spare: two free buffers of at least m 8-byte entries each.
+template <class V>
+static xt_status build_in_records(Ctx *c, uint64_t *keys, uint64_t *spare, int64_t m, int64_t nv, int b, Graph *g) {
+  const int B = 256;
+  const int lb = b + 7 <= 31 ? 7 : 31 - b;  // key = head << lb | class, 31 bits at most
+  // 4-byte values: keys and values of one side fit one 8-byte buffer
+  uint32_t *kin = reinterpret_cast<uint32_t *>(spare), *kout = reinterpret_cast<uint32_t *>(keys);
+  V *vin = nullptr, *vout = nullptr, *own_in = nullptr, *own_out = nullptr;
+  int32_t *rowof = nullptr;
+  xt_status s = XT_OK;
+  if (sizeof(V) == 4) {
+    vin = reinterpret_cast<V *>(kin + m);
+    vout = reinterpret_cast<V *>(kout + m);
+  } else {
+    s = dalloc_n(c, &own_in, size_t(m));
+    if (s == XT_OK) s = dalloc_n(c, &own_out, size_t(m));
+    vin = own_in;
+    vout = own_out;
+  }
+  if (s == XT_OK) s = dalloc_n(c, &rowof, size_t(m));
+  if (s == XT_OK) {
+    k_csr_rows<<<counted(c, grid_for(nv * 32, B, c->sm_count)), B, 0, c->stream>>>(g->d_off, nv, m, rowof, nullptr);
+    k_in_keys<V><<<counted(c, grid_for(m, B, c->sm_count)), B, 0, c->stream>>>(g->d_col, rowof, g->d_off, m, lb,
+                                                                               kin, vin);
+    s = cuda_status(c, cudaGetLastError(), "in-keys");
+  }
+  // stable: records of one (head, class) stay in position order
+  if (s == XT_OK) s = sort_pairs32<V>(c, kin, kout, vin, vout, m, b + lb);
+  if (s == XT_OK) s = keys_to_csr<uint32_t>(c, kout, m, nv, lb, g->d_ioff, nullptr);
+  if (s == XT_OK) {
+    k_in_records<V><<<counted(c, grid_for(m, B, c->sm_count)), B, 0, c->stream>>>(vout, m, rowof, g->d_off,
+                                                                                   g->d_irec);
+    s = cuda_status(c, cudaGetLastError(), "in-records");
+  }
+  dfree(c, rowof);
+  dfree(c, own_in);
+  dfree(c, own_out);
+  return s;
+}
+
+// keys: m unique oriented edges (src << b | dst, src < dst, internal ids),
+// sorted; spare: m more 8-byte entries. Emits the out-CSR and the in-records.
+static xt_status finish_csr(Ctx *c, uint64_t *keys, uint64_t *spare, int64_t m, int64_t nv, int b, Graph *g) {
+  g->ne = m;
+  // Columns are read as aligned 32-byte pairs: pad so the last pair of the
+  // last row stays inside the allocation.
   XT_TRY(dalloc_n(c, &g->d_off, size_t(nv + 1)));
   XT_TRY(dalloc_n(c, &g->d_col, size_t(m) + kColPad));
   XT_CUDA(c, cudaMemsetAsync(g->d_col + m, 0xff, sizeof(int32_t) * kColPad, c->stream));
-  XT_TRY(keys_to_csr(c, okeys, m, nv, b, g->d_off, g->d_col));
-  // in-records grouped by head, longest suffix first
+  XT_TRY(keys_to_csr<uint64_t>(c, keys, m, nv, b, g->d_off, g->d_col));
   XT_TRY(dalloc_n(c, &g->d_ioff, size_t(nv + 1)));
   XT_TRY(dalloc_n(c, &g->d_irec, size_t(m > 0 ? m : 1)));
   if (m == 0) {
     XT_CUDA(c, cudaMemsetAsync(g->d_ioff, 0, sizeof(int64_t) * (nv + 1), c->stream));
     return XT_OK;
   }
-  const int pb = bits_for(m);
-  const int lb = (b + pb + 7 <= 64) ? 7 : (b + pb < 64 ? 64 - b - pb : 0);
-  uint64_t *ik = (okeys == scratch) ? uniq : scratch;  // the buffer no longer needed
-  uint64_t *ik2 = nullptr;
-  int32_t *rowof = nullptr;
-  xt_status s = dalloc_n(c, &ik2, size_t(m));
-  if (s == XT_OK) s = dalloc_n(c, &rowof, size_t(m));
-  if (s == XT_OK) {
-    k_csr_rows<<<counted(c, grid_for(nv * 32, B, c->sm_count)), B, 0, c->stream>>>(g->d_off, nv, m, rowof, nullptr);
-    k_in_keys<<<counted(c, grid_for(m, B, c->sm_count)), B, 0, c->stream>>>(g->d_col, rowof, g->d_off, m, pb, lb,
-                                                                            ik);
-    s = cuda_status(c, cudaGetLastError(), "in-keys");
-  }
-  if (s == XT_OK) s = sort_keys(c, ik, ik2, m, b + lb + pb);
-  if (s == XT_OK) s = keys_to_csr(c, ik2, m, nv, lb + pb, g->d_ioff, nullptr);
-  if (s == XT_OK) {
-    k_in_records<<<counted(c, grid_for(m, B, c->sm_count)), B, 0, c->stream>>>(ik2, m, pb, rowof, g->d_off,
-                                                                               g->d_irec);
-    s = cuda_status(c, cudaGetLastError(), "in-records");
-  }
-  dfree(c, ik2);
-  dfree(c, rowof);
-  return s;
+  if (m < (int64_t(1) << 31)) return build_in_records<uint32_t>(c, keys, spare, m, nv, b, g);
+  return build_in_records<uint64_t>(c, keys, spare, m, nv, b, g);
 }
 
 xt_status build_from_edges(Ctx *c, int64_t nv, int64_t ne, const int32_t *d_src, const int32_t *d_dst, int orient,
@@ -361,26 +395,32 @@ xt_status build_from_edges(Ctx *c, int64_t nv, int64_t ne, const int32_t *d_src,
   do {
     if ((s = dalloc_n(c, &k0, n1)) != XT_OK) break;
     if ((s = dalloc_n(c, &k1, n1)) != XT_OK) break;
+    if (orient == XT_ORIENT_DEGREE) {
+      if ((s = dalloc_n(c, &deg, size_t(nv))) != XT_OK) break;
+      if ((s = cuda_status(c, cudaMemsetAsync(deg, 0, sizeof(int32_t) * nv, c->stream), "memset")) != XT_OK) break;
+    }
     if (ne > 0) {
-      if ((s = dalloc_n(c, &flags, n1)) != XT_OK) break;
-      k_edge_keys<<<counted(c, grid_for(ne, B, c->sm_count)), B, 0, c->stream>>>(d_src, d_dst, ne, nv, b, k0,
+      k_edge_keys<<<counted(c, grid_for(ne, B, c->sm_count)), B, 0, c->stream>>>(d_src, d_dst, ne, nv, b, k0, deg,
                                                                                  c->d_err);
       if ((s = cuda_status(c, cudaGetLastError(), "k_edge_keys")) != XT_OK) break;
       if ((s = check_err(c, "edge list")) != XT_OK) break;
+    }
+    // rank, then relabel every row: one sort of the rows in internal ids
+    if (orient == XT_ORIENT_DEGREE) {
+      if ((s = rank_and_relabel(c, deg, nv, b, k0, ne, g)) != XT_OK) break;
+      dfree(c, deg);
+      deg = nullptr;
+    }
+    if (ne > 0) {
+      if ((s = dalloc_n(c, &flags, n1)) != XT_OK) break;
       if ((s = sort_keys(c, k0, k1, ne, 2 * b)) != XT_OK) break;
       k_unique_flags<<<counted(c, grid_for(ne, B, c->sm_count)), B, 0, c->stream>>>(k1, ne, b, flags);
       if ((s = select_flagged(c, k1, flags, k0, ne, &m)) != XT_OK) break;
       dfree(c, flags);
       flags = nullptr;
     }
-    // k0[0..m) = unique undirected (lo,hi), sorted
-    if ((s = dalloc_n(c, &deg, size_t(nv))) != XT_OK) break;
-    if ((s = cuda_status(c, cudaMemsetAsync(deg, 0, sizeof(int32_t) * nv, c->stream), "memset")) != XT_OK) break;
-    k_degrees<<<counted(c, grid_for(m, B, c->sm_count)), B, 0, c->stream>>>(k0, m, b, deg);
-    if ((s = cuda_status(c, cudaGetLastError(), "degrees")) != XT_OK) break;
-    int32_t *d = deg;
-    deg = nullptr;  // owned by g from here
-    s = orient_and_finish(c, k0, k1, m, nv, b, d, orient, g);
+    // k0[0..m) = unique oriented edges, sorted
+    s = finish_csr(c, k0, k1, m, nv, b, g);
   } while (0);
   dfree(c, k0);
   dfree(c, k1);
@@ -430,9 +470,8 @@ xt_status build_from_csr(Ctx *c, int64_t nv, const int64_t *d_off, const int64_t
       if ((s = dalloc_n(c, &keys, n1)) != XT_OK) break;
       if ((s = dalloc_n(c, &sel, n1)) != XT_OK) break;
       if ((s = dalloc_n(c, &flags, n1)) != XT_OK) break;
-      if ((s = dalloc_n(c, &deg, size_t(nv))) != XT_OK) break;
-      k_degree_from_off<<<counted(c, grid_for(nv, B, c->sm_count)), B, 0, c->stream>>>(d_off, nv, deg);
       if (ne_in > 0) {
+        // the u < t entries of sorted symmetric rows: the sorted undirected set
         k_csr_lower_keys<<<counted(c, grid_for(ne_in, B, c->sm_count)), B, 0, c->stream>>>(rows, t32, ne_in, b,
                                                                                            keys, flags);
         if ((s = cuda_status(c, cudaGetLastError(), "k_csr_lower_keys")) != XT_OK) break;
@@ -440,9 +479,17 @@ xt_status build_from_csr(Ctx *c, int64_t nv, const int64_t *d_off, const int64_t
       }
       dfree(c, flags);
       flags = nullptr;
-      int32_t *d = deg;
-      deg = nullptr;
-      s = orient_and_finish(c, sel, keys, m, nv, b, d, orient, g);
+      if (orient == XT_ORIENT_DEGREE) {
+        if ((s = dalloc_n(c, &deg, size_t(nv))) != XT_OK) break;
+        k_degree_from_off<<<counted(c, grid_for(nv, B, c->sm_count)), B, 0, c->stream>>>(d_off, nv, deg);
+        if ((s = rank_and_relabel(c, deg, nv, b, sel, m, g)) != XT_OK) break;
+        dfree(c, deg);
+        deg = nullptr;
+        if (m > 0 && (s = sort_keys(c, sel, keys, m, 2 * b)) != XT_OK) break;
+        s = finish_csr(c, keys, sel, m, nv, b, g);
+      } else {
+        s = finish_csr(c, sel, keys, m, nv, b, g);
+      }
     } while (0);
     dfree(c, keys);
     dfree(c, sel);
@@ -466,14 +513,12 @@ void free_graph_device(Graph *g) {
   dfree(g->ctx, g->d_col);
   dfree(g->ctx, g->d_ioff);
   dfree(g->ctx, g->d_irec);
-  dfree(g->ctx, g->d_deg);
   dfree(g->ctx, g->d_perm);
   dfree(g->ctx, g->d_group);
   g->d_off = nullptr;
   g->d_col = nullptr;
   g->d_ioff = nullptr;
   g->d_irec = nullptr;
-  g->d_deg = nullptr;
   g->d_perm = nullptr;
   g->d_group = nullptr;
 }

@@ -745,9 +745,11 @@ __global__ void k_unpermute(const int64_t *__restrict__ in, const int32_t *__res
   XT_GRID_STRIDE(r, nv) out[n2o[r]] = in[r];
 }
 
-__global__ void k_max_i32(const int32_t *__restrict__ a, int64_t n, unsigned long long *out) {
+// largest undirected degree: out-degree + in-degree of the oriented graph
+__global__ void k_max_degree(const int64_t *__restrict__ off, const int64_t *__restrict__ ioff, int64_t nv,
+                             unsigned long long *out) {
   unsigned long long m = 0;
-  XT_GRID_STRIDE(i, n) m = max(m, (unsigned long long)a[i]);
+  XT_GRID_STRIDE(i, nv) m = max(m, (unsigned long long)(off[i + 1] - off[i] + ioff[i + 1] - ioff[i]));
   for (int o = 16; o; o >>= 1) m = max(m, __shfl_xor_sync(0xffffffffu, m, o));
   if ((threadIdx.x & 31) == 0) atomicMax(out, m);
 }
@@ -806,7 +808,7 @@ xt_status make_plan(Graph *g) {
     if ((s = cuda_status(c, cudaMemsetAsync(stats, 0, 4 * sizeof(unsigned long long), c->stream), "memset")) !=
         XT_OK)
       break;
-    k_max_i32<<<counted(c, grid_for(nv, B, c->sm_count)), B, 0, c->stream>>>(g->d_deg, nv, stats + 0);
+    k_max_degree<<<counted(c, grid_for(nv, B, c->sm_count)), B, 0, c->stream>>>(g->d_off, g->d_ioff, nv, stats + 0);
     k_max_rowlen<<<counted(c, grid_for(nv, B, c->sm_count)), B, 0, c->stream>>>(g->d_off, nv, stats + 1);
     k_max_rowlen<<<counted(c, grid_for(nv, B, c->sm_count)), B, 0, c->stream>>>(g->d_ioff, nv, stats + 2);
     // tail-grouped work, for the statistics only

@@ -27,10 +27,12 @@ namespace xt {
 using Clock = std::chrono::steady_clock;
 
 // Upper bound of the device bytes held while a query of nv vertices and ne
-// edge rows is copied in, built and counted (the builder's peak is its
-// in-record sort: 8 B/row input, 8 B/row graph-global ids, 16 B/row key
-// buffers, then 40 B per unique edge of columns, in-records, sort keys and
-// sort scratch; vertex arrays stay below 120 B/vertex through the plan).
+// edge rows is copied in, built and counted. The builder's largest phase is
+// its row sort: 8 B/row copied in, 8 B/row union ids (batches), 16 B/row key
+// buffers, 1 B/row flags and 8 B/row sort scratch (41 B/row); the in-record
+// phase holds less (16 B/row keys + 32 B per unique edge). Vertex arrays
+// stay below 120 B/vertex through the plan. 72 B/row leaves room for CUB's
+// scratch on top of these.
 int64_t serve_estimate(int64_t nv, int64_t ne) {
   if (nv < 0 || ne < 0) return -1;
   return 72 * ne + 120 * nv + (int64_t(4) << 20);

@@ -93,7 +93,6 @@ struct Graph {
   int32_t *d_col = nullptr;   // out-CSR columns N+(u), ne (+kColPad), rows ascending
   int64_t *d_ioff = nullptr;  // in-record offsets per head v, nv+1
   InRec *d_irec = nullptr;    // one record per edge u->v, grouped by v
-  int32_t *d_deg = nullptr;   // undirected degree, input ids, nv
   int32_t *d_perm = nullptr;  // internal id -> input id (null when identity)
   int64_t max_degree = 0;
   int64_t max_out_degree = 0;
