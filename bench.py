@@ -2,12 +2,14 @@
 """Headline benchmark: exact triangle count of the scale-24 R-MAT graph on B200.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl xtric|reference]
+                    [--workload rmat24|chunglu|rgg|batch|serve]
 
-Workload (one step): one exact count of R-MAT scale 24 (16,777,216 vertices,
-edge factor 16 -> 268,435,456 generated edges; quadrants .57/.19/.19/.05 with
-10% per-level noise; ids permuted; symmetrised, deduplicated, self loops
-dropped; degree-oriented int32 columns / int64 offsets), graph resident in
-HBM. Metric: oriented edges counted per second (|E+| per step / step time).
+Workload (one step, default rmat24): one exact count of R-MAT scale 24
+(16,777,216 vertices, edge factor 16 -> 268,435,456 generated edges;
+quadrants .57/.19/.19/.05 with 10% per-level noise; ids permuted;
+symmetrised, deduplicated, self loops dropped; degree-oriented int32 columns
+/ int64 offsets), graph resident in HBM. Metric: oriented edges counted per
+second (|E+| per step / step time).
 
   value : device time of the count kernel over K steps (CUDA events on the
           launching stream), graph already in HBM. The graph (2.1 GB of CSR
@@ -18,10 +20,18 @@ HBM. Metric: oriented edges counted per second (|E+| per step / step time).
 N > 1 GPUs (torchrun): independent replicas, one graph per GPU, no data-path
 collective; value = all ranks' edges / the slowest rank's time.
 
+Other single-graph workloads, same line: chunglu (the heavy-skew Chung-Lu
+graph, n = 4,194,304, exponent 2.1, mean degree 64, max expected 131,072;
+also times the per-vertex kernel and the id orientation) and rgg (the
+reference's own random geometric graph, n = 65,536, r = sqrt(16/(pi n)), as
+two strip ranks build it). batch and serve are the batching and serving
+forms (graphs/s; see run_batch and run_serve).
+
 --impl reference times the reference's own CPU counting path
 (oracle/_ref/tric_omp: main.cpp + xxtric.hpp built with USE_OPENMP against a
 one-rank MPI shim) on this host's cores, on a bounded sample of the same
-workload: the R-MAT graph of the same generator at scale 18.
+workload: for rmat24 the R-MAT graph of the same generator at scale 18; for
+chunglu a Chung-Lu graph of n = 131,072; for rgg the workload graph itself.
 """
 from __future__ import annotations
 
@@ -46,10 +56,6 @@ EDGE_FACTOR = 16
 SEED = 1
 SAMPLE_SCALE = 18
 
-
-def workload_name(scale: int) -> str:
-    return (f"R-MAT scale {scale}, edge factor 16 (a=.57 b=.19 c=.19 d=.05, 10% per-level noise, ids permuted), "
-            "symmetrised + deduped + loops dropped, degree-oriented, int32 cols / int64 offsets")
 
 
 def measured_peaks() -> dict:
@@ -136,24 +142,109 @@ class ClockSampler:
 
 
 # ---------------------------------------------------------------------------
+# single-graph workloads
+# ---------------------------------------------------------------------------
+
+CHUNGLU_N, CHUNGLU_GAMMA, CHUNGLU_MEAN, CHUNGLU_MAX = 4194304, 2.1, 64.0, 131072.0
+RGG_N, RGG_RANKS = 65536, 2
+
+
+class Workload:
+    """One graph counted per step: how to make it on the device, what it is
+    called, and the bounded sample the CPU reference is timed on."""
+
+    def __init__(self, key: str, scale: int = SCALE):
+        self.key = key
+        self.scale = scale
+        if key == "rmat24":
+            self.name = workload_name(scale)
+            self.extra = {"scale": scale, "edge_factor": EDGE_FACTOR}
+        elif key == "chunglu":
+            self.name = (f"Chung-Lu, n={CHUNGLU_N:,}, degree exponent {CHUNGLU_GAMMA}, mean degree {CHUNGLU_MEAN:g}, "
+                         f"max expected degree {CHUNGLU_MAX:,.0f}, ids permuted; symmetrised + deduped, "
+                         "degree-oriented, int32 cols / int64 offsets")
+            self.extra = {"n": CHUNGLU_N, "gamma": CHUNGLU_GAMMA, "mean_degree": CHUNGLU_MEAN,
+                          "max_expected_degree": CHUNGLU_MAX}
+        elif key == "rgg":
+            self.radius = float(np.sqrt(16.0 / (np.pi * RGG_N)))
+            self.name = (f"random geometric graph of the reference's generator (LCG seed 1, -l), n={RGG_N:,} in the "
+                         f"unit square, r=sqrt(16/(pi n))={self.radius:.5f}, -p 0, as mpiexec -n {RGG_RANKS} builds "
+                         "it; degree-oriented")
+            self.extra = {"n": RGG_N, "radius": self.radius, "strip_ranks": RGG_RANKS}
+        else:
+            raise ValueError(key)
+
+    def device_edges(self, ctx, torch):
+        """(nv, src, dst): int32 edge rows in device memory."""
+        import xxtric_b200 as xt
+        if self.key == "rmat24":
+            n, ne = 1 << self.scale, EDGE_FACTOR << self.scale
+            src = torch.empty(ne, dtype=torch.int32, device="cuda")
+            dst = torch.empty_like(src)
+            ctx.gen_rmat(self.scale, ne, SEED, src, dst)
+            return n, src, dst
+        if self.key == "chunglu":
+            cdf, ne = xt.chunglu_cdf(CHUNGLU_N, CHUNGLU_GAMMA, CHUNGLU_MEAN, CHUNGLU_MAX)
+            src = torch.empty(ne, dtype=torch.int32, device="cuda")
+            dst = torch.empty_like(src)
+            ctx.gen_chunglu(cdf, ne, SEED, src, dst)
+            return CHUNGLU_N, src, dst
+        off, tails = xt.generate_rgg(RGG_N, RGG_RANKS, self.radius)
+        src = torch.from_numpy(np.repeat(np.arange(RGG_N, dtype=np.int32), np.diff(off))).cuda()
+        dst = torch.from_numpy(tails.astype(np.int32)).cuda()
+        return RGG_N, src, dst
+
+    def cpu_sample(self):
+        """(canonical CSR, description) of the graph the CPU reference counts:
+        the workload itself where it finishes in seconds, else a smaller graph
+        of the same generator."""
+        import oracle
+        if self.key == "rmat24":
+            sc = min(self.scale, SAMPLE_SCALE)
+            n = 1 << sc
+            src, dst = oracle.rmat_edges(sc, EDGE_FACTOR << sc, SEED)
+            return oracle.canon_csr(n, src, dst), f"R-MAT scale {sc} of the same generator"
+        if self.key == "chunglu":
+            n = 1 << 17
+            mx = CHUNGLU_MAX * n / CHUNGLU_N
+            cdf, ne = oracle.chunglu_cdf(n, CHUNGLU_GAMMA, CHUNGLU_MEAN, mx)
+            src, dst = oracle.chunglu_edges(cdf, ne, SEED)
+            return (oracle.canon_csr(n, src, dst),
+                    f"Chung-Lu n={n:,} of the same generator (exponent {CHUNGLU_GAMMA}, mean {CHUNGLU_MEAN:g}, "
+                    f"max expected degree {mx:,.0f})")
+        import xxtric_b200 as xt
+        return xt.generate_rgg(RGG_N, RGG_RANKS, self.radius), "the workload graph itself"
+
+    def config(self, world: int, info: dict | None) -> dict:
+        c = {"workload": self.name, **self.extra, "seed": SEED, "orient": "degree",
+             "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+             "l2": ("inputs larger than L2 (CSR + transpose > 126 MB), no flush" if self.key != "rgg" else
+                    "graph (~10 MB) fits in L2: back-to-back counts, no flush (launch-bound size)")}
+        if info:
+            c.update({"nv": info["nv"], "oriented_edges": info["n_edges"], "max_degree": info["max_degree"],
+                      "max_out_degree": info["max_out_degree"]})
+        return c
+
+
+def workload_name(scale: int) -> str:
+    return (f"R-MAT scale {scale}, edge factor 16 (a=.57 b=.19 c=.19 d=.05, 10% per-level noise, ids permuted), "
+            "symmetrised + deduped + loops dropped, degree-oriented, int32 cols / int64 offsets")
+
+
+# ---------------------------------------------------------------------------
 # CPU baseline: the reference's own CPU path on a sample of the workload
 # ---------------------------------------------------------------------------
 
-def reference_sample(scale: int = SAMPLE_SCALE):
-    """R-MAT graph of the same generator at a smaller scale, as a vite file."""
-    import oracle
-    n = 1 << scale
-    src, dst = oracle.rmat_edges(scale, EDGE_FACTOR << scale, SEED)
-    off, tails = oracle.canon_csr(n, src, dst)
-    path = os.path.join(tempfile.gettempdir(), f"xtric_rmat{scale}_{os.getpid()}.bin")
+def write_vite(off, tails) -> str:
+    path = os.path.join(tempfile.gettempdir(), f"xtric_sample_{os.getpid()}.bin")
     rec = np.zeros(len(tails), dtype=[("t", "<i8"), ("w", "<f8")])
     rec["t"] = tails
     rec["w"] = 1.0
     with open(path, "wb") as f:
-        np.array([n, len(tails)], np.int64).tofile(f)
-        off.tofile(f)
+        np.array([len(off) - 1, len(tails)], np.int64).tofile(f)
+        np.asarray(off, np.int64).tofile(f)
         rec.tofile(f)
-    return path, off, tails, len(tails) // 2
+    return path
 
 
 def time_reference_once(path: str, off, tails, cores: int) -> tuple[float, str, int]:
@@ -173,23 +264,27 @@ def time_reference_once(path: str, off, tails, cores: int) -> tuple[float, str, 
     return time.perf_counter() - t0, "port", t
 
 
-def cpu_baseline(cores: int, steps: int = 1, warmup: int = 0) -> dict:
-    path, off, tails, n_edges = reference_sample()
+def cpu_baseline(wl: Workload, cores: int, steps: int = 1, warmup: int = 0) -> dict:
+    (off, tails), what = wl.cpu_sample()
+    n_edges = len(tails) // 2
+    path = write_vite(off, tails)
     try:
         ts = []
         kind = "reference"
         tri = -1
-        for i in range(warmup + steps):
+        i = 0
+        # at least `steps` timed runs, more while they add up to under ~10 s
+        while i < warmup + steps or (sum(ts) < 10.0 and len(ts) < 200):
             t, kind, tri = time_reference_once(path, off, tails, cores)
             if i >= warmup:
                 ts.append(t)
+            i += 1
     finally:
         os.unlink(path)
     total = sum(ts)
     return {"value": n_edges * len(ts) / total, "unit": UNIT, "cores": cores, "kind": kind,
-            "sample": f"R-MAT scale {SAMPLE_SCALE} of the same generator ({n_edges} oriented edges, "
-                      f"{tri} triangles), reference OpenMP CPU count, {len(ts)} run(s), "
-                      f"{total / len(ts):.3f} s per run",
+            "sample": f"{what} ({n_edges} oriented edges, {tri} triangles), reference OpenMP CPU count, "
+                      f"{len(ts)} run(s), {total / len(ts):.4f} s per run",
             "seconds_per_run": total / len(ts), "n_edges": n_edges}
 
 
@@ -198,34 +293,42 @@ def run_reference_arm(args) -> None:
     rank, world, _ = replicas.env_ranks()
     if rank != 0:
         return  # rank 0 alone times the CPU reference
+    if args.workload in ("batch", "serve"):
+        print(json.dumps({"impl": "reference", "unavailable": f"the {args.workload} form has no counterpart in the "
+                          "reference (it counts one graph per run); its CPU baseline is the rmat24 line"}))
+        return
+    wl = Workload(args.workload, args.scale)
     cores = os.cpu_count() or 1
     try:
-        cb = cpu_baseline(cores, steps=args.steps, warmup=args.warmup)
+        cb = cpu_baseline(wl, cores, steps=args.steps, warmup=args.warmup)
     except Exception as e:  # report, never fake a number
         print(json.dumps({"impl": "reference", "unavailable": f"reference CPU path failed: {e}"[:300]}))
         return
     line = {"metric": METRIC, "value": cb["value"], "unit": UNIT, "impl": "reference", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * cb["seconds_per_run"],
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int64",
-            "data": "synthetic", "config": config_dict(world, None),
+            "data": "synthetic", "config": wl.config(world, None),
             "cpu_baseline": {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")},
             "e2e": {"value": cb["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
 
 
-def config_dict(world: int, info: dict | None, scale: int = SCALE) -> dict:
-    c = {"workload": workload_name(scale), "scale": scale, "edge_factor": EDGE_FACTOR, "seed": SEED, "orient": "degree",
-         "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
-         "l2": "inputs larger than L2 (CSR + transpose > 2 GB), no flush"}
-    if info:
-        c.update({"nv": info["nv"], "oriented_edges": info["n_edges"], "max_degree": info["max_degree"],
-                  "max_out_degree": info["max_out_degree"]})
-    return c
-
-
 # ---------------------------------------------------------------------------
 # the product arm
 # ---------------------------------------------------------------------------
+
+def time_counts(g, stream, torch, steps: int, per_vertex=None) -> float:
+    """Mean device seconds of one count (CUDA events on the launching stream)."""
+    d = torch.zeros(1, dtype=torch.int64, device="cuda")
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    g.count_async(d, per_vertex)  # warm
+    a.record(stream)
+    for _ in range(steps):
+        g.count_async(d, per_vertex)
+    b.record(stream)
+    torch.cuda.synchronize()
+    return a.elapsed_time(b) / 1e3 / steps
+
 
 def run_xtric(args) -> None:
     import torch
@@ -233,16 +336,15 @@ def run_xtric(args) -> None:
     import xxtric_b200 as xt
     from xxtric_b200 import replicas
 
+    wl = Workload(args.workload, args.scale)
     rank, world, local = replicas.init(backend="nccl")
     torch.cuda.set_device(local)
     stream = torch.cuda.current_stream()
     ctx = xt.Context(local)
     ctx.set_stream(stream.cuda_stream)
-    n = 1 << args.scale
-    ne = EDGE_FACTOR << args.scale
-    src = torch.empty(ne, dtype=torch.int32, device="cuda")
-    dst = torch.empty_like(src)
-    ctx.gen_rmat(args.scale, ne, SEED, src, dst)
+    n, src, dst = wl.device_edges(ctx, torch)
+    ne = len(src)
+    torch.cuda.synchronize()
     g = ctx.graph_from_device_edges(n, ne, src, dst, xt.ORIENT_DEGREE)
     info = g.info()
     d_count = torch.zeros(1, dtype=torch.int64, device="cuda")
@@ -278,6 +380,21 @@ def run_xtric(args) -> None:
         raise RuntimeError(f"count changed between steps: {counts}")
     value, total_edges, t_max = replicas.aggregate(info["n_edges"] * args.steps, t_total)
 
+    extra = {}
+    if args.workload == "chunglu":
+        # the per-vertex kernel and the reference's id orientation on the same graph
+        pv = torch.zeros(n, dtype=torch.int64, device="cuda")
+        extra["per_vertex_ms"] = 1e3 * time_counts(g, stream, torch, 3, pv)
+        del pv
+        gi = ctx.graph_from_device_edges(n, ne, src, dst, xt.ORIENT_ID)
+        extra["id_orientation_ms"] = 1e3 * time_counts(gi, stream, torch, 3)
+        ii = gi.info()
+        extra["id_orientation_max_out_degree"] = ii["max_out_degree"]
+        # candidates streamed: sum over u of C(d+(u), 2), the work the orientation sets
+        extra["candidates"] = info["stream_work"]
+        extra["id_orientation_candidates"] = ii["stream_work"]
+        gi.free()
+
     # ---- end to end through the C ABI with host buffers ----
     h_src = torch.empty(ne, dtype=torch.int32, pin_memory=True)
     h_dst = torch.empty(ne, dtype=torch.int32, pin_memory=True)
@@ -311,12 +428,14 @@ def run_xtric(args) -> None:
 
     peaks = measured_peaks()
     achieved = info["alg_bytes"] / t_kernel / 1e9
-    traffic = profiled_traffic("k_count_rmat_s24.md") if args.scale == SCALE else None
+    traffic = profiled_traffic(f"k_count_{args.workload}.md") if args.scale == SCALE else None
+    if args.workload == "rmat24" and args.scale == SCALE:
+        traffic = profiled_traffic("k_count_rmat_s24.md")
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": 1e3 * t_max / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic",
-        "config": config_dict(world, info, args.scale), "triangles": counts[0],
+        "config": wl.config(world, info), "triangles": counts[0],
         "triangles_per_s": counts[0] * args.steps * world / t_max,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
                      "frac": achieved / peaks["hbm_gbs"], "traffic": traffic,
@@ -325,11 +444,11 @@ def run_xtric(args) -> None:
                      "tail_grouped_alg_bytes": info["tail_alg_bytes"]},
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 2 * 4 * ne, "d2h_bytes_per_step": 8,
                 "ms_per_step": 1e3 * t_e2e / args.e2e_steps, "steps": args.e2e_steps},
-        "gpu_launches": launches, "clocks": clocks,
+        "gpu_launches": launches, "clocks": clocks, **extra,
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
-            cb = cpu_baseline(os.cpu_count() or 1)
+            cb = cpu_baseline(wl, os.cpu_count() or 1)
             line["cpu_baseline"] = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")}
         except Exception as e:
             line["cpu_baseline"] = {"value": None, "unavailable": str(e)[:200]}
@@ -595,9 +714,10 @@ def main() -> None:
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--impl", choices=["xtric", "reference"], default="xtric")
-    ap.add_argument("--workload", choices=["rmat24", "batch", "serve"], default="rmat24",
-                    help="rmat24: the headline single-graph count; batch: the batching form; serve: the serving "
-                         "form (Poisson arrival sweep)")
+    ap.add_argument("--workload", choices=["rmat24", "chunglu", "rgg", "batch", "serve"], default="rmat24",
+                    help="rmat24: the headline single-graph count (R-MAT scale 24); chunglu: the heavy-skew "
+                         "Chung-Lu graph; rgg: the reference's small random geometric graph; batch: the batching "
+                         "form; serve: the serving form (Poisson arrival sweep)")
     ap.add_argument("--scale", type=int, default=SCALE,
                     help="R-MAT scale of the single-graph workload (24 is the headline; smaller scales are the "
                          "small cases that profiler captures run on)")

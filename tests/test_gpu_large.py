@@ -97,3 +97,32 @@ def test_size_limits(ctx):
     with pytest.raises(xt.XtError) as e:
         ctx.graph_from_edges(1 << 31, np.zeros(1, np.int32), np.zeros(1, np.int32))
     assert e.value.status == xt.XT_ERR_OVERFLOW
+
+
+def test_chunglu_config_properties(ctx):
+    """The heavy-skew workload at full size: Chung-Lu, n = 4,194,304, degree
+    exponent 2.1, mean degree 64, expected maximum 131,072. Both orientations
+    (the id order puts hubs on the part-split CTA tier), global and
+    per-vertex counts, and the hubs' local counts against the oracle."""
+    import torch
+    n = 4194304
+    cdf, m = xt.chunglu_cdf(n, 2.1, 64.0, 131072.0)
+    s = torch.empty(m, dtype=torch.int32, device="cuda")
+    d = torch.empty_like(s)
+    ctx.gen_chunglu(cdf, m, 1, s, d)
+    g = ctx.graph_from_device_edges(n, m, s, d, xt.ORIENT_DEGREE)
+    t, pv = g.count(per_vertex=True)
+    assert g.count() == t
+    inf = g.info()
+    g.free()
+    assert pv.sum() == 3 * t
+    g_id = ctx.graph_from_device_edges(n, m, s, d, xt.ORIENT_ID)
+    t_id, pv_id = g_id.count(per_vertex=True)
+    g_id.free()
+    assert t_id == t and (pv_id == pv).all()
+    off, tails = oracle.canon_csr(n, s.cpu().numpy().astype(np.int64), d.cpu().numpy().astype(np.int64))
+    deg = np.diff(off)
+    assert inf["max_degree"] == deg.max() and inf["n_edges"] * 2 == len(tails)
+    rng = np.random.default_rng(3)
+    sel = np.concatenate([np.argsort(deg)[-32:], rng.choice(n, 2000, replace=False)])
+    assert (oracle.local_counts(off, tails, sel) == pv[sel]).all()

@@ -82,3 +82,14 @@ def test_reference_binary_on_rgg_matches_golden():
     assert r["rc"] == 0
     assert r["triangles"] == GOLDEN["rgg4096"]["triangles"]
     assert r["edges"] == GOLDEN["rgg4096"]["directed_entries"]
+
+
+def test_local_counts_equal_per_vertex_merge_counts():
+    # the sampled-vertex checker of the full-size GPU tests against the
+    # independent merge counter, every vertex of a skewed graph
+    n = 1 << 13
+    cdf, m = oracle.chunglu_cdf(n, 2.1, 16.0, 2048.0)
+    s, d = oracle.chunglu_edges(cdf, m, 4)
+    off, tails = oracle.canon_csr(n, s, d)
+    _, pv = oracle.count_merge(off, tails, per_vertex=True)
+    assert (oracle.local_counts(off, tails, np.arange(n)) == pv).all()
