@@ -24,8 +24,8 @@
 //              into parts, one task per (part, chunk)
 // One persistent kernel drains the CTA tasks first (the large ones), then the
 // warp tasks, then the lane tasks, each from its own global atomic cursor.
-// Inside a task, lanes walk whole suffixes in aligned 32-byte pairs (see
-// stream_kind).
+// Inside a task, lanes walk whole suffixes in aligned 32-byte pairs, only a
+// record's first and last pair masked (see stream_kind).
 #include <cub/cub.cuh>
 
 #include "xt_internal.cuh"
@@ -304,18 +304,15 @@ __device__ __forceinline__ void members_insert(const Members &m, int32_t x) {
 
 // ---- streaming the in-record suffixes ----------------------------------------
 //
-// A pair is an aligned 32-byte block of 8 columns (two 16-byte loads). A
-// batch holds 32/S records; the S lanes of record j take its pairs k, k+S,
-// k+2S, ... so every lane streams a contiguous run of one suffix with no
-// per-column bookkeeping. Records of a head are stored longest first, so the
-// lanes of a batch run for about as many steps each. Columns outside the
-// suffix (the head side of the first pair, the next row after the last)
-// are replaced by a sentinel that no membership test accepts; the test is
-// needed only on a batch's first step and once any lane reaches its last
-// pair.
-#ifndef XT_PF_DEPTH
-#define XT_PF_DEPTH 1
-#endif
+// A pair is an aligned 32-byte block of 8 columns (one 256-bit load). A
+// record's suffix covers pairs 0 .. np-1; only its first and last pair can
+// hold columns outside the suffix (the head's side of row u, the next row).
+// A batch holds 32/S records. The S lanes of record j stream its INTERIOR
+// pairs 1, ..., np-2 — lane k takes 1+k, 1+k+S, ... — with no per-column
+// test; the two boundary pairs are masked (columns outside the suffix become
+// a sentinel that no membership test accepts) and probed in one extra step
+// (two when S = 1). Records of a head are stored longest first, so the lanes
+// of a batch run for about as many steps.
 constexpr int32_t kSentinel = -2;  // negative: below every member, and not kEmpty
 // positions inside one suffix are int32: out-degrees stay below this
 constexpr int64_t kMaxOutDegree = int64_t(1) << 30;
@@ -403,6 +400,7 @@ __device__ __forceinline__ int64_t stream_kind(const InRec *__restrict__ rec, co
   const int bsz = 32 >> lg_s;
   const int j = lane >> lg_s, k = lane & (S - 1);
   const int32_t nrec = int32_t(kend - k0);
+  const int4 sent = make_int4(kSentinel, kSentinel, kSentinel, kSentinel);
   rec += k0;
   int32_t seq = 0;
   auto claim = [&]() -> int32_t {
@@ -432,38 +430,41 @@ __device__ __forceinline__ int64_t stream_kind(const InRec *__restrict__ rec, co
     const int4 nn4 = fetch(nnkb);
     prefetch_suffix(col, n4, k, S);
     const int64_t s = int64_t(uint32_t(r4.x)) | (int64_t(r4.y) << 32);
-    const int32_t sr = int32_t(s & 7);  // suffix [sr, er) relative to its first pair
+    const int64_t p0 = s >> 3;          // the suffix's first pair
+    const int32_t sr = int32_t(s & 7);  // suffix [sr, er) relative to that pair
     const int32_t er = sr + r4.z;
     const int32_t np = r4.z > 0 ? (er + 7) >> 3 : 0;
-    const int32_t cnt = np > k ? ((np - k + S - 1) >> lg_s) : 0;  // this lane's pairs
+    const int32_t ni = np > 2 ? np - 2 : 0;                         // interior pairs
+    const int32_t cnt = ni > k ? ((ni - k + S - 1) >> lg_s) : 0;  // this lane's
     const int32_t steps = int32_t(__reduce_max_sync(0xffffffffu, uint32_t(cnt)));
-    // steps from `clean` on may hold a lane's last pair (or none)
-    const int32_t clean = int32_t(__reduce_min_sync(0xffffffffu, uint32_t(cnt))) - 1;
-    int64_t P = (s >> 3) + k;
-    int32_t q = 8 * k;  // this lane's pair, relative to the suffix's first pair
-    int4 xa = make_int4(0, 0, 0, 0), xb = xa;
-    if (cnt > 0) load_pair(col, P, xa, xb);
+    int64_t P = p0 + 1 + k;
+    int4 xa = sent, xb = sent;
+    if (cnt > 0) load_pair(col, P, xa, xb);  // in flight during the boundary step(s)
     int h = 0;
-#if XT_PF_DEPTH >= 2
-    int4 ya = xa, yb = xa;
-    if (cnt > 1) load_pair(col, P + S, ya, yb);
-#pragma unroll 2
-#endif
+    // boundary pairs: with S >= 2 lane k = 0 takes pair 0 and lane k = 1 pair
+    // np-1, in one step; with S = 1 the lane takes both, in two
+    const int nbs = S >= 2 ? 1 : 2;
+    for (int t = 0; t < nbs; t++) {
+      const int which = S >= 2 ? k : t;  // 0: first pair, 1: last pair
+      const bool ok = which == 0 ? np >= 1 : (which == 1 && np >= 2);
+      const int32_t bp = which == 0 ? 0 : np - 1;
+      int4 a = sent, b = sent;
+      if (ok) {
+        load_pair(col, p0 + bp, a, b);
+        mask_pair(a, b, sr - 8 * bp, er - 8 * bp);
+      }
+      h += probe_pair<PV, BITMAP>(a, b, m);
+    }
+    // interior pairs: every column is in the suffix; a lane past its last
+    // pair probes sentinels
     for (int32_t it = 0; it < steps; it++) {
-      int4 a = xa, b = xb;
-      const int32_t cq = q;
+      const int4 a = xa, b = xb;
       P += S;
-      q += 8 * S;
-#if XT_PF_DEPTH >= 2
-      xa = ya;
-      xb = yb;
-      if (it + 2 < cnt) load_pair(col, P + S, ya, yb);  // two steps ahead
-#else
-      if (it + 1 < cnt) load_pair(col, P, xa, xb);  // next step's pair in flight during the probes
-#endif
-      if (it == 0 || it >= clean) {
-        const bool act = it < cnt;
-        mask_pair(a, b, act ? sr - cq : 0, act ? er - cq : 0);
+      if (it + 1 < cnt) {
+        load_pair(col, P, xa, xb);  // next step's pair in flight during the probes
+      } else {
+        xa = sent;
+        xb = sent;
       }
       h += probe_pair<PV, BITMAP>(a, b, m);
     }
