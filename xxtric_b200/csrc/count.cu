@@ -37,7 +37,7 @@ namespace xt {
 #define XT_THREADS 256
 #endif
 #ifndef XT_BLOCK_WORK_LOG2
-#define XT_BLOCK_WORK_LOG2 20
+#define XT_BLOCK_WORK_LOG2 17
 #endif
 #ifndef XT_WARP_WORK
 #define XT_WARP_WORK 4096
