@@ -301,6 +301,16 @@ xt_status xt_vite_read(const char *path, int elem_bytes, int64_t *nv, int64_t *n
 xt_status xt_vite_write(const char *path, int elem_bytes, int64_t nv, const int64_t *offsets,
                         const int64_t *tails);
 
+/* Tab-separated edge list, the input of the reference's cuGraph comparison
+ * (cugraph/cug_triangle_count.py:23-26: src, dst, optional weight; ids as
+ * given, so *nv = largest id + 1). With src == NULL only *nv and *ne are
+ * filled (sizing call); otherwise up to cap rows go to src/dst
+ * (XT_ERR_OVERFLOW beyond cap). '#'/'%' comment and blank lines are skipped;
+ * a malformed line is XT_ERR_IO. */
+xt_status xt_tsv_read(const char *path, int64_t *nv, int64_t *ne, int32_t *src, int32_t *dst, int64_t cap);
+/* writes ne rows "src<TAB>dst<TAB>1" */
+xt_status xt_tsv_write(const char *path, int64_t ne, const int32_t *src, const int32_t *dst);
+
 /* Replaces GenerateRGG(nv).generate(LCG, unit weights, random_edge_pct)
  * (graph.hpp:745-1364, utils.hpp:245-430; main.cpp:90-91) as nprocs strip
  * ranks would build it under mpiexec -n nprocs (the graph depends on the rank

@@ -12,9 +12,10 @@ import pytest
 
 import oracle
 import xxtric_b200 as xt
-from conftest import ROOT, load_golden
+from conftest import ROOT, load_fixtures, load_golden
 
 GOLDEN = load_golden()
+FIX = load_fixtures()
 HEADER = os.path.join(ROOT, "include", "xtric.h")
 CLI = os.path.join(ROOT, "xxtric_b200", "xtric")
 
@@ -169,3 +170,31 @@ def test_cli_argument_errors():
     assert r.returncode == 157 and "Invalid random edge percentage" in r.stderr
     r = run_cli("-f", "/nonexistent.bin")
     assert r.returncode == 157 and "Error opening file!" in r.stdout
+
+
+def test_tsv_roundtrip_and_golden_count_input(tmp_path):
+    # the amazon0302 fixture's rows (the reference's cuGraph TSV, ids as
+    # given) written as TSV and read back: same rows, nv = largest id + 1
+    src, dst = FIX["amazon0302_src"].astype(np.int32), FIX["amazon0302_dst"].astype(np.int32)
+    p = str(tmp_path / "a.tsv")
+    xt.write_tsv(p, src, dst)
+    nv, s2, d2 = xt.read_tsv(p)
+    assert nv == GOLDEN["amazon0302"]["nv"]
+    assert (s2 == src).all() and (d2 == dst).all()
+    off, tails = oracle.canon_csr(nv, s2.astype(np.int64), d2.astype(np.int64))
+    assert oracle.count_merge(off, tails) == GOLDEN["amazon0302"]["triangles"]
+
+
+def test_tsv_comments_weights_and_errors(tmp_path):
+    p = tmp_path / "g.tsv"
+    p.write_text("# a comment\n% another\n\n0\t1\t0.5\n1 2\n2\t0\t3\r\n")
+    nv, s, d = xt.read_tsv(str(p))
+    assert nv == 3 and s.tolist() == [0, 1, 2] and d.tolist() == [1, 2, 0]
+    for bad in ("0\tx\n", "-1\t2\n", "0\n", "5\t99999999999\n"):
+        p.write_text(bad)
+        with pytest.raises(xt.XtError) as e:
+            xt.read_tsv(str(p))
+        assert e.value.status == xt.XT_ERR_IO
+    with pytest.raises(xt.XtError) as e:
+        xt.read_tsv(str(tmp_path / "missing.tsv"))
+    assert e.value.status == xt.XT_ERR_IO

@@ -99,6 +99,8 @@ _proto("xt_serve_wait", _int, _vp, _i64, _i64, _P(_i64), _P(_dbl))
 _proto("xt_serve_get_stats", _int, _vp, _vp)
 _proto("xt_serve_close", _int, _vp)
 _proto("xt_serve_batches", _i64, _vp, _vp, _i64)
+_proto("xt_tsv_read", _int, ctypes.c_char_p, _P(_i64), _P(_i64), _vp, _vp, _i64)
+_proto("xt_tsv_write", _int, ctypes.c_char_p, _i64, _vp, _vp)
 _proto("xt_graph_autotune", _int, _vp, _int, ctypes.c_char_p, _vp, _i64)
 _proto("xt_batch_spec", _int, _i64, _u64, _vp, _vp, _vp, _vp)
 _proto("xt_gen_batch", _int, _vp, _i64, _vp, _vp, _vp, _vp, _vp, _P(_vp), _P(_vp))
@@ -118,7 +120,7 @@ EXPORTED = ["xt_strerror", "xt_last_error", "xt_open", "xt_close", "xt_set_strea
             "xt_count_device_static", "xt_graph_from_batch", "xt_graph_from_device_batch", "xt_graph_groups",
             "xt_count_groups", "xt_count_groups_async", "xt_graph_capture", "xt_graph_set_tuning", "xt_graph_set_tiers",
             "xt_mem_stats", "xt_serve_estimate", "xt_serve_open", "xt_serve_submit", "xt_serve_poll",
-            "xt_serve_wait", "xt_serve_get_stats", "xt_serve_close", "xt_serve_batches",
+            "xt_serve_wait", "xt_serve_get_stats", "xt_serve_close", "xt_serve_batches", "xt_tsv_read", "xt_tsv_write",
             "xt_graph_autotune", "xt_batch_spec", "xt_gen_batch", "xt_device_free",
             "xt_gen_rmat", "xt_gen_chunglu", "xt_chunglu_cdf", "xt_gen_er", "xt_vite_read", "xt_vite_write",
             "xt_rgg_generate"]
@@ -171,6 +173,24 @@ def write_vite(path: str, offsets: np.ndarray, tails: np.ndarray, elem_bytes: in
     off = np.ascontiguousarray(offsets, np.int64)
     t = np.ascontiguousarray(tails, np.int64)
     _check(_L.xt_vite_write(path.encode(), elem_bytes, len(off) - 1, _ptr(off), _ptr(t)), f"writing {path}")
+
+
+def read_tsv(path: str) -> tuple[int, np.ndarray, np.ndarray]:
+    """Tab-separated edge list (src, dst[, weight]) with ids as given:
+    (nv = largest id + 1, src int32, dst int32)."""
+    nv, ne = _i64(0), _i64(0)
+    _check(_L.xt_tsv_read(path.encode(), ctypes.byref(nv), ctypes.byref(ne), None, None, 0), f"reading {path}")
+    src = np.empty(ne.value, np.int32)
+    dst = np.empty(ne.value, np.int32)
+    _check(_L.xt_tsv_read(path.encode(), ctypes.byref(nv), ctypes.byref(ne), _ptr(src), _ptr(dst), len(src)),
+           f"reading {path}")
+    return nv.value, src, dst
+
+
+def write_tsv(path: str, src: np.ndarray, dst: np.ndarray) -> None:
+    s = np.ascontiguousarray(src, np.int32)
+    d = np.ascontiguousarray(dst, np.int32)
+    _check(_L.xt_tsv_write(path.encode(), len(s), _ptr(s), _ptr(d)), f"writing {path}")
 
 
 def generate_rgg(nv: int, nprocs: int = 1, radius: float = 0.0, random_edge_pct: float = 0.0,

@@ -10,6 +10,7 @@
 #include <cmath>
 #include <cstring>
 #include <random>
+#include <string>
 #include <unordered_set>
 #include <vector>
 
@@ -144,6 +145,90 @@ xt_status xt_vite_write(const char *path, int elem_bytes, int64_t nv, const int6
       if (!put(&t, 4) || !put(&w, 4)) return XT_ERR_IO;
     }
   }
+  return XT_OK;
+}
+
+// Tab-separated edge lists as the reference's cuGraph comparison reads them
+// (cugraph/cug_triangle_count.py:23-26: columns src, dst, weight; ids used
+// as given, renumber=False, so nv = largest id + 1). Blank lines and lines
+// starting with '#' or '%' are skipped; a third column is read past and
+// ignored. Ids must be integers in [0, 2^31 - 1).
+xt_status xt_tsv_read(const char *path, int64_t *nv, int64_t *ne, int32_t *src, int32_t *dst, int64_t cap) {
+  if (!path || !nv || !ne) return XT_ERR_INVALID;
+  File f(fopen(path, "rb"));
+  if (!f.f) return XT_ERR_IO;
+  std::vector<char> buf(size_t(1) << 20);
+  std::string carry;
+  int64_t rows = 0, maxid = -1;
+  bool bad = false;
+  auto line = [&](const char *a, const char *b) {
+    while (a < b && (*a == ' ' || *a == '\t')) a++;
+    if (a == b || *a == '#' || *a == '%' || *a == '\r') return;
+    int64_t v[2];
+    for (int k = 0; k < 2; k++) {
+      while (a < b && (*a == ' ' || *a == '\t')) a++;
+      if (a == b || *a < '0' || *a > '9') {
+        bad = true;
+        return;
+      }
+      int64_t x = 0;
+      while (a < b && *a >= '0' && *a <= '9') {
+        x = x * 10 + (*a - '0');
+        if (x >= INT32_MAX) {
+          bad = true;
+          return;
+        }
+        a++;
+      }
+      v[k] = x;
+    }
+    if (a < b && *a != '\t' && *a != ' ' && *a != '\r') {
+      bad = true;
+      return;
+    }
+    if (src) {
+      if (rows >= cap) {
+        bad = true;
+        return;
+      }
+      src[rows] = int32_t(v[0]);
+      dst[rows] = int32_t(v[1]);
+    }
+    maxid = std::max(maxid, std::max(v[0], v[1]));
+    rows++;
+  };
+  size_t k;
+  while (!bad && (k = fread(buf.data(), 1, buf.size(), f.f)) > 0) {
+    const char *p = buf.data(), *end = p + k;
+    while (!bad) {
+      const char *nl = static_cast<const char *>(memchr(p, '\n', size_t(end - p)));
+      if (!nl) {
+        carry.append(p, end);
+        break;
+      }
+      if (!carry.empty()) {
+        carry.append(p, nl);
+        line(carry.data(), carry.data() + carry.size());
+        carry.clear();
+      } else {
+        line(p, nl);
+      }
+      p = nl + 1;
+    }
+  }
+  if (!bad && !carry.empty()) line(carry.data(), carry.data() + carry.size());
+  if (bad) return src && rows >= cap ? XT_ERR_OVERFLOW : XT_ERR_IO;
+  *ne = rows;
+  *nv = maxid + 1;
+  return XT_OK;
+}
+
+xt_status xt_tsv_write(const char *path, int64_t ne, const int32_t *src, const int32_t *dst) {
+  if (!path || ne < 0 || (ne > 0 && (!src || !dst))) return XT_ERR_INVALID;
+  File f(fopen(path, "wb"));
+  if (!f.f) return XT_ERR_IO;
+  for (int64_t i = 0; i < ne; i++)
+    if (fprintf(f.f, "%d\t%d\t1\n", src[i], dst[i]) < 0) return XT_ERR_IO;
   return XT_OK;
 }
 
