@@ -124,6 +124,13 @@ xt_status xt_count(xt_graph *g, int64_t *global, int64_t *per_vertex);
  * d_per_vertex (nullable) holds nv int64 entries and is overwritten */
 xt_status xt_count_async(xt_graph *g, int64_t *d_global, int64_t *d_per_vertex);
 
+/* No counterpart in the reference (its per-edge work is internal): the
+ * global count and, for every oriented edge, the number of triangles that
+ * contain it (its k-truss support), into a host array of n_edges entries in
+ * the order of xt_graph_get_csr (internal numbering; xt_graph_get_perm maps
+ * ids back). The supports sum to 3 x global. Synchronous. */
+xt_status xt_count_edges(xt_graph *g, int64_t *global, int64_t *support);
+
 /* Replaces the kernel launcher single_gpu_count(nv, d_indices, d_edge_list,
  * d_local_count) (counting.cuh:259-265, counting.cu:537-577): the reference's
  * device CSR (int64 offsets, int64 tails; rows sorted, deduped, symmetric)

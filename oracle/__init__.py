@@ -44,6 +44,7 @@ def lib() -> ctypes.CDLL:
             ("xo_count_xxtric", c.c_int64, [c.c_int64, _i64p, _i64p]),
             ("xo_count_merge", c.c_int64, [c.c_int64, _i64p, _i64p, c.c_void_p]),
             ("xo_local_counts", None, [c.c_int64, _i64p, _i64p, c.c_int64, _i64p, _i64p]),
+            ("xo_edge_support", None, [c.c_int64, _i64p, _i64p, _i64p]),
             ("xo_canon_csr", c.c_int64, [c.c_int64, c.c_int64, _i64p, _i64p, _i64p, _i64p]),
             ("xo_rmat_edges", None, [c.c_int, c.c_uint64, c.c_int, c.c_int, c.c_int, c.c_int, c.c_int, c.c_int64,
                                      c.c_int64, _i64p, _i64p]),
@@ -85,6 +86,15 @@ def local_counts(off: np.ndarray, tails: np.ndarray, sel: np.ndarray) -> np.ndar
     sel = np.ascontiguousarray(sel, np.int64)
     out = np.zeros(len(sel), np.int64)
     lib().xo_local_counts(len(off) - 1, off, tails, len(sel), sel, out)
+    return out
+
+
+def edge_support(off: np.ndarray, tails: np.ndarray) -> np.ndarray:
+    """Triangles on every CSR entry (a, b): |N(a) and N(b)|."""
+    off = np.ascontiguousarray(off, np.int64)
+    tails = np.ascontiguousarray(tails, np.int64)
+    out = np.zeros(len(tails), np.int64)
+    lib().xo_edge_support(len(off) - 1, off, tails, out)
     return out
 
 

@@ -148,6 +148,28 @@ void xo_local_counts(int64_t nv, const int64_t *off, const int64_t *tails, int64
   }
 }
 
+/* Triangles on every edge: for each CSR entry (a, b), |N(a) and N(b)|, by
+ * marking N(a) and counting the marked entries of N(b). The per-edge form of
+ * the per-vertex counts (a triangle credits each of its three edges). */
+void xo_edge_support(int64_t nv, const int64_t *off, const int64_t *tails, int64_t *out) {
+#pragma omp parallel
+  {
+    uint64_t *mark = (uint64_t *)calloc((size_t)(nv / 64 + 1), sizeof(uint64_t));
+#pragma omp for schedule(dynamic, 64)
+    for (int64_t a = 0; a < nv; a++) {
+      for (int64_t p = off[a]; p < off[a + 1]; p++) mark[tails[p] >> 6] |= (uint64_t)1 << (tails[p] & 63);
+      for (int64_t p = off[a]; p < off[a + 1]; p++) {
+        const int64_t b = tails[p];
+        int64_t c = 0;
+        for (int64_t j = off[b]; j < off[b + 1]; j++) c += (int64_t)((mark[tails[j] >> 6] >> (tails[j] & 63)) & 1);
+        out[p] = c;
+      }
+      for (int64_t p = off[a]; p < off[a + 1]; p++) mark[tails[p] >> 6] = 0;
+    }
+    free(mark);
+  }
+}
+
 /* ======================================================================== */
 /* canonical CSR                                                             */
 /* ======================================================================== */

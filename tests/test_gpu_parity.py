@@ -287,3 +287,57 @@ def test_each_tier_alone_vs_oracle(ctx, torch_cuda, kind):
             assert g.count_groups()[0] == expect
         finally:
             g.free()
+
+
+def oracle_support_of(off, tails, a, b):
+    """The oracle's support of undirected edges (a[i], b[i]), a < b."""
+    es = oracle.edge_support(off, tails)
+    nv = len(off) - 1
+    keys = np.repeat(np.arange(nv, dtype=np.int64), np.diff(off)) * nv + tails  # sorted: rows ascend
+    pos = np.searchsorted(keys, a.astype(np.int64) * nv + b)
+    assert (tails[pos] == b).all()
+    return es[pos]
+
+
+@pytest.mark.parametrize("name", ["k4", "k64", "iso_tail", "star_path", "er0", "rmat14", "chunglu14", "amazon0302"])
+def test_edge_support_and_clustering_vs_oracle(ctx, name):
+    f = GOLDEN[name]
+    off, tails = canon(name)
+    _, opv = oracle.count_merge(off, tails, per_vertex=True)
+    deg = np.diff(off)
+    for orient in ORIENTS:
+        g = ctx.graph_from_edges(f["nv"], FIX[name + "_src"], FIX[name + "_dst"], orient)
+        try:
+            t, sup = g.count_edges()
+            assert t == f["triangles"] and sup.sum() == 3 * t
+            a, b, s = g.edge_support()
+            assert (s == oracle_support_of(off, tails, a, b)).all()
+            assert (g.degrees() == deg).all()
+            c = g.clustering()
+            want = np.where(deg >= 2, 2.0 * opv / np.maximum(deg * (deg - 1.0), 1.0), 0.0)
+            assert np.allclose(c, want, rtol=0, atol=1e-12)
+        finally:
+            g.free()
+
+
+def test_edge_support_every_tier(ctx, torch_cuda):
+    # lane, warp and CTA tasks (hash member sets with parts on the hubs)
+    torch = torch_cuda
+    n = 1 << 15
+    cdf, m = xt.chunglu_cdf(n, 2.1, 24.0, 8192.0)
+    s = torch.empty(m, dtype=torch.int32, device="cuda")
+    d = torch.empty_like(s)
+    ctx.gen_chunglu(cdf, m, 5, s, d)
+    off, tails = oracle.canon_csr(n, s.cpu().numpy().astype(np.int64), d.cpu().numpy().astype(np.int64))
+    for orient in ORIENTS:
+        g = ctx.graph_from_device_edges(n, m, s, d, orient)
+        try:
+            ref = None
+            for lane_work, warp_work in TIERS:
+                g.set_tiers(lane_work, warp_work)
+                a, b, sup = g.edge_support()
+                if ref is None:
+                    ref = oracle_support_of(off, tails, a, b)
+                assert (sup == ref).all(), (orient, lane_work, warp_work)
+        finally:
+            g.free()

@@ -93,3 +93,17 @@ def test_local_counts_equal_per_vertex_merge_counts():
     off, tails = oracle.canon_csr(n, s, d)
     _, pv = oracle.count_merge(off, tails, per_vertex=True)
     assert (oracle.local_counts(off, tails, np.arange(n)) == pv).all()
+
+
+def test_edge_support_consistent_with_vertex_counts():
+    # every triangle puts 1 on each of its 3 edges (2 CSR entries each) and
+    # 2 on the CSR entries around each of its corners
+    n = 1 << 12
+    s, d = oracle.rmat_edges(12, 16 << 12, 3)
+    off, tails = oracle.canon_csr(n, s, d)
+    total, pv = oracle.count_merge(off, tails, per_vertex=True)
+    es = oracle.edge_support(off, tails)
+    assert es.sum() == 6 * total
+    at_v = np.zeros(n, np.int64)
+    np.add.at(at_v, np.repeat(np.arange(n), np.diff(off)), es)
+    assert (at_v == 2 * pv).all()

@@ -80,6 +80,7 @@ _proto("xt_graph_get_csr", _int, _vp, _vp, _vp)
 _proto("xt_graph_free", _int, _vp)
 _proto("xt_count", _int, _vp, _vp, _vp)
 _proto("xt_count_async", _int, _vp, _vp, _vp)
+_proto("xt_count_edges", _int, _vp, _vp, _vp)
 _proto("xt_count_device", _int, _i64, _vp, _vp, _vp, _int, _vp)
 _proto("xt_count_device_static", _int, _i64, _vp, _vp, _vp, _int, _vp)
 _proto("xt_graph_from_batch", _int, _vp, _i64, _vp, _vp, _vp, _vp, _int, _P(_vp))
@@ -116,7 +117,7 @@ _proto("xt_rgg_generate", _int, _i64, _int, _dbl, _dbl, _u64, _i64, _P(_i64), _v
 EXPORTED = ["xt_strerror", "xt_last_error", "xt_open", "xt_close", "xt_set_stream", "xt_debug_fail_alloc",
             "xt_launch_count", "xt_synchronize", "xt_graph_get_perm",
             "xt_graph_from_csr", "xt_graph_from_edges", "xt_graph_from_device_edges", "xt_graph_get_info",
-            "xt_graph_get_csr", "xt_graph_free", "xt_count", "xt_count_async", "xt_count_device",
+            "xt_graph_get_csr", "xt_graph_free", "xt_count", "xt_count_async", "xt_count_edges", "xt_count_device",
             "xt_count_device_static", "xt_graph_from_batch", "xt_graph_from_device_batch", "xt_graph_groups",
             "xt_count_groups", "xt_count_groups_async", "xt_graph_capture", "xt_graph_set_tuning", "xt_graph_set_tiers",
             "xt_mem_stats", "xt_serve_estimate", "xt_serve_open", "xt_serve_submit", "xt_serve_poll",
@@ -418,6 +419,40 @@ class DeviceGraph:
         pv = np.empty(self.nv, np.int64) if per_vertex else None
         _check(_L.xt_count(self._h, ctypes.byref(g), _ptr(pv)), "xt_count", self.ctx)
         return (g.value, pv) if per_vertex else g.value
+
+    def count_edges(self):
+        """(total, support): triangles on every oriented edge, in the order of
+        csr() (internal numbering)."""
+        g = _i64(0)
+        sup = np.empty(self.info()["n_edges"], np.int64)
+        _check(_L.xt_count_edges(self._h, ctypes.byref(g), _ptr(sup)), "xt_count_edges", self.ctx)
+        return g.value, sup
+
+    def edge_support(self):
+        """(src, dst, support) per undirected edge in INPUT ids, src < dst."""
+        off, col = self.csr()
+        _, sup = self.count_edges()
+        p = self.perm()
+        a = p[np.repeat(np.arange(len(off) - 1), np.diff(off))].astype(np.int64)
+        b = p[col].astype(np.int64)
+        return np.minimum(a, b), np.maximum(a, b), sup
+
+    def degrees(self) -> np.ndarray:
+        """Undirected degree of every vertex, input ids."""
+        off, col = self.csr()
+        d = np.diff(off) + np.bincount(col, minlength=len(off) - 1)
+        out = np.empty_like(d)
+        out[self.perm()] = d
+        return out
+
+    def clustering(self) -> np.ndarray:
+        """Local clustering coefficient 2 T(v) / (d(v) (d(v) - 1)) per vertex
+        (0 below degree 2), from the per-vertex counts."""
+        _, pv = self.count(per_vertex=True)
+        d = self.degrees().astype(np.float64)
+        with np.errstate(divide="ignore", invalid="ignore"):
+            c = np.where(d >= 2, 2.0 * pv / (d * (d - 1.0)), 0.0)
+        return c
 
     def count_async(self, d_global, d_per_vertex=None) -> None:
         _check(_L.xt_count_async(self._h, _ptr(d_global), _ptr(d_per_vertex)), "xt_count_async", self.ctx)

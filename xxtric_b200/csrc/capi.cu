@@ -328,6 +328,24 @@ xt_status xt_count(xt_graph *gr, int64_t *global, int64_t *per_vertex) {
   return s;
 }
 
+xt_status xt_count_edges(xt_graph *gr, int64_t *global, int64_t *support) {
+  if (!gr || !global || !support) return XT_ERR_INVALID;
+  Graph &g = gr->g;
+  Ctx *c = g.ctx;
+  cudaSetDevice(c->device);
+  int64_t *d = nullptr;
+  XT_TRY(dalloc_n(c, &d, size_t(1 + g.ne)));
+  xt_status s = count_graph(&g, d, nullptr, nullptr, d + 1);
+  if (s == XT_OK)
+    s = cuda_status(c, cudaMemcpyAsync(global, d, sizeof(int64_t), cudaMemcpyDeviceToHost, c->stream), "D2H");
+  if (s == XT_OK && g.ne > 0)
+    s = cuda_status(c, cudaMemcpyAsync(support, d + 1, sizeof(int64_t) * g.ne, cudaMemcpyDeviceToHost, c->stream),
+                    "D2H");
+  dfree(c, d);
+  if (s == XT_OK) s = cuda_status(c, cudaStreamSynchronize(c->stream), "count");
+  return s;
+}
+
 xt_status xt_count_device(int64_t nv, const int64_t *d_indices, const int64_t *d_edge_list, int64_t *d_count,
                           int accumulate, void *stream) {
   if (nv < 1 || !d_indices || !d_count) return XT_ERR_INVALID;

@@ -98,7 +98,7 @@ struct Plan {
   int64_t n_ttask = 0;         // lane tasks: one head per lane
   int32_t *d_tt = nullptr;
   unsigned long long *d_cursor = nullptr;  // [0] CTA, [1] warp, [2] lane task cursors
-  int grid_global = 0, grid_pv = 0;
+  int grid_global = 0, grid_pv = 0, grid_es = 0;
   int64_t block_work = 0, warp_work = 0;   // the thresholds the plan was made with
   int64_t bitmap_bits = 0;
 };
@@ -388,14 +388,33 @@ __device__ __forceinline__ int probe_pair(const int4 a, const int4 b, const Memb
          hash_test<PV>(m, b.x) + hash_test<PV>(m, b.y) + hash_test<PV>(m, b.z) + hash_test<PV>(m, b.w);
 }
 
+// Per-edge mode: a hit on column position pos0 + i (the edge u->w of the
+// triangle) is credited there and to the member's slot (the edge v->w)
+__device__ __forceinline__ int probe_pair_edges(const int4 a, const int4 b, const Members &m,
+                                                unsigned int *__restrict__ es, int64_t pos0) {
+  const int32_t x[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
+  int h = 0;
+#pragma unroll
+  for (int i = 0; i < 8; i++) {
+    if (hash_test<true>(m, x[i])) {
+      atomicAdd(&es[pos0 + i], 1u);
+      h++;
+    }
+  }
+  return h;
+}
+
 // Streams the suffixes of in-records [k0, kend) through the member set with
 // 2^lg_s lanes per record, in batches claimed from `cursor` (shared by the
 // warps of a CTA task) or taken in order (cursor null); returns this lane's
-// hits. Per-vertex mode credits each record's hits to its owner u.
-template <bool PV, bool BITMAP>
+// hits. Per-vertex mode (MODE 1) credits each record's hits to its owner u;
+// per-edge mode (MODE 2) credits them to the record's own edge u->v and each
+// hit to the edge u->w at the candidate's column.
+template <int MODE, bool BITMAP>
 __device__ __forceinline__ int64_t stream_kind(const InRec *__restrict__ rec, const int32_t *__restrict__ col,
                                                int64_t k0, int64_t kend, int lg_s, int *cursor, const Members &m,
-                                               int64_t *__restrict__ pv, int lane) {
+                                               int64_t *__restrict__ pv, unsigned int *__restrict__ es, int lane) {
+  constexpr bool PV = MODE != 0;
   const int S = 1 << lg_s;
   const int bsz = 32 >> lg_s;
   const int j = lane >> lg_s, k = lane & (S - 1);
@@ -453,12 +472,14 @@ __device__ __forceinline__ int64_t stream_kind(const InRec *__restrict__ rec, co
         load_pair(col, p0 + bp, a, b);
         mask_pair(a, b, sr - 8 * bp, er - 8 * bp);
       }
-      h += probe_pair<PV, BITMAP>(a, b, m);
+      if (MODE == 2) h += probe_pair_edges(a, b, m, es, 8 * (p0 + bp));
+      else h += probe_pair<PV, BITMAP>(a, b, m);
     }
     // interior pairs: every column is in the suffix; a lane past its last
     // pair probes sentinels
     for (int32_t it = 0; it < steps; it++) {
       const int4 a = xa, b = xb;
+      const int64_t pa = P;  // the pair in a, b
       P += S;
       if (it + 1 < cnt) {
         load_pair(col, P, xa, xb);  // next step's pair in flight during the probes
@@ -466,15 +487,17 @@ __device__ __forceinline__ int64_t stream_kind(const InRec *__restrict__ rec, co
         xa = sent;
         xb = sent;
       }
-      h += probe_pair<PV, BITMAP>(a, b, m);
+      if (MODE == 2) h += probe_pair_edges(a, b, m, es, 8 * pa);
+      else h += probe_pair<PV, BITMAP>(a, b, m);
     }
     if (PV) {
       int hr = h;
 #pragma unroll
       for (int o = 16; o; o >>= 1)
         if (o < S) hr += __shfl_down_sync(0xffffffffu, hr, o, S);
-      if (k == 0 && hr && r4.w >= 0)
+      if (MODE == 1 && k == 0 && hr && r4.w >= 0)
         atomicAdd(reinterpret_cast<unsigned long long *>(&pv[r4.w]), (unsigned long long)hr);
+      if (MODE == 2 && k == 0 && hr) atomicAdd(&es[s - 1], unsigned(hr));  // the edge u->v
     }
     hits += h;
     kb = nkb;
@@ -485,13 +508,14 @@ __device__ __forceinline__ int64_t stream_kind(const InRec *__restrict__ rec, co
   return hits;
 }
 
-template <bool PV>
+template <int MODE>
 __device__ __forceinline__ int64_t stream_suffixes(const InRec *__restrict__ rec, const int32_t *__restrict__ col,
                                                    int64_t k0, int64_t kend, int lg_s, int *cursor, const Members &m,
-                                                   int64_t *__restrict__ pv, int lane) {
+                                                   int64_t *__restrict__ pv, unsigned int *__restrict__ es,
+                                                   int lane) {
   // the membership kind is fixed per task: one specialised loop each
-  if (m.bitmap) return stream_kind<PV, true>(rec, col, k0, kend, lg_s, cursor, m, pv, lane);
-  return stream_kind<PV, false>(rec, col, k0, kend, lg_s, cursor, m, pv, lane);
+  if (MODE == 0 && m.bitmap) return stream_kind<MODE, true>(rec, col, k0, kend, lg_s, cursor, m, pv, es, lane);
+  return stream_kind<MODE, false>(rec, col, k0, kend, lg_s, cursor, m, pv, es, lane);
 }
 
 // ---- the count kernel ---------------------------------------------------------
@@ -510,6 +534,7 @@ struct CountArgs {
   unsigned long long *cursor;     // [0] CTA, [1] warp, [2] lane task cursors
   unsigned long long *global;     // the total
   int64_t *pv;                    // per-vertex counts (per-vertex mode)
+  unsigned int *es;               // per-edge counts, out-CSR order (per-edge mode)
   const int32_t *group;           // head -> group (a graph of a batch), or null
   unsigned long long *group_out;  // per-group counts when group != null
   int64_t bitmap_bits;            // largest member id range kept as a bitmap
@@ -575,14 +600,30 @@ __device__ __forceinline__ void clear_members(const Members &m, int nclear, int 
   }
 }
 
-template <bool PV>
+// Per-edge mode: adds a slot's hits to the edge v->w, w's position in the
+// task's member columns col[r0, r0 + n) found by binary search
+__device__ __forceinline__ void credit_member_edge(const int32_t *__restrict__ col, int64_t r0, int n, int32_t w,
+                                                   unsigned c, unsigned int *__restrict__ es) {
+  int lo = 0, hi = n;
+  while (lo < hi) {
+    const int mid = (lo + hi) >> 1;
+    if (col[r0 + mid] < w) lo = mid + 1;
+    else hi = mid;
+  }
+  atomicAdd(&es[r0 + lo], c);
+}
+
+// MODE 0: global count; 1: and per-vertex counts; 2: and per-edge counts
+template <int MODE>
 __global__ void __launch_bounds__(kThreads, kMinBlocks) k_count(const CountArgs a) {
   const int64_t *__restrict__ off = a.off;
   const int32_t *__restrict__ col = a.col;
   const int64_t *__restrict__ ioff = a.ioff;
   const InRec *__restrict__ rec = a.rec;
   unsigned long long *__restrict__ cursor = a.cursor;
+  constexpr bool PV = MODE != 0;  // hash member sets with per-slot hit counters
   int64_t *__restrict__ pv = a.pv;
+  unsigned int *__restrict__ es = a.es;
   extern __shared__ int32_t smem[];
   int32_t *bwords = smem;               // kBlockWords
   int32_t *bcnt = smem + kBlockWords;   // kBlockWords (per-vertex mode only)
@@ -627,7 +668,7 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) k_count(const CountArgs 
         s_soff[cur ^ 1] = so;
       }
     }
-    int64_t h = stream_suffixes<PV>(rec, col, t.k0, t.k0 + t.nrec, t.lg_s, &s_batch, m, pv, lane);
+    int64_t h = stream_suffixes<MODE>(rec, col, t.k0, t.k0 + t.nrec, t.lg_s, &s_batch, m, pv, es, lane);
     acc += h;
     if (a.group) credit_group(a, t.v, h, lane);
     if (PV) {
@@ -635,7 +676,7 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) k_count(const CountArgs 
       if (lane == 0) s_red[warp] = (unsigned long long)h;
     }
     __syncthreads();
-    if (PV) {
+    if (MODE == 1) {
       if (tid == 0) {
         unsigned long long tot = 0;
         for (int w = 0; w < kWarps; w++) tot += s_red[w];
@@ -643,8 +684,11 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) k_count(const CountArgs 
       }
       for (int i = tid; i < nclear; i += kThreads)
           if (bcnt[i]) atomicAdd(reinterpret_cast<unsigned long long *>(&pv[bwords[i]]), (unsigned long long)bcnt[i]);
-      __syncthreads();
     }
+    if (MODE == 2)
+      for (int i = tid; i < nclear; i += kThreads)
+        if (bcnt[i]) credit_member_edge(col, t.r0, t.nmem, bwords[i], unsigned(bcnt[i]), es);
+    if (PV) __syncthreads();
   }
 
   // ---- warp tasks: the CTA region split among the warps ----
@@ -666,16 +710,21 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) k_count(const CountArgs 
       for (int i = lane; i < t.nmem; i += 32) members_insert(m, mem[i]);
       __syncwarp();
       const Task tn = claim_task(&cursor[1], a.wt, a.n_wt, lane);  // read after the stream
-      int64_t h = stream_suffixes<PV>(rec, col, t.k0, t.k0 + t.nrec, t.lg_s, nullptr, m, pv, lane);
+      int64_t h = stream_suffixes<MODE>(rec, col, t.k0, t.k0 + t.nrec, t.lg_s, nullptr, m, pv, es, lane);
       acc += h;
       if (a.group) credit_group(a, t.v, h, lane);
-      if (PV) {
+      if (MODE == 1) {
         for (int o = 16; o; o >>= 1) h += __shfl_xor_sync(0xffffffffu, h, o);
         __syncwarp();
         if (lane == 0 && h) atomicAdd(reinterpret_cast<unsigned long long *>(&pv[t.v]), (unsigned long long)h);
         for (int i = lane; i < nclear; i += 32)
           if (m.cnt[i])
             atomicAdd(reinterpret_cast<unsigned long long *>(&pv[m.words[i]]), (unsigned long long)m.cnt[i]);
+      }
+      if (MODE == 2) {
+        __syncwarp();
+        for (int i = lane; i < nclear; i += 32)
+          if (m.cnt[i]) credit_member_edge(col, t.r0, t.nmem, m.words[i], unsigned(m.cnt[i]), es);
       }
       __syncwarp();
       so = stage_task(wstage, col, rec, tn, lane);
@@ -712,16 +761,21 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) k_count(const CountArgs 
         b = x;
         if (col[x] == w) {  // x < r1: w <= hi
           hu++;
-          if (PV) atomicAdd(reinterpret_cast<unsigned long long *>(&pv[w]), 1ull);
+          if (MODE == 1) atomicAdd(reinterpret_cast<unsigned long long *>(&pv[w]), 1ull);
+          if (MODE == 2) {
+            atomicAdd(&es[p], 1u);  // the edge u->w
+            atomicAdd(&es[x], 1u);  // the edge v->w
+          }
           b = x + 1;
         }
       }
       hv += hu;
-      if (PV && hu) atomicAdd(reinterpret_cast<unsigned long long *>(&pv[r.u]), (unsigned long long)hu);
+      if (MODE == 1 && hu) atomicAdd(reinterpret_cast<unsigned long long *>(&pv[r.u]), (unsigned long long)hu);
+      if (MODE == 2 && hu) atomicAdd(&es[r.s - 1], unsigned(hu));  // the edge u->v
     }
     acc += hv;
     if (hv) {
-      if (PV) atomicAdd(reinterpret_cast<unsigned long long *>(&pv[v]), (unsigned long long)hv);
+      if (MODE == 1) atomicAdd(reinterpret_cast<unsigned long long *>(&pv[v]), (unsigned long long)hv);
       if (a.group) atomicAdd(&a.group_out[a.group[v]], (unsigned long long)hv);
     }
   }
@@ -822,17 +876,18 @@ xt_status make_plan(Graph *g) {
     k_inrec_work<<<counted(c, grid_for(ne, B, c->sm_count)), B, 0, c->stream>>>(g->d_irec, ne, w);
     if ((s = exclusive_scan(c, w, P, ne + 1)) != XT_OK) break;
     // persistent grids: every CTA that fits on the device at once
-    int occ[2] = {0, 0};
-    for (int pvm = 0; pvm < 2 && s == XT_OK; pvm++) {
-      auto fn = pvm ? k_count<true> : k_count<false>;
-      const size_t bytes = count_smem_bytes(pvm != 0);
+    int occ[3] = {0, 0, 0};
+    for (int mode = 0; mode < 3 && s == XT_OK; mode++) {
+      auto fn = mode == 0 ? k_count<0> : (mode == 1 ? k_count<1> : k_count<2>);
+      const size_t bytes = count_smem_bytes(mode != 0);
       s = cuda_status(c, cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes)), "attr");
       if (s == XT_OK)
-        s = cuda_status(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ[pvm], fn, kThreads, bytes), "occ");
+        s = cuda_status(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ[mode], fn, kThreads, bytes), "occ");
     }
     if (s != XT_OK) break;
     pl->grid_global = c->sm_count * (occ[0] > 0 ? occ[0] : 1);
     pl->grid_pv = c->sm_count * (occ[1] > 0 ? occ[1] : 1);
+    pl->grid_es = c->sm_count * (occ[2] > 0 ? occ[2] : 1);
     // CTA task size: large tasks amortise the member-set build and the task
     // barrier, but every CTA should still get about 16 of them
     int64_t total_work = 0;
@@ -911,7 +966,11 @@ xt_status make_plan(Graph *g) {
   return s;
 }
 
-xt_status count_graph(Graph *g, int64_t *d_global, int64_t *d_pv, int64_t *d_groups) {
+__global__ void k_widen(const unsigned int *__restrict__ in, int64_t n, int64_t *__restrict__ out) {
+  XT_GRID_STRIDE(i, n) out[i] = int64_t(in[i]);
+}
+
+xt_status count_graph(Graph *g, int64_t *d_global, int64_t *d_pv, int64_t *d_groups, int64_t *d_support) {
   Ctx *c = g->ctx;
   if (!g->plan) XT_TRY(make_plan(g));
   Plan *pl = g->plan;
@@ -923,6 +982,12 @@ xt_status count_graph(Graph *g, int64_t *d_global, int64_t *d_pv, int64_t *d_gro
   if (d_groups) {
     if (!g->d_group) return set_error(c, XT_ERR_INVALID, "per-group counts need a graph built as a batch");
     XT_CUDA(c, cudaMemsetAsync(d_groups, 0, sizeof(int64_t) * g->n_groups, c->stream));
+  }
+  if (d_pv && d_support) return set_error(c, XT_ERR_INVALID, "per-vertex and per-edge counts are separate calls");
+  unsigned int *es = nullptr;  // per-edge counts, 32-bit while counting
+  if (d_support) {
+    XT_TRY(dalloc_n(c, &es, size_t(g->ne > 0 ? g->ne : 1)));
+    XT_CUDA(c, cudaMemsetAsync(es, 0, sizeof(unsigned int) * size_t(g->ne > 0 ? g->ne : 1), c->stream));
   }
   int64_t *pv_int = nullptr;  // per-vertex counts in internal numbering
   if (d_pv) {
@@ -944,19 +1009,25 @@ xt_status count_graph(Graph *g, int64_t *d_global, int64_t *d_pv, int64_t *d_gro
   a.cursor = pl->d_cursor;
   a.global = reinterpret_cast<unsigned long long *>(d_global);
   a.pv = pv_int;
+  a.es = es;
   a.group = d_groups ? g->d_group : nullptr;
   a.group_out = reinterpret_cast<unsigned long long *>(d_groups);
   a.bitmap_bits = pl->bitmap_bits;
   if (g->ne > 0) {
-    if (d_pv)
-      k_count<true><<<counted(c, pl->grid_pv), kThreads, count_smem_bytes(true), c->stream>>>(a);
+    if (d_support)
+      k_count<2><<<counted(c, pl->grid_es), kThreads, count_smem_bytes(true), c->stream>>>(a);
+    else if (d_pv)
+      k_count<1><<<counted(c, pl->grid_pv), kThreads, count_smem_bytes(true), c->stream>>>(a);
     else
-      k_count<false><<<counted(c, pl->grid_global), kThreads, count_smem_bytes(false), c->stream>>>(a);
+      k_count<0><<<counted(c, pl->grid_global), kThreads, count_smem_bytes(false), c->stream>>>(a);
   }
+  if (d_support && g->ne > 0)
+    k_widen<<<counted(c, grid_for(g->ne, 256, c->sm_count)), 256, 0, c->stream>>>(es, g->ne, d_support);
   if (d_pv && g->d_perm)
     k_unpermute<<<counted(c, grid_for(g->nv, 256, c->sm_count)), 256, 0, c->stream>>>(pv_int, g->d_perm, g->nv, d_pv);
   cudaError_t e = cudaGetLastError();
   if (pv_int && pv_int != d_pv) dfree(c, pv_int);
+  dfree(c, es);
   XT_CUDA(c, e);
   return XT_OK;
 }

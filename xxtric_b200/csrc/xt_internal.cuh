@@ -136,7 +136,10 @@ void free_plan(Graph *g);
 // Launches the count on the graph's context stream. d_global: one int64
 // (overwritten); d_pv: nv int64 (nullable, overwritten).
 // d_groups: n_groups int64 per-group counts (graphs built as a batch), nullable.
-xt_status count_graph(Graph *g, int64_t *d_global, int64_t *d_pv, int64_t *d_groups = nullptr);
+// d_support: ne int64, the triangles on each oriented edge in out-CSR order
+// (nullable; not together with d_pv).
+xt_status count_graph(Graph *g, int64_t *d_global, int64_t *d_pv, int64_t *d_groups = nullptr,
+                      int64_t *d_support = nullptr);
 
 }  // namespace xt
 
