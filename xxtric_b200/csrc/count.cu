@@ -56,6 +56,8 @@ constexpr int kWarpWords = kBlockWords / kWarps;  // 1024: a 1024-slot hash or a
 constexpr int kWarpDmax = kWarpWords / 4;         // hash load factor <= 1/4
 constexpr int64_t kWarpWork = XT_WARP_WORK;
 constexpr int kBlockDmax = 2048;
+// the warps' bitmap member counters share the CTA's
+static_assert(kWarps * kWarpDmax <= kBlockDmax, "warp member counters exceed the CTA's");
 constexpr int64_t kBlockWorkMin = int64_t(1) << 14;
 constexpr int64_t kBlockWorkMax = int64_t(1) << XT_BLOCK_WORK_LOG2;
 
@@ -278,7 +280,9 @@ __device__ __forceinline__ int hash_find(const int32_t *tab, uint32_t mask, int 
 // The member set N+(v) (or one part of it) in shared memory.
 struct Members {
   int32_t *words;   // bitmap words or hash slots
-  int32_t *cnt;     // per-slot hit counters (per-vertex mode, hash only)
+  int32_t *cnt;     // per-slot hit counters (per-vertex and per-edge modes, hash)
+  int32_t *pre;     // bitmap, same modes: index of the first member in each word
+  int32_t *mcnt;    // bitmap, same modes: per-member hit counters
   int32_t lo, hi;   // smallest and largest member
   uint32_t base;    // bitmap: x is bit (x & 31) of words[(x >> 5) - base]
   uint32_t nwords;  // bitmap: words in use; words[nwords] is a zero guard word
@@ -289,14 +293,16 @@ struct Members {
 
 // Chooses the structure for members mem[0, n) (ascending) that fits `words`
 // words (a bitmap only while the members' id range is at most bitmap_bits)
-// and returns how many words must be cleared.
+// and returns how many words must be cleared. In the per-vertex and
+// per-edge modes a bitmap also keeps, per word, the index of its first
+// member, so a hit finds its member's counter by a popcount.
 template <bool PV>
 __device__ __forceinline__ int members_layout(Members &m, const int32_t *mem, int n, int words, int64_t bitmap_bits) {
   m.lo = mem[0];
   m.hi = mem[n - 1];
   const int64_t range = int64_t(m.hi) - int64_t(m.lo) + 1;
   const int64_t nw = int64_t(m.hi >> 5) - int64_t(m.lo >> 5) + 1;
-  m.bitmap = !PV && nw + 1 <= int64_t(words) && range <= bitmap_bits;
+  m.bitmap = nw + 1 <= int64_t(words) && range <= bitmap_bits;
   if (m.bitmap) {
     m.base = uint32_t(m.lo >> 5);
     m.nwords = uint32_t(nw);
@@ -310,6 +316,23 @@ __device__ __forceinline__ int members_layout(Members &m, const int32_t *mem, in
   m.mask = (1u << lg) - 1;
   m.shift = 32 - lg;
   return 1 << lg;
+}
+
+// inserts member i of mem[0, n) (ascending); with ranks (per-vertex and
+// per-edge modes) also records word starts and clears the member's counter
+template <bool PV>
+__device__ __forceinline__ void members_insert_at(const Members &m, const int32_t *mem, int i) {
+  const int32_t x = mem[i];
+  if (m.bitmap) {
+    const uint32_t wd = uint32_t(x >> 5) - m.base;
+    atomicOr(reinterpret_cast<unsigned int *>(&m.words[wd]), 1u << (x & 31));
+    if (PV) {
+      if (i == 0 || uint32_t(mem[i - 1] >> 5) - m.base != wd) m.pre[wd] = i;
+      m.mcnt[i] = 0;
+    }
+  } else {
+    hash_insert(m.words, m.mask, m.shift, x);
+  }
 }
 
 __device__ __forceinline__ void members_insert(const Members &m, int32_t x) {
@@ -406,20 +429,32 @@ __device__ __forceinline__ int probe_pair(const int4 a, const int4 b, const Memb
          hash_test<PV>(m, b.x) + hash_test<PV>(m, b.y) + hash_test<PV>(m, b.z) + hash_test<PV>(m, b.w);
 }
 
-// Per-edge mode: a hit on column position pos0 + i (the edge u->w of the
-// triangle) is credited there and to the member's slot (the edge v->w)
-__device__ __forceinline__ int probe_pair_edges(const int4 a, const int4 b, const Members &m,
-                                                unsigned int *__restrict__ es, int64_t pos0) {
-  const int32_t x[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
-  int h = 0;
-#pragma unroll
-  for (int i = 0; i < 8; i++) {
-    if (hash_test<true>(m, x[i])) {
-      atomicAdd(&es[pos0 + i], 1u);
-      h++;
-    }
+// Per-vertex and per-edge modes: a hit bumps its member's counter (bitmap:
+// the member's index is the word's first index plus the set bits below;
+// hash: its slot) and, per edge, the edge u->w at column position pos
+template <int MODE, bool BITMAP>
+__device__ __forceinline__ int probe_one(const Members &m, int32_t w, unsigned int *__restrict__ es, int64_t pos) {
+  if (BITMAP) {
+    uint32_t i = uint32_t(w >> 5) - m.base;
+    i = i < m.nwords ? i : m.nwords;
+    const uint32_t x = uint32_t(m.words[i]);
+    const uint32_t bit = uint32_t(w) & 31u;
+    if (!((x >> bit) & 1u)) return 0;  // the guard word is zero: i < nwords below
+    atomicAdd(&m.mcnt[m.pre[i] + __popc(x & ((1u << bit) - 1u))], 1);
+  } else if (!hash_test<true>(m, w)) {
+    return 0;
   }
-  return h;
+  if (MODE == 2) atomicAdd(&es[pos], 1u);
+  return 1;
+}
+
+template <int MODE, bool BITMAP>
+__device__ __forceinline__ int probe_pair_counted(const int4 a, const int4 b, const Members &m,
+                                                  unsigned int *__restrict__ es, int64_t pos0) {
+  return probe_one<MODE, BITMAP>(m, a.x, es, pos0) + probe_one<MODE, BITMAP>(m, a.y, es, pos0 + 1) +
+         probe_one<MODE, BITMAP>(m, a.z, es, pos0 + 2) + probe_one<MODE, BITMAP>(m, a.w, es, pos0 + 3) +
+         probe_one<MODE, BITMAP>(m, b.x, es, pos0 + 4) + probe_one<MODE, BITMAP>(m, b.y, es, pos0 + 5) +
+         probe_one<MODE, BITMAP>(m, b.z, es, pos0 + 6) + probe_one<MODE, BITMAP>(m, b.w, es, pos0 + 7);
 }
 
 // Streams the suffixes of in-records [k0, kend) through the member set with
@@ -490,8 +525,8 @@ __device__ __forceinline__ int64_t stream_kind(const InRec *__restrict__ rec, co
         load_pair(col, p0 + bp, a, b);
         mask_pair(a, b, sr - 8 * bp, er - 8 * bp);
       }
-      if (MODE == 2) h += probe_pair_edges(a, b, m, es, 8 * (p0 + bp));
-      else h += probe_pair<PV, BITMAP>(a, b, m);
+      if (PV) h += probe_pair_counted<MODE, BITMAP>(a, b, m, es, 8 * (p0 + bp));
+      else h += probe_pair<false, BITMAP>(a, b, m);
     }
     // interior pairs: every column is in the suffix; a lane past its last
     // pair probes sentinels
@@ -505,8 +540,8 @@ __device__ __forceinline__ int64_t stream_kind(const InRec *__restrict__ rec, co
         xa = sent;
         xb = sent;
       }
-      if (MODE == 2) h += probe_pair_edges(a, b, m, es, 8 * pa);
-      else h += probe_pair<PV, BITMAP>(a, b, m);
+      if (PV) h += probe_pair_counted<MODE, BITMAP>(a, b, m, es, 8 * pa);
+      else h += probe_pair<false, BITMAP>(a, b, m);
     }
     if (PV) {
       int hr = h;
@@ -532,7 +567,7 @@ __device__ __forceinline__ int64_t stream_suffixes(const InRec *__restrict__ rec
                                                    int64_t *__restrict__ pv, unsigned int *__restrict__ es,
                                                    int lane) {
   // the membership kind is fixed per task: one specialised loop each
-  if (MODE == 0 && m.bitmap) return stream_kind<MODE, true>(rec, col, k0, kend, lg_s, cursor, m, pv, es, lane);
+  if (m.bitmap) return stream_kind<MODE, true>(rec, col, k0, kend, lg_s, cursor, m, pv, es, lane);
   return stream_kind<MODE, false>(rec, col, k0, kend, lg_s, cursor, m, pv, es, lane);
 }
 
@@ -614,7 +649,7 @@ template <bool PV>
 __device__ __forceinline__ void clear_members(const Members &m, int nclear, int t, int nt) {
   for (int i = t; i < nclear; i += nt) {
     m.words[i] = m.bitmap ? 0 : kEmpty;
-    if (PV) m.cnt[i] = 0;
+    if (PV && !m.bitmap) m.cnt[i] = 0;
   }
 }
 
@@ -644,7 +679,8 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) k_count(const CountArgs 
   unsigned int *__restrict__ es = a.es;
   extern __shared__ int32_t smem[];
   int32_t *bwords = smem;               // kBlockWords
-  int32_t *bcnt = smem + kBlockWords;   // kBlockWords (per-vertex mode only)
+  int32_t *bcnt = smem + kBlockWords;   // kBlockWords: hash counters or bitmap word starts (modes 1, 2)
+  int32_t *bmcnt = smem + 2 * kBlockWords;  // kBlockDmax: bitmap member counters (modes 1, 2)
   __shared__ __align__(16) int32_t s_stage[kStageInts];
   __shared__ Task s_task[2];
   __shared__ int s_soff[2];
@@ -673,10 +709,12 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) k_count(const CountArgs 
     Members m;
     m.words = bwords;
     m.cnt = bcnt;
+    m.pre = bcnt;
+    m.mcnt = bmcnt;
     const int nclear = members_layout<PV>(m, mem, t.nmem, kBlockWords, a.bitmap_bits);
     clear_members<PV>(m, nclear, tid, kThreads);
     __syncthreads();
-    for (int i = tid; i < t.nmem; i += kThreads) members_insert(m, mem[i]);
+    for (int i = tid; i < t.nmem; i += kThreads) members_insert_at<PV>(m, mem, i);
     __syncthreads();
     if (warp == 0) {  // stage is free again: bring in the next task
       const Task tn = claim_task(&cursor[0], a.bt, a.n_bt, lane);
@@ -700,12 +738,23 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) k_count(const CountArgs 
         for (int w = 0; w < kWarps; w++) tot += s_red[w];
         if (tot) atomicAdd(reinterpret_cast<unsigned long long *>(&pv[t.v]), tot);
       }
-      for (int i = tid; i < nclear; i += kThreads)
+      if (m.bitmap) {
+        for (int i = tid; i < t.nmem; i += kThreads)
+          if (bmcnt[i]) atomicAdd(reinterpret_cast<unsigned long long *>(&pv[col[t.r0 + i]]), (unsigned long long)bmcnt[i]);
+      } else {
+        for (int i = tid; i < nclear; i += kThreads)
           if (bcnt[i]) atomicAdd(reinterpret_cast<unsigned long long *>(&pv[bwords[i]]), (unsigned long long)bcnt[i]);
+      }
     }
-    if (MODE == 2)
-      for (int i = tid; i < nclear; i += kThreads)
-        if (bcnt[i]) credit_member_edge(col, t.r0, t.nmem, bwords[i], unsigned(bcnt[i]), es);
+    if (MODE == 2) {
+      if (m.bitmap) {
+        for (int i = tid; i < t.nmem; i += kThreads)
+          if (bmcnt[i]) atomicAdd(&es[t.r0 + i], unsigned(bmcnt[i]));
+      } else {
+        for (int i = tid; i < nclear; i += kThreads)
+          if (bcnt[i]) credit_member_edge(col, t.r0, t.nmem, bwords[i], unsigned(bcnt[i]), es);
+      }
+    }
     if (PV) __syncthreads();
   }
 
@@ -722,10 +771,12 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) k_count(const CountArgs 
       Members m;
       m.words = bwords + warp * kWarpWords;
       m.cnt = bcnt + warp * kWarpWords;
+      m.pre = m.cnt;
+      m.mcnt = bmcnt + warp * kWarpDmax;
       const int nclear = members_layout<PV>(m, mem, t.nmem, kWarpWords, a.bitmap_bits);
       clear_members<PV>(m, nclear, lane, 32);
       __syncwarp();
-      for (int i = lane; i < t.nmem; i += 32) members_insert(m, mem[i]);
+      for (int i = lane; i < t.nmem; i += 32) members_insert_at<PV>(m, mem, i);
       __syncwarp();
       const Task tn = claim_task(&cursor[1], a.wt, a.n_wt, lane);  // read after the stream
       int64_t h = stream_suffixes<MODE>(rec, col, t.k0, t.k0 + t.nrec, t.lg_s, nullptr, m, pv, es, lane);
@@ -735,14 +786,25 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) k_count(const CountArgs 
         for (int o = 16; o; o >>= 1) h += __shfl_xor_sync(0xffffffffu, h, o);
         __syncwarp();
         if (lane == 0 && h) atomicAdd(reinterpret_cast<unsigned long long *>(&pv[t.v]), (unsigned long long)h);
-        for (int i = lane; i < nclear; i += 32)
-          if (m.cnt[i])
-            atomicAdd(reinterpret_cast<unsigned long long *>(&pv[m.words[i]]), (unsigned long long)m.cnt[i]);
+        if (m.bitmap) {
+          for (int i = lane; i < t.nmem; i += 32)
+            if (m.mcnt[i])
+              atomicAdd(reinterpret_cast<unsigned long long *>(&pv[mem[i]]), (unsigned long long)m.mcnt[i]);
+        } else {
+          for (int i = lane; i < nclear; i += 32)
+            if (m.cnt[i])
+              atomicAdd(reinterpret_cast<unsigned long long *>(&pv[m.words[i]]), (unsigned long long)m.cnt[i]);
+        }
       }
       if (MODE == 2) {
         __syncwarp();
-        for (int i = lane; i < nclear; i += 32)
-          if (m.cnt[i]) credit_member_edge(col, t.r0, t.nmem, m.words[i], unsigned(m.cnt[i]), es);
+        if (m.bitmap) {
+          for (int i = lane; i < t.nmem; i += 32)
+            if (m.mcnt[i]) atomicAdd(&es[t.r0 + i], unsigned(m.mcnt[i]));
+        } else {
+          for (int i = lane; i < nclear; i += 32)
+            if (m.cnt[i]) credit_member_edge(col, t.r0, t.nmem, m.words[i], unsigned(m.cnt[i]), es);
+        }
       }
       __syncwarp();
       so = stage_task(wstage, col, rec, tn, lane);
@@ -810,7 +872,11 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) k_count(const CountArgs 
   }
 }
 
-static size_t count_smem_bytes(bool pv) { return sizeof(int32_t) * size_t(pv ? 2 : 1) * kBlockWords; }
+// dynamic shared memory: member words; in modes 1 and 2 also hash counters
+// or bitmap word starts, and bitmap member counters
+static size_t count_smem_bytes(bool pv) {
+  return sizeof(int32_t) * (pv ? size_t(2) * kBlockWords + kBlockDmax : size_t(kBlockWords));
+}
 
 // per-vertex counts in internal numbering -> input numbering
 __global__ void k_unpermute(const int64_t *__restrict__ in, const int32_t *__restrict__ n2o, int64_t nv,
