@@ -369,25 +369,9 @@ __device__ __forceinline__ void load_pair(const int32_t *__restrict__ col, int64
 }
 
 // Asks L2 to fetch [p, p + bytes) (16-byte aligned, a multiple of 16 bytes)
-// without waiting for it: the suffixes of the next batch are on their way to
-// L2 while this batch streams.
-#ifndef XT_L2_PREFETCH
-#define XT_L2_PREFETCH 1
-#endif
+// without waiting for it.
 __device__ __forceinline__ void prefetch_l2(const void *p, uint32_t bytes) {
   asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
-}
-
-// the pairs of a record's suffix, and L2 prefetch of them by the record's lane k
-__device__ __forceinline__ void prefetch_suffix(const int32_t *__restrict__ col, int4 r4, int k, int S) {
-  if (!XT_L2_PREFETCH || r4.z <= 0) return;
-  const int64_t s = int64_t(uint32_t(r4.x)) | (int64_t(r4.y) << 32);
-  const int64_t p0 = s >> 3, np = ((s & 7) + r4.z + 7) >> 3;
-  // lane k takes pieces k, k+S, ... of up to 4 KiB (128 pairs)
-  for (int64_t q = int64_t(k) * 128; q < np; q += int64_t(S) * 128) {
-    const int64_t n = np - q < 128 ? np - q : 128;
-    prefetch_l2(reinterpret_cast<const int4 *>(col) + 2 * (p0 + q), uint32_t(n * 32));
-  }
 }
 
 // keeps the columns i with lo <= i < hi
@@ -489,18 +473,17 @@ __device__ __forceinline__ int64_t stream_kind(const InRec *__restrict__ rec, co
     const int32_t r = base + j;
     return r < nrec ? __ldg(reinterpret_cast<const int4 *>(rec) + r) : make_int4(0, 0, 0, -1);
   };
-  // records are loaded two batches ahead and their suffixes sent to L2 one
-  // batch ahead
+  // records are loaded two batches ahead (an L2 prefetch of the next batch's
+  // suffixes cost more instructions than the latency it hid: s24 38.5 ms
+  // with it, 36.2 ms without)
   int32_t kb = claim();
   int4 r4 = fetch(kb);
   int32_t nkb = claim();
   int4 n4 = fetch(nkb);
-  prefetch_suffix(col, r4, k, S);
   int64_t hits = 0;
   while (kb < nrec) {  // warp-uniform
     const int32_t nnkb = claim();
     const int4 nn4 = fetch(nnkb);
-    prefetch_suffix(col, n4, k, S);
     const int64_t s = int64_t(uint32_t(r4.x)) | (int64_t(r4.y) << 32);
     const int64_t p0 = s >> 3;          // the suffix's first pair
     const int32_t sr = int32_t(s & 7);  // suffix [sr, er) relative to that pair
