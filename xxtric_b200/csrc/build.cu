@@ -155,6 +155,24 @@ __global__ void k_degree_from_off(const int64_t *__restrict__ off, int64_t nv, i
   XT_GRID_STRIDE(i, nv) deg[i] = int32_t(off[i + 1] - off[i]);
 }
 
+// padded row lengths: each row rounded up to a multiple of 8 columns
+__global__ void k_pad_len(const int64_t *__restrict__ off, int64_t nv, int64_t *__restrict__ plen) {
+  XT_GRID_STRIDE(u, nv) plen[u] = (off[u + 1] - off[u] + 7) & ~int64_t(7);
+}
+
+// row u of col -> colp[poff[u] ...], the rest of its padded span kPadSentinel
+// (a warp per row)
+__global__ void k_pad_scatter(const int64_t *__restrict__ off, const int32_t *__restrict__ col, int64_t nv,
+                              const int64_t *__restrict__ poff, int32_t *__restrict__ colp) {
+  const int lane = threadIdx.x & 31;
+  const int64_t warp = (blockIdx.x * int64_t(blockDim.x) + threadIdx.x) >> 5;
+  const int64_t nwarps = (int64_t(gridDim.x) * blockDim.x) >> 5;
+  for (int64_t u = warp; u < nv; u += nwarps) {
+    const int64_t a = off[u], len = off[u + 1] - a, q = poff[u], plen = poff[u + 1] - q;
+    for (int64_t i = lane; i < plen; i += 32) colp[q + i] = i < len ? col[a + i] : kPadSentinel;
+  }
+}
+
 // Suffix-length class, longest first: 127 - c where c is the length itself
 // below 32 and four classes per octave above, so records of one head sort
 // into runs of similar length.
@@ -186,15 +204,17 @@ __global__ void k_in_keys(const int32_t *__restrict__ col, const int32_t *__rest
   }
 }
 
-// positions sorted by (head, class) -> in-records (suffix of N+(u) after the head)
+// positions sorted by (head, class) -> in-records (suffix of N+(u) after the
+// head, as a position in the padded column array)
 template <class V>
 __global__ void k_in_records(const V *__restrict__ pos, int64_t m, const int32_t *__restrict__ rowof,
-                             const int64_t *__restrict__ off, InRec *__restrict__ rec) {
+                             const int64_t *__restrict__ off, const int64_t *__restrict__ poff,
+                             InRec *__restrict__ rec) {
   XT_GRID_STRIDE(i, m) {
     const int64_t p = int64_t(pos[i]);
     const int32_t u = rowof[p];
     InRec r;
-    r.s = p + 1;
+    r.s = poff[u] + (p - off[u]) + 1;
     r.len = int32_t(off[u + 1] - p - 1);
     r.u = u;
     rec[i] = r;
@@ -275,6 +295,17 @@ static xt_status keys_to_csr(Ctx *c, const K *keys, int64_t m, int64_t nv, int b
   return s;
 }
 
+static xt_status exclusive_scan_i64(Ctx *c, const int64_t *in, int64_t *out, int64_t n) {
+  size_t bytes = 0;
+  XT_CUDA(c, cub::DeviceScan::ExclusiveSum(nullptr, bytes, in, out, n, c->stream));
+  void *tmp = nullptr;
+  XT_TRY(dalloc(c, &tmp, bytes));
+  cudaError_t e = cub::DeviceScan::ExclusiveSum(tmp, bytes, in, out, n, c->stream);
+  dfree(c, tmp);
+  XT_CUDA(c, e);
+  return XT_OK;
+}
+
 static xt_status check_err(Ctx *c, const char *what) {
   int h = 0;
   XT_CUDA(c, cudaMemcpyAsync(&h, c->d_err, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
@@ -346,7 +377,7 @@ static xt_status build_in_records(Ctx *c, uint64_t *keys, uint64_t *spare, int64
   if (s == XT_OK) s = keys_to_csr<uint32_t>(c, kout, m, nv, lb, g->d_ioff, nullptr);
   if (s == XT_OK) {
     k_in_records<V><<<counted(c, grid_for(m, B, c->sm_count)), B, 0, c->stream>>>(vout, m, rowof, g->d_off,
-                                                                                   g->d_irec);
+                                                                                   g->d_poff, g->d_irec);
     s = cuda_status(c, cudaGetLastError(), "in-records");
   }
   dfree(c, rowof);
@@ -365,6 +396,28 @@ static xt_status finish_csr(Ctx *c, uint64_t *keys, uint64_t *spare, int64_t m, 
   XT_TRY(dalloc_n(c, &g->d_col, size_t(m) + kColPad));
   XT_CUDA(c, cudaMemsetAsync(g->d_col + m, 0xff, sizeof(int32_t) * kColPad, c->stream));
   XT_TRY(keys_to_csr<uint64_t>(c, keys, m, nv, b, g->d_off, g->d_col));
+  // padded columns: row starts on 8-column boundaries
+  {
+    const int B = 256;
+    int64_t *plen = nullptr;
+    XT_TRY(dalloc_n(c, &g->d_poff, size_t(nv + 1)));
+    XT_TRY(dalloc_n(c, &plen, size_t(nv + 1)));
+    k_pad_len<<<counted(c, grid_for(nv, B, c->sm_count)), B, 0, c->stream>>>(g->d_off, nv, plen);
+    xt_status s = cuda_status(c, cudaMemsetAsync(plen + nv, 0, sizeof(int64_t), c->stream), "memset");
+    if (s == XT_OK) s = exclusive_scan_i64(c, plen, g->d_poff, nv + 1);
+    int64_t total = 0;
+    if (s == XT_OK)
+      s = cuda_status(c, cudaMemcpyAsync(&total, g->d_poff + nv, sizeof(int64_t), cudaMemcpyDeviceToHost, c->stream),
+                      "D2H");
+    if (s == XT_OK) s = cuda_status(c, cudaStreamSynchronize(c->stream), "sync");
+    dfree(c, plen);
+    XT_TRY(s);
+    XT_TRY(dalloc_n(c, &g->d_colp, size_t(total > 0 ? total : 8)));
+    if (total > 0)
+      k_pad_scatter<<<counted(c, grid_for(nv * 32, B, c->sm_count)), B, 0, c->stream>>>(g->d_off, g->d_col, nv,
+                                                                                       g->d_poff, g->d_colp);
+    XT_CUDA(c, cudaGetLastError());
+  }
   XT_TRY(dalloc_n(c, &g->d_ioff, size_t(nv + 1)));
   XT_TRY(dalloc_n(c, &g->d_irec, size_t(m > 0 ? m : 1)));
   if (m == 0) {
@@ -513,12 +566,16 @@ void free_graph_device(Graph *g) {
   dfree(g->ctx, g->d_col);
   dfree(g->ctx, g->d_ioff);
   dfree(g->ctx, g->d_irec);
+  dfree(g->ctx, g->d_colp);
+  dfree(g->ctx, g->d_poff);
   dfree(g->ctx, g->d_perm);
   dfree(g->ctx, g->d_group);
   g->d_off = nullptr;
   g->d_col = nullptr;
   g->d_ioff = nullptr;
   g->d_irec = nullptr;
+  g->d_colp = nullptr;
+  g->d_poff = nullptr;
   g->d_perm = nullptr;
   g->d_group = nullptr;
 }

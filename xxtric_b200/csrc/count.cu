@@ -345,16 +345,15 @@ __device__ __forceinline__ void members_insert(const Members &m, int32_t x) {
 
 // ---- streaming the in-record suffixes ----------------------------------------
 //
-// A pair is an aligned 32-byte block of 8 columns (one 256-bit load). A
-// record's suffix covers pairs 0 .. np-1; only its first and last pair can
-// hold columns outside the suffix (the head's side of row u, the next row).
-// A batch holds 32/S records. The S lanes of record j stream its INTERIOR
-// pairs 1, ..., np-2 — lane k takes 1+k, 1+k+S, ... — with no per-column
-// test; the two boundary pairs are masked (columns outside the suffix become
-// a sentinel that no membership test accepts) and probed in one extra step
-// (two when S = 1). Records of a head are stored longest first, so the lanes
-// of a batch run for about as many steps.
-constexpr int32_t kSentinel = -2;  // negative: below every member, and not kEmpty
+// A pair is an aligned 32-byte block of 8 columns (one 256-bit load) of the
+// padded column array, where every row starts on a pair boundary and is
+// padded with sentinels. A record's suffix covers pairs 0 .. np-1 of its
+// row; the columns before the suffix in pair 0 are the row's own ids up to
+// the head (below every member of N+(head)) and those after it in the last
+// pair are sentinels, so no pair needs masking. A batch holds 32/S records;
+// the S lanes of record j take its pairs k, k+S, ... Records of a head are
+// stored longest first, so the lanes of a batch run for about as many steps.
+constexpr int32_t kSentinel = kPadSentinel;  // negative: below every member, and not kEmpty
 // positions inside one suffix are int32: out-degrees stay below this
 constexpr int64_t kMaxOutDegree = int64_t(1) << 30;
 
@@ -372,17 +371,6 @@ __device__ __forceinline__ void load_pair(const int32_t *__restrict__ col, int64
 // without waiting for it.
 __device__ __forceinline__ void prefetch_l2(const void *p, uint32_t bytes) {
   asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
-}
-
-// keeps the columns i with lo <= i < hi
-__device__ __forceinline__ void mask_pair(int4 &a, int4 &b, int32_t lo, int32_t hi) {
-  int32_t *x = reinterpret_cast<int32_t *>(&a);
-  int32_t *y = reinterpret_cast<int32_t *>(&b);
-#pragma unroll
-  for (int i = 0; i < 4; i++) {
-    if (uint32_t(i - lo) >= uint32_t(hi - lo)) x[i] = kSentinel;
-    if (uint32_t(i + 4 - lo) >= uint32_t(hi - lo)) y[i] = kSentinel;
-  }
 }
 
 // bitmap membership: bit (w & 31) of word (w >> 5) - base; every w outside
@@ -448,9 +436,11 @@ __device__ __forceinline__ int probe_pair_counted(const int4 a, const int4 b, co
 // per-edge mode (MODE 2) credits them to the record's own edge u->v and each
 // hit to the edge u->w at the candidate's column.
 template <int MODE, bool BITMAP>
-__device__ __forceinline__ int64_t stream_kind(const InRec *__restrict__ rec, const int32_t *__restrict__ col,
+__device__ __forceinline__ int64_t stream_kind(const InRec *__restrict__ rec, const int32_t *__restrict__ colp,
                                                int64_t k0, int64_t kend, int lg_s, int *cursor, const Members &m,
-                                               int64_t *__restrict__ pv, unsigned int *__restrict__ es, int lane) {
+                                               int64_t *__restrict__ pv, unsigned int *__restrict__ es,
+                                               const int64_t *__restrict__ off, const int64_t *__restrict__ poff,
+                                               int lane) {
   constexpr bool PV = MODE != 0;
   const int S = 1 << lg_s;
   const int bsz = 32 >> lg_s;
@@ -485,45 +475,27 @@ __device__ __forceinline__ int64_t stream_kind(const InRec *__restrict__ rec, co
     const int32_t nnkb = claim();
     const int4 nn4 = fetch(nnkb);
     const int64_t s = int64_t(uint32_t(r4.x)) | (int64_t(r4.y) << 32);
-    const int64_t p0 = s >> 3;          // the suffix's first pair
-    const int32_t sr = int32_t(s & 7);  // suffix [sr, er) relative to that pair
-    const int32_t er = sr + r4.z;
-    const int32_t np = r4.z > 0 ? (er + 7) >> 3 : 0;
-    const int32_t ni = np > 2 ? np - 2 : 0;                         // interior pairs
-    const int32_t cnt = ni > k ? ((ni - k + S - 1) >> lg_s) : 0;  // this lane's
+    const int32_t np = r4.z > 0 ? (int32_t(s & 7) + r4.z + 7) >> 3 : 0;  // pairs of the suffix
+    const int32_t cnt = np > k ? ((np - k + S - 1) >> lg_s) : 0;            // this lane's
     const int32_t steps = int32_t(__reduce_max_sync(0xffffffffu, uint32_t(cnt)));
-    int64_t P = p0 + 1 + k;
+    // per-edge mode: column positions of the unpadded CSR, row u's shift
+    const int64_t dpos = (MODE == 2 && np > 0) ? off[r4.w] - poff[r4.w] : 0;
+    int64_t P = (s >> 3) + k;
     int4 xa = sent, xb = sent;
-    if (cnt > 0) load_pair(col, P, xa, xb);  // in flight during the boundary step(s)
+    if (cnt > 0) load_pair(colp, P, xa, xb);
     int h = 0;
-    // boundary pairs: with S >= 2 lane k = 0 takes pair 0 and lane k = 1 pair
-    // np-1, in one step; with S = 1 the lane takes both, in two
-    const int nbs = S >= 2 ? 1 : 2;
-    for (int t = 0; t < nbs; t++) {
-      const int which = S >= 2 ? k : t;  // 0: first pair, 1: last pair
-      const bool ok = which == 0 ? np >= 1 : (which == 1 && np >= 2);
-      const int32_t bp = which == 0 ? 0 : np - 1;
-      int4 a = sent, b = sent;
-      if (ok) {
-        load_pair(col, p0 + bp, a, b);
-        mask_pair(a, b, sr - 8 * bp, er - 8 * bp);
-      }
-      if (PV) h += probe_pair_counted<MODE, BITMAP>(a, b, m, es, 8 * (p0 + bp));
-      else h += probe_pair<false, BITMAP>(a, b, m);
-    }
-    // interior pairs: every column is in the suffix; a lane past its last
-    // pair probes sentinels
+    // a lane past its last pair probes sentinels
     for (int32_t it = 0; it < steps; it++) {
       const int4 a = xa, b = xb;
       const int64_t pa = P;  // the pair in a, b
       P += S;
       if (it + 1 < cnt) {
-        load_pair(col, P, xa, xb);  // next step's pair in flight during the probes
+        load_pair(colp, P, xa, xb);  // next step's pair in flight during the probes
       } else {
         xa = sent;
         xb = sent;
       }
-      if (PV) h += probe_pair_counted<MODE, BITMAP>(a, b, m, es, 8 * pa);
+      if (PV) h += probe_pair_counted<MODE, BITMAP>(a, b, m, es, 8 * pa + dpos);
       else h += probe_pair<false, BITMAP>(a, b, m);
     }
     if (PV) {
@@ -533,7 +505,7 @@ __device__ __forceinline__ int64_t stream_kind(const InRec *__restrict__ rec, co
         if (o < S) hr += __shfl_down_sync(0xffffffffu, hr, o, S);
       if (MODE == 1 && k == 0 && hr && r4.w >= 0)
         atomicAdd(reinterpret_cast<unsigned long long *>(&pv[r4.w]), (unsigned long long)hr);
-      if (MODE == 2 && k == 0 && hr) atomicAdd(&es[s - 1], unsigned(hr));  // the edge u->v
+      if (MODE == 2 && k == 0 && hr) atomicAdd(&es[s - 1 + dpos], unsigned(hr));  // the edge u->v
     }
     hits += h;
     kb = nkb;
@@ -545,13 +517,14 @@ __device__ __forceinline__ int64_t stream_kind(const InRec *__restrict__ rec, co
 }
 
 template <int MODE>
-__device__ __forceinline__ int64_t stream_suffixes(const InRec *__restrict__ rec, const int32_t *__restrict__ col,
+__device__ __forceinline__ int64_t stream_suffixes(const InRec *__restrict__ rec, const int32_t *__restrict__ colp,
                                                    int64_t k0, int64_t kend, int lg_s, int *cursor, const Members &m,
                                                    int64_t *__restrict__ pv, unsigned int *__restrict__ es,
+                                                   const int64_t *__restrict__ off, const int64_t *__restrict__ poff,
                                                    int lane) {
   // the membership kind is fixed per task: one specialised loop each
-  if (m.bitmap) return stream_kind<MODE, true>(rec, col, k0, kend, lg_s, cursor, m, pv, es, lane);
-  return stream_kind<MODE, false>(rec, col, k0, kend, lg_s, cursor, m, pv, es, lane);
+  if (m.bitmap) return stream_kind<MODE, true>(rec, colp, k0, kend, lg_s, cursor, m, pv, es, off, poff, lane);
+  return stream_kind<MODE, false>(rec, colp, k0, kend, lg_s, cursor, m, pv, es, off, poff, lane);
 }
 
 // ---- the count kernel ---------------------------------------------------------
@@ -559,6 +532,8 @@ __device__ __forceinline__ int64_t stream_suffixes(const InRec *__restrict__ rec
 struct CountArgs {
   const int64_t *off;
   const int32_t *col;
+  const int32_t *colp;  // padded columns (suffixes are streamed from here)
+  const int64_t *poff;  // padded row starts
   const int64_t *ioff;
   const InRec *rec;
   const Task *bt;  // CTA tasks
@@ -707,7 +682,8 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) k_count(const CountArgs 
         s_soff[cur ^ 1] = so;
       }
     }
-    int64_t h = stream_suffixes<MODE>(rec, col, t.k0, t.k0 + t.nrec, t.lg_s, &s_batch, m, pv, es, lane);
+    int64_t h = stream_suffixes<MODE>(rec, a.colp, t.k0, t.k0 + t.nrec, t.lg_s, &s_batch, m, pv, es, off, a.poff,
+                                      lane);
     acc += h;
     if (a.group) credit_group(a, t.v, h, lane);
     if (PV) {
@@ -762,7 +738,8 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) k_count(const CountArgs 
       for (int i = lane; i < t.nmem; i += 32) members_insert_at<PV>(m, mem, i);
       __syncwarp();
       const Task tn = claim_task(&cursor[1], a.wt, a.n_wt, lane);  // read after the stream
-      int64_t h = stream_suffixes<MODE>(rec, col, t.k0, t.k0 + t.nrec, t.lg_s, nullptr, m, pv, es, lane);
+      int64_t h = stream_suffixes<MODE>(rec, a.colp, t.k0, t.k0 + t.nrec, t.lg_s, nullptr, m, pv, es, off, a.poff,
+                                        lane);
       acc += h;
       if (a.group) credit_group(a, t.v, h, lane);
       if (MODE == 1) {
@@ -807,12 +784,15 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) k_count(const CountArgs 
     const int64_t r0 = off[v], r1 = off[v + 1];
     const int32_t lo = col[r0], hi = col[r1 - 1];
     int64_t hv = 0;
+    const int32_t *__restrict__ colp = a.colp;
     for (int64_t k = ioff[v]; k < ioff[v + 1]; k++) {
       const InRec r = rec[k];
+      // per-edge mode: row u's shift from padded to unpadded positions
+      const int64_t dpos = MODE == 2 ? off[r.u] - a.poff[r.u] : 0;
       int64_t b = r0;  // members below b are below every remaining candidate
       int32_t hu = 0;
       for (int64_t p = r.s; p < r.s + r.len; p++) {
-        const int32_t w = col[p];
+        const int32_t w = colp[p];
         if (w > hi) break;  // the suffix ascends
         if (w < lo) continue;
         int64_t x = b, y = r1;
@@ -826,7 +806,7 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) k_count(const CountArgs 
           hu++;
           if (MODE == 1) atomicAdd(reinterpret_cast<unsigned long long *>(&pv[w]), 1ull);
           if (MODE == 2) {
-            atomicAdd(&es[p], 1u);  // the edge u->w
+            atomicAdd(&es[p + dpos], 1u);  // the edge u->w
             atomicAdd(&es[x], 1u);  // the edge v->w
           }
           b = x + 1;
@@ -834,7 +814,7 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) k_count(const CountArgs 
       }
       hv += hu;
       if (MODE == 1 && hu) atomicAdd(reinterpret_cast<unsigned long long *>(&pv[r.u]), (unsigned long long)hu);
-      if (MODE == 2 && hu) atomicAdd(&es[r.s - 1], unsigned(hu));  // the edge u->v
+      if (MODE == 2 && hu) atomicAdd(&es[r.s - 1 + dpos], unsigned(hu));  // the edge u->v
     }
     acc += hv;
     if (hv) {
@@ -1075,8 +1055,8 @@ xt_status count_graph(Graph *g, int64_t *d_global, int64_t *d_pv, int64_t *d_gro
   if (!g->plan) XT_TRY(make_plan(g));
   Plan *pl = g->plan;
   // pairs of columns are read with 32-byte vector loads
-  if (reinterpret_cast<uintptr_t>(g->d_col) % 32 != 0)
-    return set_error(c, XT_ERR_CUDA, "column array is not 32-byte aligned");
+  if (reinterpret_cast<uintptr_t>(g->d_colp) % 32 != 0)
+    return set_error(c, XT_ERR_CUDA, "padded column array is not 32-byte aligned");
   XT_CUDA(c, cudaMemsetAsync(pl->d_cursor, 0, 3 * sizeof(unsigned long long), c->stream));
   XT_CUDA(c, cudaMemsetAsync(d_global, 0, sizeof(int64_t), c->stream));
   if (d_groups) {
@@ -1098,6 +1078,8 @@ xt_status count_graph(Graph *g, int64_t *d_global, int64_t *d_pv, int64_t *d_gro
   CountArgs a;
   a.off = g->d_off;
   a.col = g->d_col;
+  a.colp = g->d_colp;
+  a.poff = g->d_poff;
   a.ioff = g->d_ioff;
   a.rec = g->d_irec;
   a.bt = pl->d_bt;

@@ -30,7 +30,8 @@ using Clock = std::chrono::steady_clock;
 // edge rows is copied in, built and counted. The builder's largest phase is
 // its row sort: 8 B/row copied in, 8 B/row union ids (batches), 16 B/row key
 // buffers, 1 B/row flags and 8 B/row sort scratch (41 B/row); the in-record
-// phase holds less (16 B/row keys + 32 B per unique edge). Vertex arrays
+// phase holds less (16 B/row keys + 36 B per unique edge, the padded columns
+// included). Vertex arrays
 // stay below 120 B/vertex through the plan. 72 B/row leaves room for CUB's
 // scratch on top of these.
 int64_t serve_estimate(int64_t nv, int64_t ne) {

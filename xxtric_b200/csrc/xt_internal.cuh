@@ -70,8 +70,13 @@ xt_status set_error(Ctx *c, xt_status s, const std::string &msg);
 // ---- oriented graph on the device ------------------------------------------
 struct Plan;  // degree-binned schedule, built once per graph
 
+// Pad value of the padded column array: negative, so below every vertex id
+// (no membership test accepts it).
+constexpr int32_t kPadSentinel = -2;
+
 // In-record of edge u->v, stored with the head v: the columns of N+(u) that
-// rank above v, i.e. the suffix d_col[s, s+len) after v's own position.
+// rank above v, i.e. the suffix d_colp[s, s+len) after v's own position
+// (s indexes the padded column array).
 // Every triangle (u,v,w) has its w in exactly this suffix and in N+(v).
 struct __align__(16) InRec {
   int64_t s;
@@ -93,6 +98,11 @@ struct Graph {
   int32_t *d_col = nullptr;   // out-CSR columns N+(u), ne (+kColPad), rows ascending
   int64_t *d_ioff = nullptr;  // in-record offsets per head v, nv+1
   InRec *d_irec = nullptr;    // one record per edge u->v, grouped by v
+  // The columns again, each row starting on an 8-column (32-byte) boundary
+  // and padded with kPadSentinel: the count streams suffixes from here in
+  // whole 32-byte pairs without masking. d_poff[u] is row u's start.
+  int32_t *d_colp = nullptr;
+  int64_t *d_poff = nullptr;  // nv+1
   int32_t *d_perm = nullptr;  // internal id -> input id (null when identity)
   int64_t max_degree = 0;
   int64_t max_out_degree = 0;
