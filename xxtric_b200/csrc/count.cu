@@ -37,7 +37,7 @@ namespace xt {
 #define XT_THREADS 256
 #endif
 #ifndef XT_BLOCK_WORK_LOG2
-#define XT_BLOCK_WORK_LOG2 17
+#define XT_BLOCK_WORK_LOG2 16
 #endif
 #ifndef XT_WARP_WORK
 #define XT_WARP_WORK 4096
@@ -45,10 +45,12 @@ namespace xt {
 constexpr int kThreads = XT_THREADS;
 constexpr int kWarps = kThreads / 32;
 #ifndef XT_MIN_BLOCKS
-#define XT_MIN_BLOCKS 3
+#define XT_MIN_BLOCKS 4
 #endif
-// CTAs per SM the register budget is sized for: 3 x 256 threads leave ~80
-// registers a thread, and fewer tasks in flight keep more of their suffixes in L2
+// CTAs per SM the register budget is sized for: 4 x 256 threads leave 64
+// registers a thread (no spills). Swept with the task size at R-MAT s24:
+// 3 CTAs/SM with 2^17-candidate tasks 34.2 ms, 4 with 2^17 33.8 ms, 4 with
+// 2^16 32.1 ms, 4 with 2^15 35.1 ms, 5 (spilling) 53.9 ms
 constexpr int kMinBlocks = XT_MIN_BLOCKS;
 constexpr int kBlockWords = 8192;  // CTA region: 8192-slot hash or 2^18-bit bitmap
 // warp tasks run after the CTA tasks and split the CTA region among the warps
