@@ -341,3 +341,23 @@ def test_edge_support_every_tier(ctx, torch_cuda):
                 assert (sup == ref).all(), (orient, lane_work, warp_work)
         finally:
             g.free()
+
+
+@pytest.mark.parametrize("orient", ORIENTS)
+def test_graph_statistics(ctx, orient):
+    # the plan's statistics against the same sums taken on the host from
+    # the oriented CSR the library exposes
+    name = "chunglu14"
+    f = GOLDEN[name]
+    g = ctx.graph_from_edges(f["nv"], FIX[name + "_src"], FIX[name + "_dst"], orient)
+    try:
+        inf = g.info()
+        off, col = g.csr()
+        dout = np.diff(off)
+        din = np.bincount(col, minlength=len(dout))
+        assert inf["max_out_degree"] == dout.max() and inf["max_in_degree"] == din.max()
+        assert inf["max_degree"] == (dout + din).max()
+        assert inf["wedge_work"] == int(dout[col].sum())
+        assert inf["stream_work"] == int((dout * (dout - 1) // 2).sum())
+    finally:
+        g.free()

@@ -124,12 +124,31 @@ __global__ void k_inrec_work(const InRec *__restrict__ rec, int64_t ne, int64_t 
   XT_GRID_STRIDE(e, ne) w[e] = rec[e].len;
 }
 
-// tail-grouped work (statistics): d+(col[e]) per out-edge
-__global__ void k_outedge_work(const int32_t *__restrict__ col, int64_t ne, const int64_t *__restrict__ off,
-                               int64_t *__restrict__ w) {
-  XT_GRID_STRIDE(e, ne) {
-    const int32_t v = col[e];
-    w[e] = off[v + 1] - off[v];
+// Graph statistics in one pass over the vertices: st[0] the largest degree
+// (out + in), st[1] the largest out-degree, st[2] the largest in-degree,
+// st[3] the tail-grouped work sum over edges u->v of d+(v) = sum over v of
+// d-(v) d+(v)
+__global__ void k_vertex_stats(const int64_t *__restrict__ off, const int64_t *__restrict__ ioff, int64_t nv,
+                               unsigned long long *__restrict__ st) {
+  unsigned long long md = 0, mo = 0, mi = 0, wsum = 0;
+  XT_GRID_STRIDE(i, nv) {
+    const unsigned long long dout = off[i + 1] - off[i], din = ioff[i + 1] - ioff[i];
+    md = max(md, dout + din);
+    mo = max(mo, dout);
+    mi = max(mi, din);
+    wsum += dout * din;
+  }
+  for (int o = 16; o; o >>= 1) {
+    md = max(md, __shfl_xor_sync(0xffffffffu, md, o));
+    mo = max(mo, __shfl_xor_sync(0xffffffffu, mo, o));
+    mi = max(mi, __shfl_xor_sync(0xffffffffu, mi, o));
+    wsum += __shfl_xor_sync(0xffffffffu, wsum, o);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    atomicMax(&st[0], md);
+    atomicMax(&st[1], mo);
+    atomicMax(&st[2], mi);
+    atomicAdd(&st[3], wsum);
   }
 }
 
@@ -849,22 +868,6 @@ __global__ void k_unpermute(const int64_t *__restrict__ in, const int32_t *__res
   XT_GRID_STRIDE(r, nv) out[n2o[r]] = in[r];
 }
 
-// largest undirected degree: out-degree + in-degree of the oriented graph
-__global__ void k_max_degree(const int64_t *__restrict__ off, const int64_t *__restrict__ ioff, int64_t nv,
-                             unsigned long long *out) {
-  unsigned long long m = 0;
-  XT_GRID_STRIDE(i, nv) m = max(m, (unsigned long long)(off[i + 1] - off[i] + ioff[i + 1] - ioff[i]));
-  for (int o = 16; o; o >>= 1) m = max(m, __shfl_xor_sync(0xffffffffu, m, o));
-  if ((threadIdx.x & 31) == 0) atomicMax(out, m);
-}
-
-__global__ void k_max_rowlen(const int64_t *__restrict__ off, int64_t nv, unsigned long long *out) {
-  unsigned long long m = 0;
-  XT_GRID_STRIDE(i, nv) m = max(m, (unsigned long long)(off[i + 1] - off[i]));
-  for (int o = 16; o; o >>= 1) m = max(m, __shfl_xor_sync(0xffffffffu, m, o));
-  if ((threadIdx.x & 31) == 0) atomicMax(out, m);
-}
-
 // ---- host side --------------------------------------------------------------
 
 static xt_status exclusive_scan(Ctx *c, const int64_t *in, int64_t *out, int64_t n) {
@@ -912,15 +915,7 @@ xt_status make_plan(Graph *g) {
     if ((s = cuda_status(c, cudaMemsetAsync(stats, 0, 4 * sizeof(unsigned long long), c->stream), "memset")) !=
         XT_OK)
       break;
-    k_max_degree<<<counted(c, grid_for(nv, B, c->sm_count)), B, 0, c->stream>>>(g->d_off, g->d_ioff, nv, stats + 0);
-    k_max_rowlen<<<counted(c, grid_for(nv, B, c->sm_count)), B, 0, c->stream>>>(g->d_off, nv, stats + 1);
-    k_max_rowlen<<<counted(c, grid_for(nv, B, c->sm_count)), B, 0, c->stream>>>(g->d_ioff, nv, stats + 2);
-    // tail-grouped work, for the statistics only
-    k_outedge_work<<<counted(c, grid_for(ne, B, c->sm_count)), B, 0, c->stream>>>(g->d_col, ne, g->d_off, w);
-    if ((s = cuda_status(c, cudaMemsetAsync(w + ne, 0, sizeof(int64_t), c->stream), "memset")) != XT_OK) break;
-    if ((s = exclusive_scan(c, w, P, ne + 1)) != XT_OK) break;
-    int64_t tail_work = 0;
-    if ((s = d2h(c, &tail_work, P + ne, sizeof(int64_t))) != XT_OK) break;
+    k_vertex_stats<<<counted(c, grid_for(nv, B, c->sm_count)), B, 0, c->stream>>>(g->d_off, g->d_ioff, nv, stats);
     // suffix lengths, prefix-summed in head order
     k_inrec_work<<<counted(c, grid_for(ne, B, c->sm_count)), B, 0, c->stream>>>(g->d_irec, ne, w);
     if ((s = exclusive_scan(c, w, P, ne + 1)) != XT_OK) break;
@@ -989,7 +984,7 @@ xt_status make_plan(Graph *g) {
     g->max_degree = int64_t(hs[0]);
     g->max_out_degree = int64_t(hs[1]);
     g->max_in_degree = int64_t(hs[2]);
-    g->wedge_work = tail_work;
+    g->wedge_work = int64_t(hs[3]);
     g->stream_work = h[2];
     if (g->max_out_degree >= kMaxOutDegree) {
       s = set_error(c, XT_ERR_OVERFLOW, "an oriented out-degree of 2^30 or more is not supported");
