@@ -50,7 +50,8 @@ def test_no_device_is_reported_not_faked():
 def test_serve_estimate_is_linear_and_covers_the_build():
     # admission figure: grows with both sizes, adds up over a batch, and is
     # at least the bytes the builder's largest phase holds (8 B/row copied in,
-    # 8 B/row global ids, 16 B/row keys, 40 B per unique edge in the in-record sort)
+    # 8 B/row union ids, 16 B/row keys, 40 B per unique edge while the
+    # in-records are gathered)
     e = xt.serve_estimate
     assert e(-1, 0) < 0 and e(1, -1) < 0
     base = e(0, 0)

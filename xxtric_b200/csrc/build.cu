@@ -188,37 +188,33 @@ __device__ __forceinline__ uint32_t len_class_desc(int64_t len) {
 }
 
 // (head << lb | length class) sort key and position value for every
-// out-CSR position: lb (0..7) bits of the class fit beside the head in 31 bits
+// out-CSR position, and the position's in-record written in position order
+// (rows ascend with positions, so these reads are near sequential): lb
+// (0..7) bits of the class fit beside the head in 31 bits
 template <class V>
 __global__ void k_in_keys(const int32_t *__restrict__ col, const int32_t *__restrict__ rowof,
-                          const int64_t *__restrict__ off, int64_t m, int lb, uint32_t *__restrict__ ik,
-                          V *__restrict__ iv) {
+                          const int64_t *__restrict__ off, const int64_t *__restrict__ poff, int64_t m, int lb,
+                          uint32_t *__restrict__ ik, V *__restrict__ iv, InRec *__restrict__ recp) {
   XT_GRID_STRIDE(p, m) {
+    const int32_t u = rowof[p];
+    const int64_t a = off[u], len = off[u + 1] - p - 1;
     uint32_t k = uint32_t(col[p]) << lb;
-    if (lb > 0) {
-      const int64_t len = off[rowof[p] + 1] - p - 1;
-      k |= len_class_desc(len) >> (7 - lb);
-    }
+    if (lb > 0) k |= len_class_desc(len) >> (7 - lb);
     ik[p] = k;
     iv[p] = V(p);
+    InRec r;
+    r.s = poff[u] + (p - a) + 1;  // the suffix, in the padded column array
+    r.len = int32_t(len);
+    r.u = u;
+    recp[p] = r;
   }
 }
 
-// positions sorted by (head, class) -> in-records (suffix of N+(u) after the
-// head, as a position in the padded column array)
+// positions sorted by (head, class) -> in-records grouped by head
 template <class V>
-__global__ void k_in_records(const V *__restrict__ pos, int64_t m, const int32_t *__restrict__ rowof,
-                             const int64_t *__restrict__ off, const int64_t *__restrict__ poff,
+__global__ void k_in_records(const V *__restrict__ pos, int64_t m, const InRec *__restrict__ recp,
                              InRec *__restrict__ rec) {
-  XT_GRID_STRIDE(i, m) {
-    const int64_t p = int64_t(pos[i]);
-    const int32_t u = rowof[p];
-    InRec r;
-    r.s = poff[u] + (p - off[u]) + 1;
-    r.len = int32_t(off[u + 1] - p - 1);
-    r.u = u;
-    rec[i] = r;
-  }
+  XT_GRID_STRIDE(i, m) rec[i] = recp[int64_t(pos[i])];
 }
 
 // ---------------------------------------------------------------------------
@@ -355,6 +351,7 @@ static xt_status build_in_records(Ctx *c, uint64_t *keys, uint64_t *spare, int64
   uint32_t *kin = reinterpret_cast<uint32_t *>(spare), *kout = reinterpret_cast<uint32_t *>(keys);
   V *vin = nullptr, *vout = nullptr, *own_in = nullptr, *own_out = nullptr;
   int32_t *rowof = nullptr;
+  InRec *recp = nullptr;  // in-records in out-position order
   xt_status s = XT_OK;
   if (sizeof(V) == 4) {
     vin = reinterpret_cast<V *>(kin + m);
@@ -366,21 +363,25 @@ static xt_status build_in_records(Ctx *c, uint64_t *keys, uint64_t *spare, int64
     vout = own_out;
   }
   if (s == XT_OK) s = dalloc_n(c, &rowof, size_t(m));
+  if (s == XT_OK) s = dalloc_n(c, &recp, size_t(m));
   if (s == XT_OK) {
     k_csr_rows<<<counted(c, grid_for(nv * 32, B, c->sm_count)), B, 0, c->stream>>>(g->d_off, nv, m, rowof, nullptr);
-    k_in_keys<V><<<counted(c, grid_for(m, B, c->sm_count)), B, 0, c->stream>>>(g->d_col, rowof, g->d_off, m, lb,
-                                                                               kin, vin);
+    k_in_keys<V><<<counted(c, grid_for(m, B, c->sm_count)), B, 0, c->stream>>>(g->d_col, rowof, g->d_off, g->d_poff,
+                                                                               m, lb, kin, vin, recp);
     s = cuda_status(c, cudaGetLastError(), "in-keys");
   }
+  dfree(c, rowof);
+  rowof = nullptr;
   // stable: records of one (head, class) stay in position order
   if (s == XT_OK) s = sort_pairs32<V>(c, kin, kout, vin, vout, m, b + lb);
   if (s == XT_OK) s = keys_to_csr<uint32_t>(c, kout, m, nv, lb, g->d_ioff, nullptr);
+  // the records' own array comes after the sort, when its scratch is free
+  if (s == XT_OK) s = dalloc_n(c, &g->d_irec, size_t(m));
   if (s == XT_OK) {
-    k_in_records<V><<<counted(c, grid_for(m, B, c->sm_count)), B, 0, c->stream>>>(vout, m, rowof, g->d_off,
-                                                                                   g->d_poff, g->d_irec);
+    k_in_records<V><<<counted(c, grid_for(m, B, c->sm_count)), B, 0, c->stream>>>(vout, m, recp, g->d_irec);
     s = cuda_status(c, cudaGetLastError(), "in-records");
   }
-  dfree(c, rowof);
+  dfree(c, recp);
   dfree(c, own_in);
   dfree(c, own_out);
   return s;
@@ -419,8 +420,8 @@ static xt_status finish_csr(Ctx *c, uint64_t *keys, uint64_t *spare, int64_t m, 
     XT_CUDA(c, cudaGetLastError());
   }
   XT_TRY(dalloc_n(c, &g->d_ioff, size_t(nv + 1)));
-  XT_TRY(dalloc_n(c, &g->d_irec, size_t(m > 0 ? m : 1)));
   if (m == 0) {
+    XT_TRY(dalloc_n(c, &g->d_irec, 1));
     XT_CUDA(c, cudaMemsetAsync(g->d_ioff, 0, sizeof(int64_t) * (nv + 1), c->stream));
     return XT_OK;
   }
