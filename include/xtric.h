@@ -276,7 +276,8 @@ typedef struct {
 int64_t xt_serve_batches(xt_server *srv, xt_serve_batch *out, int64_t max);
 /* Stops admitting, fails the queued queries with XT_ERR_CLOSED, lets the
  * batches in flight finish, joins the workers and frees everything; results
- * not yet taken are lost. */
+ * not yet taken are lost. No other call on this server may run during or
+ * after it (a thread still waiting in xt_serve_wait must return first). */
 xt_status xt_serve_close(xt_server *srv);
 
 /* ---- synthetic inputs on the device --------------------------------------
