@@ -647,7 +647,9 @@ __device__ __forceinline__ void credit_member_edge(const int32_t *__restrict__ c
 
 // MODE 0: global count; 1: and per-vertex counts; 2: and per-edge counts
 template <int MODE>
-__global__ void __launch_bounds__(kThreads, kMinBlocks) k_count(const CountArgs a) {
+// (the per-vertex and per-edge modes hold 72 KB of shared memory, so two of
+// their CTAs fit an SM: their register budget is sized for two)
+__global__ void __launch_bounds__(kThreads, MODE == 0 ? kMinBlocks : 2) k_count(const CountArgs a) {
   const int64_t *__restrict__ off = a.off;
   const int32_t *__restrict__ col = a.col;
   const int64_t *__restrict__ ioff = a.ioff;
