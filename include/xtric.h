@@ -171,6 +171,11 @@ xt_status xt_graph_from_batch(xt_ctx *ctx, int64_t n_graphs, const int64_t *vert
 xt_status xt_graph_from_device_batch(xt_ctx *ctx, int64_t n_graphs, const int64_t *vertex_offsets,
                                      const int64_t *edge_offsets, const int32_t *d_src, const int32_t *d_dst,
                                      int orient, xt_graph **out);
+/* One call: builds the batch (host buffers, as xt_graph_from_batch), counts
+ * it once and frees it; *total and per_graph (n_graphs entries, nullable)
+ * receive the counts. */
+xt_status xt_batch_count(xt_ctx *ctx, int64_t n_graphs, const int64_t *vertex_offsets, const int64_t *edge_offsets,
+                         const int32_t *src, const int32_t *dst, int orient, int64_t *total, int64_t *per_graph);
 /* graphs in a batch (0 for a single graph) */
 int64_t xt_graph_groups(const xt_graph *g);
 /* total and per-graph counts (host buffer of xt_graph_groups entries, nullable) */

@@ -60,10 +60,12 @@ def test_small_batch_generators_and_counts_vs_oracle(ctx):
             t2, per2 = bg.count_groups()
             assert t2 == total and (per2 == per).all()
         bg.free()
-    # host-buffer entry point
+    # host-buffer entry points: the graph object and the one-call count
     bg = ctx.graph_from_batch(voff, eoff, s, d)
     assert bg.count_groups()[1].tolist() == expect
     bg.free()
+    total1, per1 = ctx.batch_count(voff, eoff, s, d)
+    assert per1.tolist() == expect and total1 == sum(expect)
     # capture while the context runs on the legacy default stream (handle 0),
     # which cannot itself be captured; replays still count on it
     c0 = xt.Context(0)

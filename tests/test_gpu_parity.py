@@ -361,3 +361,13 @@ def test_graph_statistics(ctx, orient):
         assert inf["stream_work"] == int((dout * (dout - 1) // 2).sum())
     finally:
         g.free()
+
+
+def test_cpp_mirror_batch_edges_and_server(tmp_path):
+    # the C++ host mirror's batch count, per-edge count and server on the GPU
+    import subprocess
+    from test_host import compile_mirror_check
+    exe = compile_mirror_check(tmp_path)
+    r = subprocess.run([exe], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert r.stdout.split("\n")[:3] == ["batch 5 4 1", "edges 4 6 12", "served 4 1"], r.stdout

@@ -199,3 +199,24 @@ def test_tsv_comments_weights_and_errors(tmp_path):
     with pytest.raises(xt.XtError) as e:
         xt.read_tsv(str(tmp_path / "missing.tsv"))
     assert e.value.status == xt.XT_ERR_IO
+
+
+def compile_mirror_check(tmp_path):
+    exe = str(tmp_path / "mirror_check")
+    lib_dir = os.path.join(ROOT, "xxtric_b200")
+    r = subprocess.run(["g++", "-O1", "-std=c++17", "-I", ROOT, "-I", os.path.join(ROOT, "include"),
+                        os.path.join(ROOT, "tests", "cpp", "mirror_check.cpp"), "-o", exe, "-L", lib_dir,
+                        "-lxtb200", "-Wl,-rpath," + lib_dir], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    return exe
+
+
+def test_cpp_mirror_compiles_and_reports_no_device(tmp_path):
+    # the C++ mirror of the batch, per-edge and serving entry points builds
+    # against the library; without a GPU it reports the library's status
+    import torch
+    exe = compile_mirror_check(tmp_path)
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present (the GPU test runs the program)")
+    r = subprocess.run([exe], capture_output=True, text=True, timeout=120)
+    assert r.returncode == 3 and r.stdout.startswith("error 9"), r.stdout

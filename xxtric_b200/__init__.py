@@ -87,6 +87,7 @@ _proto("xt_graph_from_batch", _int, _vp, _i64, _vp, _vp, _vp, _vp, _int, _P(_vp)
 _proto("xt_graph_from_device_batch", _int, _vp, _i64, _vp, _vp, _vp, _vp, _int, _P(_vp))
 _proto("xt_graph_groups", _i64, _vp)
 _proto("xt_count_groups", _int, _vp, _vp, _vp)
+_proto("xt_batch_count", _int, _vp, _i64, _vp, _vp, _vp, _vp, _int, _P(_i64), _vp)
 _proto("xt_count_groups_async", _int, _vp, _vp, _vp)
 _proto("xt_graph_capture", _int, _vp)
 _proto("xt_graph_set_tuning", _int, _vp, _i64, _i64, _i64)
@@ -119,7 +120,7 @@ EXPORTED = ["xt_strerror", "xt_last_error", "xt_open", "xt_close", "xt_set_strea
             "xt_graph_from_csr", "xt_graph_from_edges", "xt_graph_from_device_edges", "xt_graph_get_info",
             "xt_graph_get_csr", "xt_graph_free", "xt_count", "xt_count_async", "xt_count_edges", "xt_count_device",
             "xt_count_device_static", "xt_graph_from_batch", "xt_graph_from_device_batch", "xt_graph_groups",
-            "xt_count_groups", "xt_count_groups_async", "xt_graph_capture", "xt_graph_set_tuning", "xt_graph_set_tiers",
+            "xt_count_groups", "xt_count_groups_async", "xt_batch_count", "xt_graph_capture", "xt_graph_set_tuning", "xt_graph_set_tiers",
             "xt_mem_stats", "xt_serve_estimate", "xt_serve_open", "xt_serve_submit", "xt_serve_poll",
             "xt_serve_wait", "xt_serve_get_stats", "xt_serve_close", "xt_serve_batches", "xt_tsv_read", "xt_tsv_write",
             "xt_graph_autotune", "xt_batch_spec", "xt_gen_batch", "xt_device_free",
@@ -342,6 +343,18 @@ class Context:
                                ctypes.byref(ps), ctypes.byref(pd)), "xt_gen_batch", self)
         ne = int(eoff[-1])
         return eoff, DeviceArray(self, ps.value or 0, ne, "<i4", 4), DeviceArray(self, pd.value or 0, ne, "<i4", 4)
+
+    def batch_count(self, vertex_offsets, edge_offsets, src, dst, orient: int = ORIENT_DEGREE):
+        """Build, count and free a batch in one call (xt_batch_count): (total, per-graph counts)."""
+        voff = np.ascontiguousarray(vertex_offsets, np.int64)
+        eoff = np.ascontiguousarray(edge_offsets, np.int64)
+        s_ = np.ascontiguousarray(src, np.int32)
+        d_ = np.ascontiguousarray(dst, np.int32)
+        per = np.zeros(len(voff) - 1, np.int64)
+        t = _i64(0)
+        _check(_L.xt_batch_count(self._h, len(voff) - 1, _ptr(voff), _ptr(eoff), _ptr(s_), _ptr(d_), orient,
+                                 ctypes.byref(t), _ptr(per)), "xt_batch_count", self)
+        return t.value, per
 
     def graph_from_batch(self, vertex_offsets, edge_offsets, src, dst, orient: int = ORIENT_DEGREE,
                          device: bool = False) -> "DeviceGraph":

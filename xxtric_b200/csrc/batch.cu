@@ -685,6 +685,16 @@ xt_status xt_count_groups(xt_graph *gr, int64_t *total, int64_t *per_group) {
 
 int64_t xt_graph_groups(const xt_graph *gr) { return gr ? gr->g.n_groups : -1; }
 
+xt_status xt_batch_count(xt_ctx *ctx, int64_t n_graphs, const int64_t *vertex_offsets, const int64_t *edge_offsets,
+                         const int32_t *src, const int32_t *dst, int orient, int64_t *total, int64_t *per_graph) {
+  if (!ctx || !total) return XT_ERR_INVALID;
+  xt_graph *g = nullptr;
+  XT_TRY(xt_graph_from_batch(ctx, n_graphs, vertex_offsets, edge_offsets, src, dst, orient, &g));
+  const xt_status s = xt_count_groups(g, total, per_graph);
+  xt_graph_free(g);
+  return s;
+}
+
 xt_status xt_graph_capture(xt_graph *gr) {
   if (!gr) return XT_ERR_INVALID;
   cudaSetDevice(gr->g.ctx->device);

@@ -158,6 +158,14 @@ class TriangleCountingSingle {
     check(xt_count(dg_, &t, per_vertex.data()), "counting", ctx_);
     return t;
   }
+  // triangles on every oriented edge (k-truss support), in the order of the
+  // library's oriented CSR (internal numbering, see xt_graph_get_csr/_perm)
+  GraphElem count_edges(std::vector<GraphElem> &support) {
+    support.assign(size_t(info().n_edges), 0);
+    int64_t t = 0;
+    check(xt_count_edges(dg_, &t, support.data()), "counting", ctx_);
+    return t;
+  }
   xt_graph_info info() const {
     xt_graph_info i{};
     xt_graph_get_info(dg_, &i);
@@ -174,6 +182,67 @@ class TriangleCountingSingle {
   Graph *g_;
   xt_ctx *ctx_ = nullptr;
   xt_graph *dg_ = nullptr;
+};
+
+// Many graphs counted in one launch: graph g has vertices
+// [vertex_offsets[g], vertex_offsets[g+1]) and rows [edge_offsets[g],
+// edge_offsets[g+1]) of src/dst (graph-local ids). Returns the total and
+// fills per_graph.
+inline GraphElem BatchCount(const std::vector<int64_t> &vertex_offsets, const std::vector<int64_t> &edge_offsets,
+                            const std::vector<int32_t> &src, const std::vector<int32_t> &dst,
+                            std::vector<GraphElem> &per_graph, int orient = XT_ORIENT_DEGREE, int device = 0) {
+  xt_ctx *ctx = nullptr;
+  check(xt_open(device, &ctx), "opening the CUDA device");
+  const int64_t ng = int64_t(vertex_offsets.size()) - 1;
+  per_graph.assign(size_t(ng > 0 ? ng : 0), 0);
+  int64_t t = 0;
+  const xt_status s = xt_batch_count(ctx, ng, vertex_offsets.data(), edge_offsets.data(), src.data(), dst.data(),
+                                     orient, &t, per_graph.data());
+  const std::string detail = xt_last_error(ctx);
+  xt_close(ctx);
+  if (s != XT_OK) throw Error(s, std::string("batch count: ") + xt_strerror(s) + " (" + detail + ")");
+  return t;
+}
+
+// Count queries served by device-memory-budget admission and continuous
+// batching (xt_serve_*): submit() returns a ticket, wait() its count. The
+// query's edge rows are read while it runs: keep them alive until wait().
+class Server {
+ public:
+  explicit Server(int device = 0, int64_t budget_bytes = 0, int slots = 0, int orient = XT_ORIENT_DEGREE) {
+    xt_serve_config c{};
+    c.budget_bytes = budget_bytes;
+    c.slots = slots;
+    c.orient = orient;
+    check(xt_serve_open(device, &c, &srv_), "opening the server");
+  }
+  ~Server() {
+    if (srv_) xt_serve_close(srv_);
+  }
+  Server(const Server &) = delete;
+  Server &operator=(const Server &) = delete;
+  int64_t submit(int64_t nv, const std::vector<int32_t> &src, const std::vector<int32_t> &dst) {
+    if (src.size() != dst.size()) throw Error(XT_ERR_INVALID, "src and dst differ in length");
+    int64_t ticket = 0;
+    check(xt_serve_submit(srv_, nv, int64_t(src.size()), src.data(), dst.data(), &ticket), "submitting");
+    return ticket;
+  }
+  // the count of the query (blocks); latency_s receives submit-to-result seconds
+  GraphElem wait(int64_t ticket, double *latency_s = nullptr) {
+    int64_t c = 0;
+    double lat = 0;
+    check(xt_serve_wait(srv_, ticket, -1, &c, &lat), "query");
+    if (latency_s) *latency_s = lat;
+    return c;
+  }
+  xt_serve_stats stats() {
+    xt_serve_stats s{};
+    check(xt_serve_get_stats(srv_, &s), "server statistics");
+    return s;
+  }
+
+ private:
+  xt_server *srv_ = nullptr;
 };
 
 }  // namespace xtb200
