@@ -142,8 +142,9 @@ xt_status xt_count_device(int64_t nv, const int64_t *d_indices, const int64_t *d
                           int accumulate, void *cuda_stream);
 
 /* No counterpart in the reference. The count of the same device CSR as
- * xt_count_device (int64 offsets, int64 tails; rows sorted, deduped,
- * symmetric), for callers that cannot allocate device memory while they run:
+ * xt_count_device (int64 offsets, int64 tails; rows sorted ascending without
+ * repeats or self loops, symmetric: this entry cannot sort, so it checks and
+ * rejects other rows), for callers that cannot allocate device memory while they run:
  * it calls no cudaMalloc, cudaFree or other allocating routine. Its scratch is
  * one fixed 64 MiB array inside the library, present on every GPU that loads
  * the library until the process exits; it holds 8 bytes per vertex, so
@@ -151,8 +152,9 @@ xt_status xt_count_device(int64_t nv, const int64_t *d_indices, const int64_t *d
  * device sets up the array's address (make it before any stream capture).
  * Calls that overlap on one device race on the shared array: serialise them.
  * Orientation is by vertex id. Overwrites *d_count, or adds to it when
- * accumulate != 0; XT_ERR_INVALID when a row lacks a back edge (input not
- * symmetric). Synchronises the given stream before returning. */
+ * accumulate != 0; XT_ERR_INVALID when a row is out of order, repeats an
+ * id, holds its own id or an id outside [0, nv), or lacks a back edge (input
+ * not symmetric). Synchronises the given stream before returning. */
 xt_status xt_count_device_static(int64_t nv, const int64_t *d_indices, const int64_t *d_edge_list,
                                  int64_t *d_count, int accumulate, void *cuda_stream);
 

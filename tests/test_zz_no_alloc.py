@@ -70,6 +70,19 @@ def test_static_scratch_size_limit_and_bad_input():
     with pytest.raises(xt.XtError) as e:
         xt.count_device_static(3, off2, tails2, out, stream=torch.cuda.current_stream().cuda_stream)
     assert e.value.status == xt.XT_ERR_INVALID
+    # rows this entry cannot repair (it has no room to sort): out of order, a
+    # repeated id, the row's own id, an id past nv. Its input check rejects
+    # them before any pass indexes memory with them.
+    bad = [([0, 2, 4, 6], [2, 1, 0, 2, 0, 1]),   # row 0 out of order
+           ([0, 3, 5, 7], [1, 1, 2, 0, 2, 0, 1]),  # row 0 repeats 1
+           ([0, 3, 5, 7], [0, 1, 2, 0, 2, 0, 1]),  # row 0 holds 0
+           ([0, 2, 4, 6], [1, 5, 0, 2, 0, 1])]     # id 5 with nv = 3
+    for o, t in bad:
+        with pytest.raises(xt.XtError) as e:
+            xt.count_device_static(3, torch.tensor(o, dtype=torch.int64, device="cuda"),
+                                   torch.tensor(t, dtype=torch.int64, device="cuda"), out,
+                                   stream=torch.cuda.current_stream().cuda_stream)
+        assert e.value.status == xt.XT_ERR_INVALID, (o, t)
     # a valid graph afterwards still counts
     xt.count_device_static(3, off, tails, out, stream=torch.cuda.current_stream().cuda_stream)
     torch.cuda.synchronize()

@@ -77,9 +77,29 @@ __global__ void k_na_init(Header *hdr) {
   hdr->err = 0;
 }
 
+// Input check, a warp per row: offsets that do not decrease, ids in [0, nv),
+// rows strictly ascending (no repeats) and without the row's own id. A
+// violation sets hdr->err (bit 2) and the passes below do nothing, so an
+// unsorted row or an id past nv cannot steer shared- or global-memory indices.
+__global__ void k_na_check(int64_t nv, const int64_t *__restrict__ off, const int64_t *__restrict__ tails,
+                           Header *hdr) {
+  const int lane = threadIdx.x & 31;
+  const int64_t nwarps = (int64_t(gridDim.x) * blockDim.x) >> 5;
+  for (int64_t v = (blockIdx.x * int64_t(blockDim.x) + threadIdx.x) >> 5; v < nv; v += nwarps) {
+    const int64_t e0 = off[v], e1 = off[v + 1];
+    bool bad = e1 < e0;
+    for (int64_t p = e0 + lane; !bad && p < e1; p += 32) {
+      const int64_t t = tails[p];
+      bad = t < 0 || t >= nv || t == v || (p > e0 && tails[p - 1] >= t);
+    }
+    if (__any_sync(0xffffffffu, bad) && lane == 0) atomicOr(&hdr->err, 2);
+  }
+}
+
 // split point of every row, and the heads whose out-list is too long for a warp
 __global__ void k_na_split(int64_t nv, const int64_t *__restrict__ off, const int64_t *__restrict__ tails,
                            Scratch sc) {
+  if (sc.hdr->err) return;  // the input check failed
   for (int64_t v = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; v < nv; v += int64_t(gridDim.x) * blockDim.x) {
     int64_t lo = off[v], hi = off[v + 1];
     const int64_t e0 = lo, e1 = hi;
@@ -118,6 +138,7 @@ struct NaSet {
   __device__ __forceinline__ void insert(int32_t x) const {
     if (bitmap) {
       const uint32_t d = uint32_t(x - lo);
+      if (d > uint32_t(hi - lo)) return;  // only on a row out of order (rejected by k_na_check)
       atomicOr(reinterpret_cast<unsigned int *>(&words[d >> 5]), 1u << (d & 31));
       return;
     }
@@ -187,6 +208,7 @@ __global__ void __launch_bounds__(kThreads) k_na_warp(int64_t nv, const int64_t 
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   int32_t *words = words_all + warp * kWarpWords;
   int64_t hits = 0;
+  if (sc.hdr->err) return;  // the input check failed
   while (true) {
     unsigned long long b = 0;
     if (lane == 0) b = atomicAdd(&sc.hdr->cursor_w, (unsigned long long)kHeadBatch);
@@ -217,7 +239,7 @@ __global__ void __launch_bounds__(kThreads) k_na_cta(const int64_t *__restrict__
   __shared__ int32_t words[kBlockWords];
   __shared__ int64_t s_head;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int64_t n_heavy = int64_t(sc.hdr->n_heavy);
+  const int64_t n_heavy = sc.hdr->err ? 0 : int64_t(sc.hdr->n_heavy);  // nothing when the input check failed
   int64_t hits = 0;
   while (true) {
     if (tid == 0) s_head = int64_t(atomicAdd(&sc.hdr->cursor_c, 1ull));
@@ -287,6 +309,9 @@ extern "C" xt_status xt_count_device_static(int64_t nv, const int64_t *d_indices
   int sms = 148;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   k_na_init<<<1, 1, 0, st>>>(sc.hdr);
+  const int64_t gw = (nv * 32 + kThreads - 1) / kThreads;
+  k_na_check<<<unsigned(gw < int64_t(sms) * 32 ? gw : int64_t(sms) * 32), kThreads, 0, st>>>(nv, d_indices,
+                                                                                             d_edge_list, sc.hdr);
   const int64_t gs = (nv + kThreads - 1) / kThreads;
   k_na_split<<<unsigned(gs < int64_t(sms) * 32 ? gs : int64_t(sms) * 32), kThreads, 0, st>>>(nv, d_indices,
                                                                                              d_edge_list, sc);
