@@ -15,6 +15,8 @@
 // n > m range, taken from the head's side.
 #include <cub/cub.cuh>
 
+#include <algorithm>
+
 #include "xt_internal.cuh"
 
 namespace xt {
@@ -429,8 +431,47 @@ static xt_status finish_csr(Ctx *c, uint64_t *keys, uint64_t *spare, int64_t m, 
   return build_in_records<uint64_t>(c, keys, spare, m, nv, b, g);
 }
 
+// Copies the host rows into d_src/d_dst in chunks on the copy stream; the
+// context stream turns each chunk into keys (and degree counts) once it has
+// landed.
+static xt_status upload_and_key(Ctx *c, const HostRows &up, int64_t nv, int64_t ne, int32_t *d_src, int32_t *d_dst,
+                                int b, uint64_t *keys, int32_t *deg) {
+  constexpr int kChunks = 8;
+  const int B = 256;
+  if (!c->copy_stream) XT_CUDA(c, cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking));
+  cudaEvent_t ev[kChunks + 1] = {};
+  xt_status s = XT_OK;
+  for (int i = 0; i <= kChunks && s == XT_OK; i++)
+    s = cuda_status(c, cudaEventCreateWithFlags(&ev[i], cudaEventDisableTiming), "event");
+  // the copy stream starts after the buffers' stream-ordered allocation
+  if (s == XT_OK) s = cuda_status(c, cudaEventRecord(ev[kChunks], c->stream), "event");
+  if (s == XT_OK) s = cuda_status(c, cudaStreamWaitEvent(c->copy_stream, ev[kChunks], 0), "event");
+  const int64_t step = (ne + kChunks - 1) / kChunks;
+  for (int i = 0; i < kChunks && s == XT_OK; i++) {
+    const int64_t a = int64_t(i) * step, n = std::min(step, ne - a);
+    if (n <= 0) break;
+    s = cuda_status(c, cudaMemcpyAsync(d_src + a, up.src + a, sizeof(int32_t) * n, cudaMemcpyHostToDevice,
+                                       c->copy_stream), "H2D");
+    if (s == XT_OK)
+      s = cuda_status(c, cudaMemcpyAsync(d_dst + a, up.dst + a, sizeof(int32_t) * n, cudaMemcpyHostToDevice,
+                                         c->copy_stream), "H2D");
+    if (s == XT_OK) s = cuda_status(c, cudaEventRecord(ev[i], c->copy_stream), "event");
+    if (s == XT_OK) s = cuda_status(c, cudaStreamWaitEvent(c->stream, ev[i], 0), "event");
+    if (s == XT_OK) {
+      k_edge_keys<<<counted(c, grid_for(n, B, c->sm_count)), B, 0, c->stream>>>(d_src + a, d_dst + a, n, nv, b,
+                                                                               keys + a, deg, c->d_err);
+      s = cuda_status(c, cudaGetLastError(), "k_edge_keys");
+    }
+  }
+  if (s != XT_OK) cudaStreamSynchronize(c->copy_stream);  // no copy outlives a failed build
+  // the events have been waited on by the context stream; destroying them now is allowed
+  for (int i = 0; i <= kChunks; i++)
+    if (ev[i]) cudaEventDestroy(ev[i]);
+  return s;
+}
+
 xt_status build_from_edges(Ctx *c, int64_t nv, int64_t ne, const int32_t *d_src, const int32_t *d_dst, int orient,
-                           Graph *g) {
+                           Graph *g, const HostRows *upload) {
   if (nv < 1 || ne < 0) return set_error(c, XT_ERR_INVALID, "nv must be >= 1 and ne >= 0");
   if (nv > (int64_t(1) << 31) - 1) return set_error(c, XT_ERR_OVERFLOW, "nv must be below 2^31");
   if (orient != XT_ORIENT_ID && orient != XT_ORIENT_DEGREE) return set_error(c, XT_ERR_INVALID, "bad orientation");
@@ -454,9 +495,15 @@ xt_status build_from_edges(Ctx *c, int64_t nv, int64_t ne, const int32_t *d_src,
       if ((s = cuda_status(c, cudaMemsetAsync(deg, 0, sizeof(int32_t) * nv, c->stream), "memset")) != XT_OK) break;
     }
     if (ne > 0) {
-      k_edge_keys<<<counted(c, grid_for(ne, B, c->sm_count)), B, 0, c->stream>>>(d_src, d_dst, ne, nv, b, k0, deg,
-                                                                                 c->d_err);
-      if ((s = cuda_status(c, cudaGetLastError(), "k_edge_keys")) != XT_OK) break;
+      if (upload) {
+        s = upload_and_key(c, *upload, nv, ne, const_cast<int32_t *>(d_src), const_cast<int32_t *>(d_dst), b, k0,
+                           deg);
+        if (s != XT_OK) break;
+      } else {
+        k_edge_keys<<<counted(c, grid_for(ne, B, c->sm_count)), B, 0, c->stream>>>(d_src, d_dst, ne, nv, b, k0,
+                                                                                   deg, c->d_err);
+        if ((s = cuda_status(c, cudaGetLastError(), "k_edge_keys")) != XT_OK) break;
+      }
       if ((s = check_err(c, "edge list")) != XT_OK) break;
     }
     // rank, then relabel every row: one sort of the rows in internal ids

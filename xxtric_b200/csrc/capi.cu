@@ -131,6 +131,10 @@ xt_status xt_close(xt_ctx *ctx) {
   cudaSetDevice(c->device);
   cudaStreamSynchronize(c->stream);
   cudaFree(c->d_err);
+  if (c->copy_stream) {
+    cudaStreamSynchronize(c->copy_stream);
+    cudaStreamDestroy(c->copy_stream);
+  }
   if (c->own_stream) cudaStreamDestroy(c->stream);
   delete ctx;
   return XT_OK;
@@ -199,12 +203,17 @@ xt_status xt_graph_from_edges(xt_ctx *ctx, int64_t nv, int64_t ne, const int32_t
   int32_t *ds = nullptr, *dd = nullptr;
   XT_TRY(dalloc_n(c, &ds, size_t(ne > 0 ? ne : 1)));
   xt_status s = dalloc_n(c, &dd, size_t(ne > 0 ? ne : 1));
-  if (s == XT_OK && ne > 0) {
-    s = cuda_status(c, cudaMemcpyAsync(ds, src, sizeof(int32_t) * ne, cudaMemcpyHostToDevice, c->stream), "H2D");
-    if (s == XT_OK)
-      s = cuda_status(c, cudaMemcpyAsync(dd, dst, sizeof(int32_t) * ne, cudaMemcpyHostToDevice, c->stream), "H2D");
+  xt_graph *gr = nullptr;
+  if (s == XT_OK) {
+    gr = new (std::nothrow) xt_graph();
+    if (!gr) s = XT_ERR_OOM;
   }
-  if (s == XT_OK) s = xt_graph_from_device_edges(ctx, nv, ne, ds, dd, orient, out);
+  if (s == XT_OK) {
+    // the copy-in runs in chunks beside the first build step
+    const HostRows up{src, dst};
+    s = build_from_edges(c, nv, ne, ds, dd, orient, &gr->g, &up);
+    s = finish_build(ctx, gr, s, out);
+  }
   dfree(c, ds);
   dfree(c, dd);
   return s;

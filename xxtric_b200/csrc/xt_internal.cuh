@@ -23,6 +23,7 @@ struct Ctx {
   size_t smem_optin = 0;  // max dynamic shared memory per block (opt-in)
   cudaStream_t stream = nullptr;
   bool own_stream = false;
+  cudaStream_t copy_stream = nullptr;  // host-to-device copies that overlap the build (created on first use)
   std::string last_error;
   int64_t fail_alloc_countdown = 0;  // test hook: >0 counts down to a failing allocation
   // device-side error word reused by kernels that check their own inputs
@@ -124,10 +125,18 @@ struct Graph {
   Plan *plan = nullptr;
 };
 
+// Optional: the rows still in host memory. build_from_edges then copies
+// them into d_src/d_dst (device buffers of ne rows) in chunks on the
+// context's copy stream and turns each chunk into keys as soon as it lands,
+// so key generation overlaps the copy-in.
+struct HostRows {
+  const int32_t *src, *dst;
+};
+
 // Builds the oriented CSR from a device edge list (int32 ids) of ne rows.
 // Rows may repeat, be one-directional or self loops.
 xt_status build_from_edges(Ctx *c, int64_t nv, int64_t ne, const int32_t *d_src, const int32_t *d_dst,
-                           int orient, Graph *g);
+                           int orient, Graph *g, const HostRows *upload = nullptr);
 // Builds from a device CSR (int64 offsets and tails). canonical: rows already
 // sorted, deduped, symmetric and loop-free, so no sort is needed.
 xt_status build_from_csr(Ctx *c, int64_t nv, const int64_t *d_off, const int64_t *d_tails, bool canonical,
