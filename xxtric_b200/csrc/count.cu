@@ -58,7 +58,7 @@ constexpr int kWarpWords = kBlockWords / kWarps;  // 1024: a 1024-slot hash or a
 constexpr int kWarpDmax = kWarpWords / 4;         // hash load factor <= 1/4
 constexpr int64_t kWarpWork = XT_WARP_WORK;
 constexpr int kBlockDmax = 2048;
-// the warps' bitmap member counters share the CTA's
+// the warps' member counters share the CTA's
 static_assert(kWarps * kWarpDmax <= kBlockDmax, "warp member counters exceed the CTA's");
 constexpr int64_t kBlockWorkMin = int64_t(1) << 14;
 constexpr int64_t kBlockWorkMax = int64_t(1) << XT_BLOCK_WORK_LOG2;
@@ -278,11 +278,12 @@ __device__ __forceinline__ uint32_t hash_slot(int32_t x, int shift) {
   return (uint32_t(x) * 0x9E3779B1u) >> shift;
 }
 
-__device__ __forceinline__ void hash_insert(int32_t *tab, uint32_t mask, int shift, int32_t x) {
+// inserts x and returns its slot
+__device__ __forceinline__ uint32_t hash_insert(int32_t *tab, uint32_t mask, int shift, int32_t x) {
   uint32_t h = hash_slot(x, shift);
   while (true) {
     const int32_t old = atomicCAS(&tab[h], kEmpty, x);
-    if (old == kEmpty || old == x) return;
+    if (old == kEmpty || old == x) return h;
     h = (h + 1) & mask;
   }
 }
@@ -301,9 +302,9 @@ __device__ __forceinline__ int hash_find(const int32_t *tab, uint32_t mask, int 
 // The member set N+(v) (or one part of it) in shared memory.
 struct Members {
   int32_t *words;   // bitmap words or hash slots
-  int32_t *cnt;     // per-slot hit counters (per-vertex and per-edge modes, hash)
-  int32_t *pre;     // bitmap, same modes: index of the first member in each word
-  int32_t *mcnt;    // bitmap, same modes: per-member hit counters
+  uint16_t *idx;    // per-vertex and per-edge modes: per bitmap word, the index of its first
+                    // member; per hash slot, the index of the member it holds
+  int32_t *mcnt;    // same modes: per-member hit counters
   int32_t lo, hi;   // smallest and largest member
   uint32_t base;    // bitmap: x is bit (x & 31) of words[(x >> 5) - base]
   uint32_t nwords;  // bitmap: words in use; words[nwords] is a zero guard word
@@ -316,7 +317,8 @@ struct Members {
 // words (a bitmap only while the members' id range is at most bitmap_bits)
 // and returns how many words must be cleared. In the per-vertex and
 // per-edge modes a bitmap also keeps, per word, the index of its first
-// member, so a hit finds its member's counter by a popcount.
+// member, so a hit finds its member's counter by a popcount; a hash keeps
+// the index of the member in each used slot.
 template <bool PV>
 __device__ __forceinline__ int members_layout(Members &m, const int32_t *mem, int n, int words, int64_t bitmap_bits) {
   m.lo = mem[0];
@@ -339,21 +341,21 @@ __device__ __forceinline__ int members_layout(Members &m, const int32_t *mem, in
   return 1 << lg;
 }
 
-// inserts member i of mem[0, n) (ascending); with ranks (per-vertex and
-// per-edge modes) also records word starts and clears the member's counter
+// inserts member i of mem[0, n) (ascending); with counters (per-vertex and
+// per-edge modes) also records where the member's counter is found and
+// clears it
 template <bool PV>
 __device__ __forceinline__ void members_insert_at(const Members &m, const int32_t *mem, int i) {
   const int32_t x = mem[i];
   if (m.bitmap) {
     const uint32_t wd = uint32_t(x >> 5) - m.base;
     atomicOr(reinterpret_cast<unsigned int *>(&m.words[wd]), 1u << (x & 31));
-    if (PV) {
-      if (i == 0 || uint32_t(mem[i - 1] >> 5) - m.base != wd) m.pre[wd] = i;
-      m.mcnt[i] = 0;
-    }
+    if (PV && (i == 0 || uint32_t(mem[i - 1] >> 5) - m.base != wd)) m.idx[wd] = uint16_t(i);
   } else {
-    hash_insert(m.words, m.mask, m.shift, x);
+    const uint32_t slot = hash_insert(m.words, m.mask, m.shift, x);
+    if (PV) m.idx[slot] = uint16_t(i);
   }
+  if (PV) m.mcnt[i] = 0;
 }
 
 __device__ __forceinline__ void members_insert(const Members &m, int32_t x) {
@@ -380,10 +382,13 @@ constexpr int64_t kMaxOutDegree = int64_t(1) << 30;
 
 // One 256-bit load per lane (sm_100 vector width; the column array is
 // 256-byte aligned, so every pair is 32-byte aligned): one L1 wavefront per
-// line touched instead of one per 16-byte half.
+// line touched instead of one per 16-byte half. A record's lanes walk
+// consecutive pairs, so each load asks L2 for the 256 bytes around it (the
+// next steps' pairs) and skips L1, where a pair is never read twice (s22
+// 5.74 -> 5.62 ms, s24 32.02 -> 31.77 ms).
 __device__ __forceinline__ void load_pair(const int32_t *__restrict__ col, int64_t P, int4 &a, int4 &b) {
   const int32_t *p = col + 8 * P;
-  asm volatile("ld.global.nc.v8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+  asm volatile("ld.global.nc.L1::no_allocate.L2::256B.v8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
                : "=r"(a.x), "=r"(a.y), "=r"(a.z), "=r"(a.w), "=r"(b.x), "=r"(b.y), "=r"(b.z), "=r"(b.w)
                : "l"(p));
 }
@@ -408,7 +413,7 @@ __device__ __forceinline__ int hash_test(const Members &m, int32_t w) {
   if (uint32_t(w - m.lo) > uint32_t(m.hi - m.lo)) return 0;  // sentinels too
   const int slot = hash_find(m.words, m.mask, m.shift, w);
   if (slot < 0) return 0;
-  if (PV) atomicAdd(&m.cnt[slot], 1);
+  if (PV) atomicAdd(&m.mcnt[m.idx[slot]], 1);
   return 1;
 }
 
@@ -424,7 +429,8 @@ __device__ __forceinline__ int probe_pair(const int4 a, const int4 b, const Memb
 
 // Per-vertex and per-edge modes: a hit bumps its member's counter (bitmap:
 // the member's index is the word's first index plus the set bits below;
-// hash: its slot) and, per edge, the edge u->w at column position pos
+// hash: the index kept beside its slot) and, per edge, the edge u->w at
+// column position pos
 template <int MODE, bool BITMAP>
 __device__ __forceinline__ int probe_one(const Members &m, int32_t w, unsigned int *__restrict__ es, int64_t pos) {
   if (BITMAP) {
@@ -433,7 +439,7 @@ __device__ __forceinline__ int probe_one(const Members &m, int32_t w, unsigned i
     const uint32_t x = uint32_t(m.words[i]);
     const uint32_t bit = uint32_t(w) & 31u;
     if (!((x >> bit) & 1u)) return 0;  // the guard word is zero: i < nwords below
-    atomicAdd(&m.mcnt[m.pre[i] + __popc(x & ((1u << bit) - 1u))], 1);
+    atomicAdd(&m.mcnt[m.idx[i] + __popc(x & ((1u << bit) - 1u))], 1);
   } else if (!hash_test<true>(m, w)) {
     return 0;
   }
@@ -626,42 +632,28 @@ __device__ __forceinline__ int stage_task(int32_t *stage, const int32_t *__restr
 // clears the first nclear words of the member set (thread t of nt)
 template <bool PV>
 __device__ __forceinline__ void clear_members(const Members &m, int nclear, int t, int nt) {
-  for (int i = t; i < nclear; i += nt) {
-    m.words[i] = m.bitmap ? 0 : kEmpty;
-    if (PV && !m.bitmap) m.cnt[i] = 0;
-  }
-}
-
-// Per-edge mode: adds a slot's hits to the edge v->w, w's position in the
-// task's member columns col[r0, r0 + n) found by binary search
-__device__ __forceinline__ void credit_member_edge(const int32_t *__restrict__ col, int64_t r0, int n, int32_t w,
-                                                   unsigned c, unsigned int *__restrict__ es) {
-  int lo = 0, hi = n;
-  while (lo < hi) {
-    const int mid = (lo + hi) >> 1;
-    if (col[r0 + mid] < w) lo = mid + 1;
-    else hi = mid;
-  }
-  atomicAdd(&es[r0 + lo], c);
+  for (int i = t; i < nclear; i += nt) m.words[i] = m.bitmap ? 0 : kEmpty;
 }
 
 // MODE 0: global count; 1: and per-vertex counts; 2: and per-edge counts
 template <int MODE>
-// (the per-vertex and per-edge modes hold 72 KB of shared memory, so two of
-// their CTAs fit an SM: their register budget is sized for two)
-__global__ void __launch_bounds__(kThreads, MODE == 0 ? kMinBlocks : 2) k_count(const CountArgs a) {
+// (the per-vertex and per-edge modes hold 56 KB of shared memory, so three
+// of their CTAs fit an SM: their register budget is sized for three)
+__global__ void __launch_bounds__(kThreads, MODE == 0 ? kMinBlocks : 3) k_count(const CountArgs a) {
   const int64_t *__restrict__ off = a.off;
   const int32_t *__restrict__ col = a.col;
   const int64_t *__restrict__ ioff = a.ioff;
   const InRec *__restrict__ rec = a.rec;
   unsigned long long *__restrict__ cursor = a.cursor;
-  constexpr bool PV = MODE != 0;  // hash member sets with per-slot hit counters
+  constexpr bool PV = MODE != 0;  // member sets with per-member hit counters
   int64_t *__restrict__ pv = a.pv;
   unsigned int *__restrict__ es = a.es;
   extern __shared__ int32_t smem[];
-  int32_t *bwords = smem;               // kBlockWords
-  int32_t *bcnt = smem + kBlockWords;   // kBlockWords: hash counters or bitmap word starts (modes 1, 2)
-  int32_t *bmcnt = smem + 2 * kBlockWords;  // kBlockDmax: bitmap member counters (modes 1, 2)
+  int32_t *bwords = smem;  // kBlockWords
+  // modes 1, 2: kBlockWords 16-bit member indices (bitmap word starts or
+  // hash slot owners), then kBlockDmax member counters
+  uint16_t *bidx = reinterpret_cast<uint16_t *>(smem + kBlockWords);
+  int32_t *bmcnt = smem + kBlockWords + kBlockWords / 2;
   __shared__ __align__(16) int32_t s_stage[kStageInts];
   __shared__ Task s_task[2];
   __shared__ int s_soff[2];
@@ -689,8 +681,7 @@ __global__ void __launch_bounds__(kThreads, MODE == 0 ? kMinBlocks : 2) k_count(
     const int32_t *mem = s_stage + s_soff[cur];
     Members m;
     m.words = bwords;
-    m.cnt = bcnt;
-    m.pre = bcnt;
+    m.idx = bidx;
     m.mcnt = bmcnt;
     const int nclear = members_layout<PV>(m, mem, t.nmem, kBlockWords, a.bitmap_bits);
     clear_members<PV>(m, nclear, tid, kThreads);
@@ -720,22 +711,12 @@ __global__ void __launch_bounds__(kThreads, MODE == 0 ? kMinBlocks : 2) k_count(
         for (int w = 0; w < kWarps; w++) tot += s_red[w];
         if (tot) atomicAdd(reinterpret_cast<unsigned long long *>(&pv[t.v]), tot);
       }
-      if (m.bitmap) {
-        for (int i = tid; i < t.nmem; i += kThreads)
-          if (bmcnt[i]) atomicAdd(reinterpret_cast<unsigned long long *>(&pv[col[t.r0 + i]]), (unsigned long long)bmcnt[i]);
-      } else {
-        for (int i = tid; i < nclear; i += kThreads)
-          if (bcnt[i]) atomicAdd(reinterpret_cast<unsigned long long *>(&pv[bwords[i]]), (unsigned long long)bcnt[i]);
-      }
+      for (int i = tid; i < t.nmem; i += kThreads)
+        if (bmcnt[i]) atomicAdd(reinterpret_cast<unsigned long long *>(&pv[col[t.r0 + i]]), (unsigned long long)bmcnt[i]);
     }
     if (MODE == 2) {
-      if (m.bitmap) {
-        for (int i = tid; i < t.nmem; i += kThreads)
-          if (bmcnt[i]) atomicAdd(&es[t.r0 + i], unsigned(bmcnt[i]));
-      } else {
-        for (int i = tid; i < nclear; i += kThreads)
-          if (bcnt[i]) credit_member_edge(col, t.r0, t.nmem, bwords[i], unsigned(bcnt[i]), es);
-      }
+      for (int i = tid; i < t.nmem; i += kThreads)
+        if (bmcnt[i]) atomicAdd(&es[t.r0 + i], unsigned(bmcnt[i]));
     }
     if (PV) __syncthreads();
   }
@@ -752,8 +733,7 @@ __global__ void __launch_bounds__(kThreads, MODE == 0 ? kMinBlocks : 2) k_count(
       const int32_t *mem = wstage + so;
       Members m;
       m.words = bwords + warp * kWarpWords;
-      m.cnt = bcnt + warp * kWarpWords;
-      m.pre = m.cnt;
+      m.idx = bidx + warp * kWarpWords;
       m.mcnt = bmcnt + warp * kWarpDmax;
       const int nclear = members_layout<PV>(m, mem, t.nmem, kWarpWords, a.bitmap_bits);
       clear_members<PV>(m, nclear, lane, 32);
@@ -769,25 +749,14 @@ __global__ void __launch_bounds__(kThreads, MODE == 0 ? kMinBlocks : 2) k_count(
         for (int o = 16; o; o >>= 1) h += __shfl_xor_sync(0xffffffffu, h, o);
         __syncwarp();
         if (lane == 0 && h) atomicAdd(reinterpret_cast<unsigned long long *>(&pv[t.v]), (unsigned long long)h);
-        if (m.bitmap) {
-          for (int i = lane; i < t.nmem; i += 32)
-            if (m.mcnt[i])
-              atomicAdd(reinterpret_cast<unsigned long long *>(&pv[mem[i]]), (unsigned long long)m.mcnt[i]);
-        } else {
-          for (int i = lane; i < nclear; i += 32)
-            if (m.cnt[i])
-              atomicAdd(reinterpret_cast<unsigned long long *>(&pv[m.words[i]]), (unsigned long long)m.cnt[i]);
-        }
+        for (int i = lane; i < t.nmem; i += 32)
+          if (m.mcnt[i])
+            atomicAdd(reinterpret_cast<unsigned long long *>(&pv[mem[i]]), (unsigned long long)m.mcnt[i]);
       }
       if (MODE == 2) {
         __syncwarp();
-        if (m.bitmap) {
-          for (int i = lane; i < t.nmem; i += 32)
-            if (m.mcnt[i]) atomicAdd(&es[t.r0 + i], unsigned(m.mcnt[i]));
-        } else {
-          for (int i = lane; i < nclear; i += 32)
-            if (m.cnt[i]) credit_member_edge(col, t.r0, t.nmem, m.words[i], unsigned(m.cnt[i]), es);
-        }
+        for (int i = lane; i < t.nmem; i += 32)
+          if (m.mcnt[i]) atomicAdd(&es[t.r0 + i], unsigned(m.mcnt[i]));
       }
       __syncwarp();
       so = stage_task(wstage, col, rec, tn, lane);
@@ -861,7 +830,8 @@ __global__ void __launch_bounds__(kThreads, MODE == 0 ? kMinBlocks : 2) k_count(
 // dynamic shared memory: member words; in modes 1 and 2 also hash counters
 // or bitmap word starts, and bitmap member counters
 static size_t count_smem_bytes(bool pv) {
-  return sizeof(int32_t) * (pv ? size_t(2) * kBlockWords + kBlockDmax : size_t(kBlockWords));
+  return pv ? sizeof(int32_t) * (kBlockWords + kBlockDmax) + sizeof(uint16_t) * kBlockWords
+            : sizeof(int32_t) * kBlockWords;
 }
 
 // per-vertex counts in internal numbering -> input numbering
