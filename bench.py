@@ -412,16 +412,16 @@ def run_xtric(args) -> None:
         g2.free()
     replicas.barrier()
     torch.cuda.synchronize()
-    e_start = torch.cuda.Event(enable_timing=True)
-    e_end = torch.cuda.Event(enable_timing=True)
-    e_start.record(stream)
-    for _ in range(args.e2e_steps):
+    marks = [torch.cuda.Event(enable_timing=True) for _ in range(args.e2e_steps + 1)]
+    marks[0].record(stream)
+    for i in range(args.e2e_steps):
         g2 = ctx.graph_from_edges(n, hs, hd, xt.ORIENT_DEGREE)  # H2D + build + orient + plan
         e2e_counts.append(g2.count())                          # count + D2H of the result
         g2.free()
-    e_end.record(stream)
+        marks[i + 1].record(stream)
     torch.cuda.synchronize()
-    t_e2e = e_start.elapsed_time(e_end) / 1e3
+    t_e2e = marks[0].elapsed_time(marks[-1]) / 1e3
+    e2e_step_ms = [marks[i].elapsed_time(marks[i + 1]) for i in range(args.e2e_steps)]
     if set(e2e_counts) != set(counts):
         raise RuntimeError(f"end-to-end count {e2e_counts} differs from {counts}")
     e2e_value, _, _ = replicas.aggregate(info["n_edges"] * args.e2e_steps, t_e2e)
@@ -443,7 +443,8 @@ def run_xtric(args) -> None:
                      "kernel_ms": 1e3 * t_kernel, "peak_source": peaks["source"],
                      "tail_grouped_alg_bytes": info["tail_alg_bytes"]},
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 2 * 4 * ne, "d2h_bytes_per_step": 8,
-                "ms_per_step": 1e3 * t_e2e / args.e2e_steps, "steps": args.e2e_steps},
+                "ms_per_step": 1e3 * t_e2e / args.e2e_steps, "steps": args.e2e_steps,
+                "step_ms": [round(x, 2) for x in e2e_step_ms]},
         "gpu_launches": launches, "clocks": clocks, **extra,
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -712,7 +713,7 @@ def main() -> None:
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
-    ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--impl", choices=["xtric", "reference"], default="xtric")
     ap.add_argument("--workload", choices=["rmat24", "chunglu", "rgg", "batch", "serve"], default="rmat24",
                     help="rmat24: the headline single-graph count (R-MAT scale 24); chunglu: the heavy-skew "
