@@ -232,9 +232,22 @@ __global__ void k_plan_fill(int64_t nv, const int64_t *__restrict__ off, const i
     const int64_t k0 = ioff[v], k1 = ioff[v + 1];
     if (nt) tt[nt_pos[v]] = int32_t(v);
     if (nw) {
-      // a few records spread over the whole warp
-      int32_t lg_s = 5;
-      while (lg_s > 0 && (int64_t(32) >> lg_s) < k1 - k0) lg_s--;
+      // The lanes per record that take the warp the fewest steps. Records
+      // are stored longest first, so a batch of 32 / S records runs as many
+      // steps as its first record needs on S lanes (its pairs: the suffix
+      // length plus an average offset into its first pair, over 8); each
+      // batch also costs about one step of set-up.
+      int32_t lg_s = 0;
+      int64_t best = INT64_MAX;
+      for (int32_t ls = 0; ls <= 5; ls++) {
+        const int64_t B = int64_t(32) >> ls, S = int64_t(1) << ls;
+        int64_t steps = 0;
+        for (int64_t i = k0; i < k1; i += B) steps += 1 + ((P[i + 1] - P[i] + 11) / 8 + S - 1) / S;
+        if (steps < best) {
+          best = steps;
+          lg_s = ls;
+        }
+      }
       wt[nw_pos[v]] = make_task(v, k0, k1, off[v], off[v + 1], lg_s);
     }
     if (!nb) continue;
