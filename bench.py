@@ -406,7 +406,7 @@ def run_xtric(args) -> None:
     torch.cuda.empty_cache()
     hs, hd = h_src.numpy(), h_dst.numpy()
     e2e_counts = []
-    for _ in range(1):  # warm the allocator pool and the builder
+    for _ in range(2):  # warm the allocator pool and the builder (the first two steps grow the pool)
         g2 = ctx.graph_from_edges(n, hs, hd, xt.ORIENT_DEGREE)
         e2e_counts.append(g2.count())
         g2.free()

@@ -211,22 +211,6 @@ __device__ __forceinline__ int32_t lanes_log2(int64_t R, int64_t W, int warps, c
   return lg_s;
 }
 
-// Estimated warp-steps of streaming in-records [k0, k1) (longest first) at
-// 2^ls lanes per record with `warps` warps claiming batches: the steps of
-// all batches over the warps (each batch costs about one step of set-up
-// plus what its first record needs), plus the longest batch (the tail).
-// The batches' first records are sampled, at most 64 of them.
-__device__ __forceinline__ int64_t batch_cost(const int64_t *__restrict__ P, int64_t k0, int64_t k1, int ls,
-                                              int warps) {
-  const int64_t B = int64_t(32) >> ls, S = int64_t(1) << ls;
-  const int64_t nb = (k1 - k0 + B - 1) / B;
-  const int64_t m = nb < 64 ? nb : 64;
-  auto steps = [&](int64_t i) { return 1 + ((P[i + 1] - P[i] + 11) / 8 + S - 1) / S; };
-  int64_t sum = 0;
-  for (int64_t j = 0; j < m; j++) sum += steps(k0 + (j * nb / m) * B);
-  return sum * nb / m / warps + steps(k0);
-}
-
 __device__ __forceinline__ Task make_task(int64_t v, int64_t k0, int64_t k1, int64_t r0, int64_t r1, int32_t lg_s) {
   Task t;
   t.k0 = k0;
@@ -272,18 +256,9 @@ __global__ void k_plan_fill(int64_t nv, const int64_t *__restrict__ off, const i
     for (int64_t c = 0; c < chunks; c++) {
       const int64_t kend = (c + 1 == chunks) ? k1 : lower_bound_i64(P, prev, k1, base + (work * (c + 1)) / chunks);
       if (kend <= prev) continue;  // empty chunk (one in-record carries more work)
-      // the heuristic's choice or a neighbour, whichever the step estimate prefers
-      const int32_t h = lanes_log2(kend - prev, P[kend] - P[prev], kWarps, pp);
-      int32_t lg_s = h;
-      int64_t best = batch_cost(P, prev, kend, h, kWarps);
-      for (int32_t ls = h - 1; ls <= h + 1; ls += 2) {
-        if (ls < 0 || ls > 5) continue;
-        const int64_t c = batch_cost(P, prev, kend, ls, kWarps);
-        if (c < best) {
-          best = c;
-          lg_s = ls;
-        }
-      }
+      // (a per-chunk step estimate like the warp tasks' bought 0.17 ms of
+      // count at s24 for 5.8 ms of plan: one thread walks a head's chunks)
+      const int32_t lg_s = lanes_log2(kend - prev, P[kend] - P[prev], kWarps, pp);
       for (int64_t p = 0; p < parts; p++) {
         const int64_t r0 = off[v] + p * kBlockDmax;
         const int64_t r1 = min(off[v + 1], r0 + kBlockDmax);
