@@ -162,16 +162,20 @@ __global__ void k_pad_len(const int64_t *__restrict__ off, int64_t nv, int64_t *
   XT_GRID_STRIDE(u, nv) plen[u] = (off[u + 1] - off[u] + 7) & ~int64_t(7);
 }
 
-// row u of col -> colp[poff[u] ...], the rest of its padded span kPadSentinel
-// (a warp per row)
-__global__ void k_pad_scatter(const int64_t *__restrict__ off, const int32_t *__restrict__ col, int64_t nv,
-                              const int64_t *__restrict__ poff, int32_t *__restrict__ colp) {
-  const int lane = threadIdx.x & 31;
-  const int64_t warp = (blockIdx.x * int64_t(blockDim.x) + threadIdx.x) >> 5;
-  const int64_t nwarps = (int64_t(gridDim.x) * blockDim.x) >> 5;
-  for (int64_t u = warp; u < nv; u += nwarps) {
-    const int64_t a = off[u], len = off[u + 1] - a, q = poff[u], plen = poff[u + 1] - q;
-    for (int64_t i = lane; i < plen; i += 32) colp[q + i] = i < len ? col[a + i] : kPadSentinel;
+// sorted keys (row << b | col) -> the padded columns: key i, the j-th of its
+// row, goes to colp[poff[row] + j]; the row's last key also fills the rest
+// of the row's padded span with kPadSentinel (a thread per key, so short
+// rows cost no idle lanes)
+__global__ void k_pad_fill(const uint64_t *__restrict__ keys, int64_t m, int b, const int64_t *__restrict__ off,
+                           const int64_t *__restrict__ poff, int32_t *__restrict__ colp) {
+  const uint64_t mask = (uint64_t(1) << b) - 1;
+  XT_GRID_STRIDE(i, m) {
+    const uint64_t k = keys[i];
+    const int64_t row = int64_t(k >> b);
+    const int64_t q = poff[row] + (i - off[row]);
+    colp[q] = int32_t(k & mask);
+    if (i + 1 == off[row + 1])
+      for (int64_t t = q + 1, e = poff[row + 1]; t < e; t++) colp[t] = kPadSentinel;
   }
 }
 
@@ -194,13 +198,15 @@ __device__ __forceinline__ uint32_t len_class_desc(int64_t len) {
 // (rows ascend with positions, so these reads are near sequential): lb
 // (0..7) bits of the class fit beside the head in 31 bits
 template <class V>
-__global__ void k_in_keys(const int32_t *__restrict__ col, const int32_t *__restrict__ rowof,
-                          const int64_t *__restrict__ off, const int64_t *__restrict__ poff, int64_t m, int lb,
-                          uint32_t *__restrict__ ik, V *__restrict__ iv, InRec *__restrict__ recp) {
+__global__ void k_in_keys(const uint64_t *__restrict__ keys, int b, const int64_t *__restrict__ off,
+                          const int64_t *__restrict__ poff, int64_t m, int lb, uint32_t *__restrict__ ik,
+                          V *__restrict__ iv, InRec *__restrict__ recp) {
+  const uint64_t mask = (uint64_t(1) << b) - 1;
   XT_GRID_STRIDE(p, m) {
-    const int32_t u = rowof[p];
+    const uint64_t e = keys[p];  // the out-CSR entry at position p: its row and column
+    const int32_t u = int32_t(e >> b);
     const int64_t a = off[u], len = off[u + 1] - p - 1;
-    uint32_t k = uint32_t(col[p]) << lb;
+    uint32_t k = uint32_t(e & mask) << lb;
     if (lb > 0) k |= len_class_desc(len) >> (7 - lb);
     ik[p] = k;
     iv[p] = V(p);
@@ -344,7 +350,8 @@ static xt_status rank_and_relabel(Ctx *c, const int32_t *deg, int64_t nv, int b,
 }
 
 // In-records grouped by head (d_ioff, d_irec), longest suffix first, from the
-// out-CSR. keys/spare: two free buffers of at least m 8-byte entries each.
+// out-CSR. keys: the out-CSR's m sorted keys (row << b | col), read here and
+// then overwritten; spare: a free buffer of at least m 8-byte entries.
 template <class V>
 static xt_status build_in_records(Ctx *c, uint64_t *keys, uint64_t *spare, int64_t m, int64_t nv, int b, Graph *g) {
   const int B = 256;
@@ -352,7 +359,6 @@ static xt_status build_in_records(Ctx *c, uint64_t *keys, uint64_t *spare, int64
   // 4-byte values: keys and values of one side fit one 8-byte buffer
   uint32_t *kin = reinterpret_cast<uint32_t *>(spare), *kout = reinterpret_cast<uint32_t *>(keys);
   V *vin = nullptr, *vout = nullptr, *own_in = nullptr, *own_out = nullptr;
-  int32_t *rowof = nullptr;
   InRec *recp = nullptr;  // in-records in out-position order
   xt_status s = XT_OK;
   if (sizeof(V) == 4) {
@@ -364,16 +370,13 @@ static xt_status build_in_records(Ctx *c, uint64_t *keys, uint64_t *spare, int64
     vin = own_in;
     vout = own_out;
   }
-  if (s == XT_OK) s = dalloc_n(c, &rowof, size_t(m));
   if (s == XT_OK) s = dalloc_n(c, &recp, size_t(m));
   if (s == XT_OK) {
-    k_csr_rows<<<counted(c, grid_for(nv * 32, B, c->sm_count)), B, 0, c->stream>>>(g->d_off, nv, m, rowof, nullptr);
-    k_in_keys<V><<<counted(c, grid_for(m, B, c->sm_count)), B, 0, c->stream>>>(g->d_col, rowof, g->d_off, g->d_poff,
-                                                                               m, lb, kin, vin, recp);
+    // the sorted keys still hold each position's row and column
+    k_in_keys<V><<<counted(c, grid_for(m, B, c->sm_count)), B, 0, c->stream>>>(keys, b, g->d_off, g->d_poff, m, lb,
+                                                                               kin, vin, recp);
     s = cuda_status(c, cudaGetLastError(), "in-keys");
   }
-  dfree(c, rowof);
-  rowof = nullptr;
   // stable: records of one (head, class) stay in position order
   if (s == XT_OK) s = sort_pairs32<V>(c, kin, kout, vin, vout, m, b + lb);
   if (s == XT_OK) s = keys_to_csr<uint32_t>(c, kout, m, nv, lb, g->d_ioff, nullptr);
@@ -417,8 +420,8 @@ static xt_status finish_csr(Ctx *c, uint64_t *keys, uint64_t *spare, int64_t m, 
     XT_TRY(s);
     XT_TRY(dalloc_n(c, &g->d_colp, size_t(total > 0 ? total : 8)));
     if (total > 0)
-      k_pad_scatter<<<counted(c, grid_for(nv * 32, B, c->sm_count)), B, 0, c->stream>>>(g->d_off, g->d_col, nv,
-                                                                                       g->d_poff, g->d_colp);
+      k_pad_fill<<<counted(c, grid_for(m, B, c->sm_count)), B, 0, c->stream>>>(keys, m, b, g->d_off, g->d_poff,
+                                                                               g->d_colp);
     XT_CUDA(c, cudaGetLastError());
   }
   XT_TRY(dalloc_n(c, &g->d_ioff, size_t(nv + 1)));
