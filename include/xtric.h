@@ -130,6 +130,9 @@ xt_status xt_count_async(xt_graph *g, int64_t *d_global, int64_t *d_per_vertex);
  * the order of xt_graph_get_csr (internal numbering; xt_graph_get_perm maps
  * ids back). The supports sum to 3 x global. Synchronous. */
 xt_status xt_count_edges(xt_graph *g, int64_t *global, int64_t *support);
+/* the same into device memory, asynchronous on the context stream;
+ * d_support holds n_edges int64 entries and is overwritten */
+xt_status xt_count_edges_async(xt_graph *g, int64_t *d_global, int64_t *d_support);
 
 /* Replaces the kernel launcher single_gpu_count(nv, d_indices, d_edge_list,
  * d_local_count) (counting.cuh:259-265, counting.cu:537-577): the reference's

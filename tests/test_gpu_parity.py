@@ -339,6 +339,14 @@ def test_edge_support_every_tier(ctx, torch_cuda):
                 if ref is None:
                     ref = oracle_support_of(off, tails, a, b)
                 assert (sup == ref).all(), (orient, lane_work, warp_work)
+            # the device-output form gives the same supports, in csr() order
+            t, host = g.count_edges()
+            dg = torch.zeros(1, dtype=torch.int64, device="cuda")
+            ds = torch.full((len(host),), -1, dtype=torch.int64, device="cuda")
+            torch.cuda.synchronize()
+            g.count_edges_async(dg.data_ptr(), ds.data_ptr())
+            ctx.synchronize()
+            assert int(dg.item()) == t and (ds.cpu().numpy() == host).all()
         finally:
             g.free()
 

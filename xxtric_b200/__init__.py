@@ -81,6 +81,7 @@ _proto("xt_graph_free", _int, _vp)
 _proto("xt_count", _int, _vp, _vp, _vp)
 _proto("xt_count_async", _int, _vp, _vp, _vp)
 _proto("xt_count_edges", _int, _vp, _vp, _vp)
+_proto("xt_count_edges_async", _int, _vp, _vp, _vp)
 _proto("xt_count_device", _int, _i64, _vp, _vp, _vp, _int, _vp)
 _proto("xt_count_device_static", _int, _i64, _vp, _vp, _vp, _int, _vp)
 _proto("xt_graph_from_batch", _int, _vp, _i64, _vp, _vp, _vp, _vp, _int, _P(_vp))
@@ -118,7 +119,7 @@ _proto("xt_rgg_generate", _int, _i64, _int, _dbl, _dbl, _u64, _i64, _P(_i64), _v
 EXPORTED = ["xt_strerror", "xt_last_error", "xt_open", "xt_close", "xt_set_stream", "xt_debug_fail_alloc",
             "xt_launch_count", "xt_synchronize", "xt_graph_get_perm",
             "xt_graph_from_csr", "xt_graph_from_edges", "xt_graph_from_device_edges", "xt_graph_get_info",
-            "xt_graph_get_csr", "xt_graph_free", "xt_count", "xt_count_async", "xt_count_edges", "xt_count_device",
+            "xt_graph_get_csr", "xt_graph_free", "xt_count", "xt_count_async", "xt_count_edges", "xt_count_edges_async", "xt_count_device",
             "xt_count_device_static", "xt_graph_from_batch", "xt_graph_from_device_batch", "xt_graph_groups",
             "xt_count_groups", "xt_count_groups_async", "xt_batch_count", "xt_graph_capture", "xt_graph_set_tuning", "xt_graph_set_tiers",
             "xt_mem_stats", "xt_serve_estimate", "xt_serve_open", "xt_serve_submit", "xt_serve_poll",
@@ -469,6 +470,11 @@ class DeviceGraph:
 
     def count_async(self, d_global, d_per_vertex=None) -> None:
         _check(_L.xt_count_async(self._h, _ptr(d_global), _ptr(d_per_vertex)), "xt_count_async", self.ctx)
+
+    def count_edges_async(self, d_global, d_support) -> None:
+        """Global count and per-edge supports into device memory (d_support:
+        n_edges int64 entries), queued on the context stream."""
+        _check(_L.xt_count_edges_async(self._h, _ptr(d_global), _ptr(d_support)), "xt_count_edges_async", self.ctx)
 
     @property
     def groups(self) -> int:
