@@ -444,7 +444,8 @@ def run_xtric(args) -> None:
                      "tail_grouped_alg_bytes": info["tail_alg_bytes"]},
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 2 * 4 * ne, "d2h_bytes_per_step": 8,
                 "ms_per_step": 1e3 * t_e2e / args.e2e_steps, "steps": args.e2e_steps,
-                "step_ms": [round(x, 2) for x in e2e_step_ms]},
+                "step_ms": [round(x, 2) for x in e2e_step_ms],
+                "median_step_ms": round(statistics.median(e2e_step_ms), 2)},
         "gpu_launches": launches, "clocks": clocks, **extra,
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

@@ -496,7 +496,7 @@ static std::string tune_key(const Graph *g) {
   };
   char buf[512];
   // the schedule revision keeps timings of an older kernel from being reused
-  snprintf(buf, sizeof buf, "sched5|%s|sm%d|orient%d|nv2^%d|ne2^%d|work2^%d|groups%lld", p.name, p.multiProcessorCount,
+  snprintf(buf, sizeof buf, "sched6|%s|sm%d|orient%d|nv2^%d|ne2^%d|work2^%d|groups%lld", p.name, p.multiProcessorCount,
            g->orient, lg(g->nv), lg(g->ne), lg(g->stream_work), (long long)g->n_groups);
   for (char *q = buf; *q; q++)
     if (*q == ' ') *q = '_';

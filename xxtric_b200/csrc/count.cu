@@ -80,7 +80,7 @@ struct PlanParams {
 #define XT_LANE_PAIRS 2
 #endif
 #ifndef XT_TINY_WORK
-#define XT_TINY_WORK 64
+#define XT_TINY_WORK 32
 #endif
 constexpr int32_t kEmpty = -1;
 
