@@ -25,8 +25,8 @@
 //              into parts, one task per (part, chunk)
 // One persistent kernel drains the CTA tasks first (the large ones), then the
 // warp tasks, then the lane tasks, each from its own global atomic cursor.
-// Inside a task, lanes walk whole suffixes in aligned 32-byte pairs, only a
-// record's first and last pair masked (see stream_kind).
+// Inside a task, lanes walk whole suffixes in aligned 32-byte pairs of the
+// padded column array, with no masking (see stream_kind).
 #include <cub/cub.cuh>
 
 #include "xt_internal.cuh"
