@@ -220,3 +220,19 @@ def test_cpp_mirror_compiles_and_reports_no_device(tmp_path):
         pytest.skip("a GPU is present (the GPU test runs the program)")
     r = subprocess.run([exe], capture_output=True, text=True, timeout=120)
     assert r.returncode == 3 and r.stdout.startswith("error 9"), r.stdout
+
+
+def test_bench_traffic_comes_from_the_committed_profile():
+    # the bench line's roofline.traffic is the DRAM bytes per full-size
+    # k_count launch recorded in profiles/; it must parse and be of the
+    # size the profile's table states (tens of GB at R-MAT scale 24)
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("bench_mod", os.path.join(ROOT, "bench.py"))
+    bench = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(bench)
+    t = bench.profiled_traffic("k_count_rmat_s24.md")
+    assert isinstance(t, int) and 1e10 < t < 2e11
+    text = open(os.path.join(ROOT, "profiles", "k_count_rmat_s24.md")).read()
+    gb = float(re.search(r"dram__bytes_read\.sum \| ([0-9.]+) GB", text).group(1))
+    assert abs(t / 1e9 - gb) < 0.1
+    assert bench.profiled_traffic("no_such_profile.md") is None
