@@ -1,4 +1,7 @@
-// The batching form: many independent graphs counted in one launch.
+// The batching form: many independent graphs counted in one launch. It has
+// no counterpart in the reference, whose driver reads or generates one graph
+// per run and counts it once (main.cpp:76-192); each graph's count here
+// equals what the plain single-graph path returns for it.
 //
 // Layout: the graphs are one disjoint union. Graph g owns the ids
 // [voff[g], voff[g+1]) of one concatenated CSR built by the ordinary builder

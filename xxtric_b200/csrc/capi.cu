@@ -1,5 +1,8 @@
 // C ABI entry points (include/xtric.h): contexts, allocation, graph build,
-// counting and the generators.
+// counting and the generators. Together they replace the reference's
+// single-device engine TriangleCountingSingle (xxtric-gpu.hpp:27 constructor:
+// copies the CSR to the device; :192 count(); :272 clear(): frees it) and
+// its kernel launcher single_gpu_count (counting.cu:537-577).
 #include <cmath>
 #include <cstring>
 #include <new>

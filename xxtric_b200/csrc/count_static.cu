@@ -1,5 +1,6 @@
 // xt_count_device_static: the triangle count of a device CSR in the
-// reference's layout that allocates no device memory at all.
+// reference's layout (the int64 offsets and tails that single_gpu_count
+// takes, counting.cu:537-577) that allocates no device memory at all.
 //
 // Who needs it: callers that must not allocate on the device while they run,
 // e.g. a solver whose device memory is entirely pre-reserved by another

@@ -1,4 +1,8 @@
-// Deterministic synthetic-graph generators on the device. Every edge is a
+// Deterministic synthetic-graph generators on the device: R-MAT, Chung-Lu
+// and Erdos-Renyi inputs of the benchmark configurations. The reference
+// generates only its random geometric graph (graph.hpp:745-1364, restated
+// on the host in host/host_io.cpp) and otherwise reads edge lists from
+// files (cugraph/cug_triangle_count.py:23-25). Every edge is a
 // pure function of (seed, edge index), so the same seed yields the same
 // edge list on any GPU and in the CPU oracle's twins of these functions.
 // Integer arithmetic only (quadrant choice by 64x64->128 high products,

@@ -1,5 +1,7 @@
 // The serving form: a request loop that admits count queries under a device
-// memory budget and batches whatever is queued whenever a slot frees up.
+// memory budget and batches whatever is queued whenever a slot frees up. No
+// counterpart in the reference (one graph per run, main.cpp:76-192); every
+// served count equals the query's count through the plain path.
 //
 // Threads: the caller's threads submit and poll; each slot is one host
 // worker thread with its own context (CUDA stream). A free worker takes the
