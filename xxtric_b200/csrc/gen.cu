@@ -1,5 +1,5 @@
 // Deterministic synthetic-graph generators on the device: R-MAT, Chung-Lu
-// and Erdos-Renyi inputs of the benchmark configurations. The reference
+// and Erdos-Renyi graphs. The reference
 // generates only its random geometric graph (graph.hpp:745-1364, restated
 // on the host in host/host_io.cpp) and otherwise reads edge lists from
 // files (cugraph/cug_triangle_count.py:23-25). Every edge is a
