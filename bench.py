@@ -58,6 +58,25 @@ SAMPLE_SCALE = 18
 
 
 
+def env_ranks() -> tuple[int, int, int]:
+    """(rank, world, local rank) from torchrun's environment, without joining
+    a process group or loading the product library."""
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    return rank, world, int(os.environ.get("LOCAL_RANK", str(rank)))
+
+
+def cpu_model() -> str:
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
 def measured_peaks() -> dict:
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(p):
@@ -67,16 +86,17 @@ def measured_peaks() -> dict:
     return {"hbm_gbs": 6650.0, "source": "fallback"}
 
 
-def profiled_traffic(name: str):
-    """DRAM bytes per launch of k_count on this workload from the committed
-    ncu summary (profiles/<name>), if one exists."""
+def profiled_value(name: str, key: str):
+    """A `key: value` line of the committed ncu summary profiles/<name> (the
+    figures the roofline takes from a capture: DRAM bytes per launch, issue
+    utilisation), or None when there is no such summary."""
     p = os.path.join(ROOT, "profiles", name)
     if not os.path.exists(p):
         return None
     for line in open(p):
-        if line.strip().startswith("dram_bytes_per_launch_full_size:"):
+        if line.strip().startswith(key + ":"):
             try:
-                return int(float(line.split(":")[1].split()[0]))
+                return float(line.split(":", 1)[1].split()[0])
             except ValueError:
                 return None
     return None
@@ -195,25 +215,30 @@ class Workload:
         return RGG_N, src, dst
 
     def cpu_sample(self):
-        """(canonical CSR, description) of the graph the CPU reference counts:
-        the workload itself where it finishes in seconds, else a smaller graph
-        of the same generator."""
+        """(canonical CSR, description, config) of the graph the CPU reference
+        counts: the workload itself where it finishes in seconds, else a
+        smaller graph of the same generator. Built by the oracle alone (the
+        reference arm loads nothing of the product)."""
         import oracle
         if self.key == "rmat24":
             sc = min(self.scale, SAMPLE_SCALE)
             n = 1 << sc
             src, dst = oracle.rmat_edges(sc, EDGE_FACTOR << sc, SEED)
-            return oracle.canon_csr(n, src, dst), f"R-MAT scale {sc} of the same generator"
+            cfg = {"workload": workload_name(sc), "scale": sc, "edge_factor": EDGE_FACTOR}
+            return oracle.canon_csr(n, src, dst), f"R-MAT scale {sc} of the same generator", cfg
         if self.key == "chunglu":
             n = 1 << 17
             mx = CHUNGLU_MAX * n / CHUNGLU_N
             cdf, ne = oracle.chunglu_cdf(n, CHUNGLU_GAMMA, CHUNGLU_MEAN, mx)
             src, dst = oracle.chunglu_edges(cdf, ne, SEED)
-            return (oracle.canon_csr(n, src, dst),
-                    f"Chung-Lu n={n:,} of the same generator (exponent {CHUNGLU_GAMMA}, mean {CHUNGLU_MEAN:g}, "
+            what = (f"Chung-Lu n={n:,} of the same generator (exponent {CHUNGLU_GAMMA}, mean {CHUNGLU_MEAN:g}, "
                     f"max expected degree {mx:,.0f})")
-        import xxtric_b200 as xt
-        return xt.generate_rgg(RGG_N, RGG_RANKS, self.radius), "the workload graph itself"
+            cfg = {"workload": what + ", ids permuted; symmetrised + deduped", "n": n, "gamma": CHUNGLU_GAMMA,
+                   "mean_degree": CHUNGLU_MEAN, "max_expected_degree": mx}
+            return oracle.canon_csr(n, src, dst), what, cfg
+        # the reference's own generator restated by the oracle (literal all-pairs form)
+        cfg = {"workload": self.name, **self.extra}
+        return oracle.ref_rgg(RGG_N, RGG_RANKS, self.radius), "the workload graph itself", cfg
 
     def config(self, world: int, info: dict | None) -> dict:
         c = {"workload": self.name, **self.extra, "seed": SEED, "orient": "degree",
@@ -265,7 +290,7 @@ def time_reference_once(path: str, off, tails, cores: int) -> tuple[float, str, 
 
 
 def cpu_baseline(wl: Workload, cores: int, steps: int = 1, warmup: int = 0) -> dict:
-    (off, tails), what = wl.cpu_sample()
+    (off, tails), what, cfg = wl.cpu_sample()
     n_edges = len(tails) // 2
     path = write_vite(off, tails)
     try:
@@ -282,15 +307,16 @@ def cpu_baseline(wl: Workload, cores: int, steps: int = 1, warmup: int = 0) -> d
     finally:
         os.unlink(path)
     total = sum(ts)
-    return {"value": n_edges * len(ts) / total, "unit": UNIT, "cores": cores, "kind": kind,
+    return {"value": n_edges * len(ts) / total, "unit": UNIT, "cores": cores, "cpu_model": cpu_model(),
+            "kind": kind,
             "sample": f"{what} ({n_edges} oriented edges, {tri} triangles), reference OpenMP CPU count, "
                       f"{len(ts)} run(s), {total / len(ts):.4f} s per run",
-            "seconds_per_run": total / len(ts), "n_edges": n_edges}
+            "seconds_per_run": total / len(ts), "n_edges": n_edges, "triangles": tri, "config": cfg,
+            "csr": (off, tails)}
 
 
 def run_reference_arm(args) -> None:
-    from xxtric_b200 import replicas
-    rank, world, _ = replicas.env_ranks()
+    rank, world, _ = env_ranks()
     if rank != 0:
         return  # rank 0 alone times the CPU reference
     if args.workload in ("batch", "serve"):
@@ -304,11 +330,16 @@ def run_reference_arm(args) -> None:
     except Exception as e:  # report, never fake a number
         print(json.dumps({"impl": "reference", "unavailable": f"reference CPU path failed: {e}"[:300]}))
         return
+    # the config names the graph actually timed (a bounded sample of the
+    # workload where the workload itself would take minutes per step)
+    cfg = dict(cb["config"], seed=SEED, orient="the reference's vertex-id precedence (xxtric.hpp:165)",
+               parallelism=f"{cores} OpenMP threads on the host, one rank", sample_of=wl.name,
+               oriented_edges=cb["n_edges"], triangles=cb["triangles"])
     line = {"metric": METRIC, "value": cb["value"], "unit": UNIT, "impl": "reference", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * cb["seconds_per_run"],
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int64",
-            "data": "synthetic", "config": wl.config(world, None),
-            "cpu_baseline": {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")},
+            "data": "synthetic", "config": cfg,
+            "cpu_baseline": {k: cb[k] for k in ("value", "unit", "cores", "cpu_model", "kind", "sample")},
             "e2e": {"value": cb["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
 
@@ -396,11 +427,47 @@ def run_xtric(args) -> None:
         gi.free()
 
     # ---- end to end through the C ABI with host buffers ----
+    e2e = run_e2e(args, ctx, stream, torch, n, ne, src, dst, g, counts, info) if not args.no_e2e else None
+    del src, dst
+    g.free()
+    roofline = roofline_fields(args, info, t_kernel)
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1e3 * t_max / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic",
+        "config": wl.config(world, info), "triangles": counts[0],
+        "triangles_per_s": counts[0] * args.steps * world / t_max,
+        "roofline": roofline, "e2e": e2e, "gpu_launches": launches, "clocks": clocks, **extra,
+    }
+
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            cb = cpu_baseline(wl, os.cpu_count() or 1)
+            line["cpu_baseline"] = {k: cb[k] for k in ("value", "unit", "cores", "cpu_model", "kind", "sample")}
+            line["cpu_sample_on_gpu"] = sample_on_gpu(ctx, stream, torch, cb)
+        except Exception as e:
+            line["cpu_baseline"] = {"value": None, "unavailable": str(e)[:200]}
+    if not args.no_forms and args.workload == "rmat24":
+        # the batching and serving forms, summarised (the full lines: --workload batch|serve)
+        line["batch"] = measure_batch(ctx, stream, torch, steps=5, warmup=3, e2e_steps=2)["summary"]
+        line["serve"] = measure_serve(ctx, local, torch, SERVE_RATES_DEFAULT, max_queries=400)["summary"]
+    del ctx
+    replicas.finish()
+    if rank == 0:
+        print(json.dumps(line))
+
+
+def run_e2e(args, ctx, stream, torch, n, ne, src, dst, g, counts, info) -> dict:
+    """The same metric through the C ABI with host buffers: per step the
+    int32 edge list is copied in from pinned memory, built into the oriented
+    CSR, planned, counted, and the count read back. Frees the resident graph
+    first (its memory goes to the builder)."""
+    import xxtric_b200 as xt
+    from xxtric_b200 import replicas
     h_src = torch.empty(ne, dtype=torch.int32, pin_memory=True)
     h_dst = torch.empty(ne, dtype=torch.int32, pin_memory=True)
     h_src.copy_(src)
     h_dst.copy_(dst)
-    del src, dst
     g.free()
     torch.cuda.synchronize()
     torch.cuda.empty_cache()
@@ -426,38 +493,68 @@ def run_xtric(args) -> None:
         raise RuntimeError(f"end-to-end count {e2e_counts} differs from {counts}")
     e2e_value, _, _ = replicas.aggregate(info["n_edges"] * args.e2e_steps, t_e2e)
 
+    return {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 2 * 4 * ne, "d2h_bytes_per_step": 8,
+            "ms_per_step": 1e3 * t_e2e / args.e2e_steps, "steps": args.e2e_steps,
+            "step_ms": [round(x, 2) for x in e2e_step_ms],
+            "median_step_ms": round(statistics.median(e2e_step_ms), 2)}
+
+
+def roofline_fields(args, info: dict, t_kernel: float) -> dict:
+    """The count kernel's roofline. `achieved` is DRAM bytes per launch over
+    the kernel's CUDA-event time in this run, the DRAM bytes taken from the
+    committed ncu capture of one launch of this workload (`traffic_source`);
+    without a capture it falls back to the bytes the schedule's loads request
+    (`basis` says which). Beside it: the requested (logical) bytes, the
+    compulsory footprint (each array read once), the tail-grouped formula's
+    bytes, and the issue-slot utilisation of the small-case capture."""
     peaks = measured_peaks()
-    achieved = info["alg_bytes"] / t_kernel / 1e9
-    traffic = profiled_traffic(f"k_count_{args.workload}.md") if args.scale == SCALE else None
-    if args.workload == "rmat24" and args.scale == SCALE:
-        traffic = profiled_traffic("k_count_rmat_s24.md")
-    line = {
-        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": 1e3 * t_max / args.steps, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic",
-        "config": wl.config(world, info), "triangles": counts[0],
-        "triangles_per_s": counts[0] * args.steps * world / t_max,
-        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
-                     "frac": achieved / peaks["hbm_gbs"], "traffic": traffic,
-                     "kernel": "k_count<false>", "alg_bytes_per_launch": info["alg_bytes"],
-                     "kernel_ms": 1e3 * t_kernel, "peak_source": peaks["source"],
-                     "tail_grouped_alg_bytes": info["tail_alg_bytes"]},
-        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 2 * 4 * ne, "d2h_bytes_per_step": 8,
-                "ms_per_step": 1e3 * t_e2e / args.e2e_steps, "steps": args.e2e_steps,
-                "step_ms": [round(x, 2) for x in e2e_step_ms],
-                "median_step_ms": round(statistics.median(e2e_step_ms), 2)},
-        "gpu_launches": launches, "clocks": clocks, **extra,
-    }
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        try:
-            cb = cpu_baseline(wl, os.cpu_count() or 1)
-            line["cpu_baseline"] = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")}
-        except Exception as e:
-            line["cpu_baseline"] = {"value": None, "unavailable": str(e)[:200]}
-    del ctx
-    replicas.finish()
-    if rank == 0:
-        print(json.dumps(line))
+    peak = peaks["hbm_gbs"]
+    name = {"rmat24": "k_count_rmat_s24.md", "chunglu": "k_count_chunglu.md"}.get(args.workload)
+    dram = profiled_value(name, "dram_bytes_per_launch_full_size") if name and args.scale == SCALE else None
+    logical = info["alg_bytes"] / t_kernel / 1e9
+    r = {"bound": "hbm", "peak": peak, "unit": "GB/s", "peak_source": peaks["source"],
+         "kernel": "k_count<0>", "kernel_ms": 1e3 * t_kernel}
+    if dram:
+        a = dram / t_kernel / 1e9
+        r.update({"achieved": a, "frac": a / peak, "traffic": int(dram),
+                  "basis": "DRAM bytes per launch (ncu capture of one full-size launch) / kernel time in this run",
+                  "traffic_source": f"profiles/{name} (dram__bytes_read.sum + dram__bytes_write.sum)"})
+    else:
+        r.update({"achieved": logical, "frac": logical / peak, "traffic": None,
+                  "basis": "bytes the schedule's loads request (no ncu capture of this workload committed)",
+                  "traffic_source": None})
+    r.update({"logical_bytes": info["alg_bytes"], "logical_achieved": logical, "logical_frac": logical / peak,
+              "footprint_bytes": info["footprint_bytes"],
+              "footprint_frac": info["footprint_bytes"] / t_kernel / 1e9 / peak,
+              "tail_grouped_alg_bytes": info["tail_alg_bytes"],
+              "tail_grouped_frac": info["tail_alg_bytes"] / t_kernel / 1e9 / peak})
+    small = {"rmat24": "k_count_rmat_s22.md"}.get(args.workload)
+    if small:
+        iss = profiled_value(small, "issue_slots_busy_frac")
+        if iss is not None:
+            r["issue_frac"] = iss
+            r["issue_source"] = f"profiles/{small} (ncu --set full, R-MAT scale 22: sm__inst_issued / issue slots)"
+    return r
+
+
+def sample_on_gpu(ctx, stream, torch, cb: dict) -> dict:
+    """The CPU baseline's sample graph counted on the GPU: the same graph on
+    both sides (built from the same canonical CSR), device time of the count."""
+    import xxtric_b200 as xt
+    off, tails = cb["csr"]
+    g = ctx.graph_from_csr(off, tails, canonical=True)
+    d = torch.zeros(1, dtype=torch.int64, device="cuda")
+    g.count_async(d)
+    torch.cuda.synchronize()
+    tri = int(d.item())
+    t = time_counts(g, stream, torch, 20)
+    ne = g.info()["n_edges"]
+    g.free()
+    if tri != cb["triangles"]:
+        raise RuntimeError(f"sample graph: GPU {tri} triangles, reference {cb['triangles']}")
+    return {"graph": cb["sample"].split(" (")[0], "oriented_edges": ne, "triangles": tri,
+            "gpu_count_ms": 1e3 * t, "gpu_value": ne / t, "cpu_value": cb["value"],
+            "gpu_over_cpu": (ne / t) / cb["value"], "unit": UNIT}
 
 
 BATCH_GRAPHS = 4096
@@ -466,20 +563,13 @@ BATCH_WORKLOAD = ("4,096 graphs: half unit-square random geometric, half Erdos-R
                   "per-graph offset tables, degree-oriented")
 
 
-def run_batch(args) -> None:
-    """Batching form: all graphs in one persistent launch (captured CUDA graph)
-    vs the plain per-graph path on the same GPU; every per-graph count checked
-    against the plain path's."""
-    import torch
-
+def measure_batch(ctx, stream, torch, steps: int, warmup: int, e2e_steps: int) -> dict:
+    """Batching form on one GPU: the 4,096 graphs built as one union, counted
+    in one persistent launch (captured CUDA graph, autotuned schedule), against
+    the plain per-graph path on the same GPU (each graph built and counted
+    alone); every per-graph count checked against the plain path's. Returns
+    the figures ("summary" holds the few that the default bench line carries)."""
     import xxtric_b200 as xt
-    from xxtric_b200 import replicas
-
-    rank, world, local = replicas.init(backend="nccl")
-    torch.cuda.set_device(local)
-    stream = torch.cuda.current_stream()
-    ctx = xt.Context(local)
-    ctx.set_stream(stream.cuda_stream)
     spec = xt.batch_spec(BATCH_GRAPHS, SEED)
     eoff, d_src, d_dst = ctx.gen_batch(spec)
     voff = np.concatenate([[0], np.cumsum(spec["n"])]).astype(np.int64)
@@ -492,26 +582,20 @@ def run_batch(args) -> None:
     info = bg.info()
     d_total = torch.zeros(1, dtype=torch.int64, device="cuda")
     d_per = torch.zeros(ng, dtype=torch.int64, device="cuda")
-    for _ in range(args.warmup):
+    for _ in range(warmup):
         bg.count_groups_async(d_total, d_per)
-    replicas.barrier()
     torch.cuda.synchronize()
-    sampler = ClockSampler(torch.cuda.current_device()) if rank == 0 else None
-    if sampler:
-        sampler.start()
     l0 = ctx.launches
     a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     a.record(stream)
-    for _ in range(args.steps):
+    for _ in range(steps):
         bg.count_groups_async(d_total, d_per)
     b.record(stream)
     torch.cuda.synchronize()
     launches = ctx.launches - l0
-    clocks = sampler.stop() if sampler else None
     t_batch = a.elapsed_time(b) / 1e3
     per = d_per.cpu().numpy()
     total = int(d_total.item())
-    value, _, t_max = replicas.aggregate(ng * args.steps, t_batch)
     bg.free()
     # end to end, batched: host edge lists -> device -> one build -> one count -> per-graph counts
     ts = torch.as_tensor(d_src, device="cuda")
@@ -527,13 +611,13 @@ def run_batch(args) -> None:
     torch.cuda.synchronize()
     ea, eb = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     ea.record(stream)
-    for _ in range(args.e2e_steps):
+    for _ in range(e2e_steps):
         g2 = ctx.graph_from_batch(voff, eoff, hs, hd)
         _, per_e2e = g2.count_groups()
         g2.free()
     eb.record(stream)
     torch.cuda.synchronize()
-    t_e2e = ea.elapsed_time(eb) / 1e3 / args.e2e_steps
+    t_e2e = ea.elapsed_time(eb) / 1e3 / e2e_steps
     if not (per_e2e == per).all():
         raise RuntimeError("end-to-end batch counts differ from the device-resident ones")
     # plain per-graph path: each graph built and counted on its own
@@ -556,27 +640,72 @@ def run_batch(args) -> None:
     plain_e2e_s = time.perf_counter() - p0
     d_src.free()
     d_dst.free()
+    del ts, td, h_src, h_dst
+    torch.cuda.empty_cache()
+    graphs_per_s = ng * steps / t_batch
+    out = {
+        "graphs": ng, "vertices": int(voff[-1]), "edges_generated": int(eoff[-1]), "oriented_edges": info["n_edges"],
+        "triangles": total, "t_batch": t_batch, "steps": steps, "launches": launches,
+        "graphs_per_s": graphs_per_s, "oriented_edges_per_s": info["n_edges"] * steps / t_batch,
+        "e2e_graphs_per_s": ng / t_e2e, "e2e_ms": 1e3 * t_e2e,
+        "h2d_bytes_per_step": 8 * int(eoff[-1]) + 16 * (ng + 1), "d2h_bytes_per_step": 8 * (ng + 1),
+        "plain_count_graphs_per_s": ng / plain_count_s, "plain_e2e_graphs_per_s": ng / plain_e2e_s,
+        "plain_count_s": plain_count_s, "plain_e2e_s": plain_e2e_s,
+        "per_graph_counts_equal_plain": bool(plain_ok), "build_s": build_s, "autotune": tune.get("best", tune),
+    }
+    out["summary"] = {
+        "workload": BATCH_WORKLOAD, "graphs_per_s": round(graphs_per_s, 1),
+        "plain_graphs_per_s": round(ng / plain_count_s, 1), "speedup_vs_plain": round(graphs_per_s * plain_count_s / ng, 3),
+        "e2e_graphs_per_s": round(ng / t_e2e, 1), "plain_e2e_graphs_per_s": round(ng / plain_e2e_s, 1),
+        "e2e_speedup_vs_plain": round(plain_e2e_s / t_e2e, 3),
+        "per_graph_counts_equal_plain": bool(plain_ok), "triangles": total, "ms_per_batch_count": 1e3 * t_batch / steps,
+        "note": "count: device time of one captured launch over all graphs vs the sum of per-graph count times; "
+                "e2e: host edge lists in, per-graph counts out, vs building and counting each graph alone",
+    }
+    return out
+
+
+def run_batch(args) -> None:
+    """The batching form's own bench line (graphs/s)."""
+    import torch
+
+    import xxtric_b200 as xt
+    from xxtric_b200 import replicas
+
+    rank, world, local = replicas.init(backend="nccl")
+    torch.cuda.set_device(local)
+    stream = torch.cuda.current_stream()
+    ctx = xt.Context(local)
+    ctx.set_stream(stream.cuda_stream)
+    replicas.barrier()
+    sampler = ClockSampler(torch.cuda.current_device()) if rank == 0 else None
+    if sampler:
+        sampler.start()
+    m = measure_batch(ctx, stream, torch, args.steps, args.warmup, args.e2e_steps)
+    clocks = sampler.stop() if sampler else None
+    value, _, t_max = replicas.aggregate(m["graphs"] * args.steps, m["t_batch"])
     replicas.finish()
     if rank != 0:
         return
+    ng = m["graphs"]
     line = {
         "metric": "graphs/s (batched count, 4096 graphs)", "value": value, "unit": "graphs/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t_max / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic",
-        "config": {"workload": BATCH_WORKLOAD, "graphs": ng, "vertices": int(voff[-1]), "edges_generated":
-                   int(eoff[-1]), "oriented_edges": info["n_edges"], "seed": SEED,
+        "config": {"workload": BATCH_WORKLOAD, "graphs": ng, "vertices": m["vertices"],
+                   "edges_generated": m["edges_generated"], "oriented_edges": m["oriented_edges"], "seed": SEED,
                    "l2": "inputs larger than L2, no flush", "launch": "one persistent kernel, captured CUDA graph"},
-        "triangles": total,
-        "oriented_edges_per_s": info["n_edges"] * args.steps * world / t_max,
-        "e2e": {"value": ng / t_e2e, "unit": "graphs/s", "ms_per_step": 1e3 * t_e2e,
-                "h2d_bytes_per_step": 8 * int(eoff[-1]) + 16 * (ng + 1), "d2h_bytes_per_step": 8 * (ng + 1)},
-        "plain": {"count_graphs_per_s": ng / plain_count_s, "e2e_graphs_per_s": ng / plain_e2e_s,
-                  "count_s": plain_count_s, "e2e_s": plain_e2e_s,
+        "triangles": m["triangles"],
+        "oriented_edges_per_s": m["oriented_edges"] * args.steps * world / t_max,
+        "e2e": {"value": m["e2e_graphs_per_s"], "unit": "graphs/s", "ms_per_step": m["e2e_ms"],
+                "h2d_bytes_per_step": m["h2d_bytes_per_step"], "d2h_bytes_per_step": m["d2h_bytes_per_step"]},
+        "plain": {"count_graphs_per_s": m["plain_count_graphs_per_s"], "e2e_graphs_per_s": m["plain_e2e_graphs_per_s"],
+                  "count_s": m["plain_count_s"], "e2e_s": m["plain_e2e_s"],
                   "note": "each graph built and counted alone (device edge lists), same GPU"},
-        "speedup_vs_plain": {"count": (ng / t_batch * args.steps) / (ng / plain_count_s),
-                             "e2e": (ng / t_e2e) / (ng / plain_e2e_s)},
-        "per_graph_counts_equal_plain": bool(plain_ok), "build_s": build_s,
-        "autotune": tune.get("best", tune), "gpu_launches": launches, "clocks": clocks,
+        "speedup_vs_plain": {"count": m["graphs_per_s"] / m["plain_count_graphs_per_s"],
+                             "e2e": m["e2e_graphs_per_s"] / m["plain_e2e_graphs_per_s"]},
+        "per_graph_counts_equal_plain": m["per_graph_counts_equal_plain"], "build_s": m["build_s"],
+        "autotune": m["autotune"], "gpu_launches": m["launches"], "clocks": clocks,
     }
     print(json.dumps(line))
 
@@ -586,26 +715,22 @@ SERVE_WORKLOAD = ("count queries on R-MAT graphs (a=.57 b=.19 c=.19 d=.05, edge 
                   "lists (int32) copied in per query; degree-oriented")
 SERVE_RATES = (10, 30, 100, 300, 1000, 3000, 10000)
 SERVE_POOL = 48
+# the default bench line: one rate below saturation, one above
+SERVE_RATES_DEFAULT = (100, 3000)
 
 
 def _pct(xs, q):
     return float(np.percentile(np.asarray(xs) * 1e3, q)) if len(xs) else None
 
 
-def run_serve(args) -> None:
-    """Serving form: Poisson arrival streams at several rates, served with
+def measure_serve(ctx, local: int, torch, rates, max_queries: int = 600) -> dict:
+    """Serving form: Poisson arrival streams at the given rates, served with
     admission by memory budget and continuous batching (xt_serve_*), against
     the plain per-query path (build + count per query, one at a time) under
-    the same arrivals. Every served count must equal the query's solo count."""
-    import torch
-
+    the same arrivals. Every served and plain count is checked against the
+    query's solo count. Returns the sweep ("summary": the default line's)."""
     import xxtric_b200 as xt
-    from xxtric_b200 import replicas
-
-    rank, world, local = replicas.init(backend="nccl")
-    torch.cuda.set_device(local)
     rng = np.random.default_rng(SEED + 5)
-    ctx = xt.Context(local)
     pool = []  # (nv, pinned src, pinned dst)
     for i in range(SERVE_POOL):
         scale = int(rng.integers(10, 21))
@@ -636,8 +761,8 @@ def run_serve(args) -> None:
     sweep = []
     exact = True
     l_plain0 = ctx.launches
-    for lam in SERVE_RATES:
-        n = int(min(600, max(30, 3 * lam)))
+    for lam in rates:
+        n = int(min(max_queries, max(30, 3 * lam)))
         arr = np.cumsum(rng.exponential(1.0 / lam, n))
         arr -= arr[0]
         which = rng.integers(0, SERVE_POOL, n)
@@ -679,6 +804,35 @@ def run_serve(args) -> None:
                       "plain": {"p50_ms": _pct(plat, 50), "p99_ms": _pct(plat, 99), "graphs_per_s": n / plain_s}})
     st = srv.stats()
     srv.close()
+    out = {"pool": pool, "sweep": sweep, "exact": bool(exact), "stats": st, "stats0": st0,
+           "plain_launches": ctx.launches - l_plain0}
+    out["summary"] = {
+        "workload": SERVE_WORKLOAD, "budget_bytes": st["budget_bytes"], "slots": 3,
+        "rates": [{"rate_per_s": r["rate_per_s"], "queries": r["queries"],
+                   "served_p50_ms": round(r["served"]["p50_ms"], 2), "served_p99_ms": round(r["served"]["p99_ms"], 2),
+                   "served_graphs_per_s": round(r["served"]["graphs_per_s"], 1),
+                   "plain_p50_ms": round(r["plain"]["p50_ms"], 2), "plain_p99_ms": round(r["plain"]["p99_ms"], 2),
+                   "plain_graphs_per_s": round(r["plain"]["graphs_per_s"], 1),
+                   "graphs_per_batch": round(r["served"]["graphs_per_batch"], 2)} for r in sweep],
+        "counts_equal_solo": bool(exact),
+        "note": "served: xt_serve_* with admission by device-memory budget and continuous batching; plain: "
+                "build + count per query, one at a time, same arrivals; latency = submit to result",
+    }
+    return out
+
+
+def run_serve(args) -> None:
+    """The serving form's own bench line: the full rate sweep."""
+    import torch
+
+    import xxtric_b200 as xt
+    from xxtric_b200 import replicas
+
+    rank, world, local = replicas.init(backend="nccl")
+    torch.cuda.set_device(local)
+    ctx = xt.Context(local)
+    m = measure_serve(ctx, local, torch, SERVE_RATES)
+    sweep, st, st0, pool = m["sweep"], m["stats"], m["stats0"], m["pool"]
     top = sweep[-1]
     line = {
         "metric": "graphs/s (served count queries, Poisson arrivals)", "value": top["served"]["graphs_per_s"],
@@ -694,18 +848,18 @@ def run_serve(args) -> None:
                 "h2d_bytes_per_step": 8 * top["edge_rows"], "d2h_bytes_per_step": 8 * top["queries"],
                 "note": "a step is one rate's stream; the served path is end to end by construction"},
         "speedup_vs_plain_at_top_rate": top["served"]["graphs_per_s"] / top["plain"]["graphs_per_s"],
-        "counts_equal_solo": bool(exact),
+        "counts_equal_solo": m["exact"],
         "server": {k: st[k] - st0.get(k, 0) if k in ("submitted", "completed", "batches", "launches") else st[k]
                    for k in ("submitted", "completed", "failed", "rejected", "batches", "max_batch", "budget_peak",
                              "device_peak", "launches")},
         "gpu_launches": st["launches"] - st0["launches"],
-        "plain_launches": ctx.launches - l_plain0,
+        "plain_launches": m["plain_launches"],
     }
     ctx.close()
     replicas.finish()
     if rank == 0:
         print(json.dumps(line))
-    if not exact:
+    if not m["exact"]:
         raise SystemExit("served counts differ from the solo counts")
 
 
@@ -724,6 +878,10 @@ def main() -> None:
                     help="R-MAT scale of the single-graph workload (24 is the headline; smaller scales are the "
                          "small cases that profiler captures run on)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-forms", action="store_true",
+                    help="leave the batching and serving summaries out of the default line")
+    ap.add_argument("--no-e2e", action="store_true",
+                    help="skip the end-to-end leg (profiler captures of the count kernel)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)  # timing rule: at least 3 untimed warm-up steps
     if args.impl == "reference":

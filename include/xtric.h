@@ -46,7 +46,11 @@ typedef enum { XT_ORIENT_ID = 0, XT_ORIENT_DEGREE = 1 } xt_orient;
 /* xt_graph_from_csr flag: the CSR is already canonical (rows sorted, no
  * duplicates, symmetric, no self loops), the contract under which the
  * reference reads vite files (graph.hpp:294-395), so deduplication is skipped.
- * Without it the rows are canonicalised on the device first. */
+ * The reference trusts that contract; here one device pass checks it (rows
+ * strictly ascending without their own id, every entry listed back in its
+ * partner's row) and the build returns XT_ERR_INVALID before using a row
+ * that breaks it. Without the flag the rows are canonicalised on the device
+ * first. */
 #define XT_CSR_CANONICAL 1
 
 typedef struct xt_ctx xt_ctx;
@@ -62,11 +66,16 @@ typedef struct {
   int64_t wedge_work;     /* sum over oriented (u,v) of d+(v): items a tail-grouped count streams */
   int64_t stream_work;    /* sum over u of C(d+(u),2): candidate columns this count streams (the
                              suffix of N+(u) after each out-neighbour) */
-  int64_t alg_bytes;      /* bytes this count reads at least once: 16(nv+1) offsets + 4|E+| member
-                             columns + 16|E+| in-records + 4 stream_work candidates */
+  int64_t alg_bytes;      /* bytes the count's loads request, repeats included (a suffix streamed by
+                             several heads counts each time; L2 serves many of the repeats):
+                             16(nv+1) offsets + 4|E+| member columns + 16|E+| in-records +
+                             4 stream_work candidate columns */
   int64_t tail_alg_bytes; /* the tail-grouped figure: 8(nv+1) + 4|E+| + sum (16 + 4 d+(v)) */
   int32_t orient;         /* xt_orient used */
   int32_t reserved;
+  int64_t footprint_bytes; /* bytes of the arrays the count reads, each counted once: offsets and
+                              in-record offsets 16(nv+1), columns 4|E+|, padded columns, in-records
+                              16|E+|: the DRAM traffic of a count that never re-reads */
 } xt_graph_info;
 
 /* ---- context ------------------------------------------------------------
@@ -139,7 +148,9 @@ xt_status xt_count_edges_async(xt_graph *g, int64_t *d_global, int64_t *d_suppor
  * device CSR (int64 offsets, int64 tails; rows sorted, deduped, symmetric)
  * is oriented and counted on the given stream. Unlike the reference, which
  * accumulates into a caller-zeroed counter and reports nothing, this
- * overwrites *d_count (accumulate != 0 adds instead) and returns errors.
+ * overwrites *d_count (accumulate != 0 adds instead) and returns errors;
+ * rows that break the layout's promise are rejected with XT_ERR_INVALID (see
+ * XT_CSR_CANONICAL) and *d_count is left as it was.
  * Scratch memory is allocated stream-ordered and released before return. */
 xt_status xt_count_device(int64_t nv, const int64_t *d_indices, const int64_t *d_edge_list, int64_t *d_count,
                           int accumulate, void *cuda_stream);
@@ -155,9 +166,13 @@ xt_status xt_count_device(int64_t nv, const int64_t *d_indices, const int64_t *d
  * device sets up the array's address (make it before any stream capture).
  * Calls that overlap on one device race on the shared array: serialise them.
  * Orientation is by vertex id. Overwrites *d_count, or adds to it when
- * accumulate != 0; XT_ERR_INVALID when a row is out of order, repeats an
- * id, holds its own id or an id outside [0, nv), or lacks a back edge (input
- * not symmetric). Synchronises the given stream before returning. */
+ * accumulate != 0; XT_ERR_INVALID when an offset is negative or decreases, a
+ * row is out of order, repeats an id, holds its own id or an id outside
+ * [0, nv), or an edge is listed in one of its two rows only (input not
+ * symmetric, in either direction); on any error *d_count keeps its value.
+ * XT_ERR_CUDA, before anything is launched, when a CUDA error from earlier
+ * work is still pending (it is left for the caller to read). Synchronises the
+ * given stream before returning. */
 xt_status xt_count_device_static(int64_t nv, const int64_t *d_indices, const int64_t *d_edge_list,
                                  int64_t *d_count, int accumulate, void *cuda_stream);
 

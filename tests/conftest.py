@@ -37,5 +37,13 @@ def load_golden():
         return json.load(f)["fixtures"]
 
 
+def load_golden_large():
+    """Counts of the full-size benchmark graphs pinned on the CPU by
+    tests/golden/make_golden_large.py (both oracle counters, and the
+    reference's own binary where recorded)."""
+    with open(os.path.join(GOLDEN_DIR, "golden.json")) as f:
+        return json.load(f).get("large", {})
+
+
 def load_fixtures():
     return dict(np.load(os.path.join(GOLDEN_DIR, "fixtures.npz")))

@@ -128,7 +128,13 @@ def main():
         n = int(a.max()) + 1
         file_fixture("amazon0302", n, a[:, 0], a[:, 1], "cugraph/example-inputs/amazon0302_adj.tsv (ids as given)")
     np.savez_compressed(os.path.join(HERE, "fixtures.npz"), **arrays)
-    with open(os.path.join(HERE, "golden.json"), "w") as f:
+    path = os.path.join(HERE, "golden.json")
+    if os.path.exists(path):  # keep the full-size pins of make_golden_large.py
+        with open(path) as f:
+            old = json.load(f)
+        if "large" in old:
+            golden["large"] = old["large"]
+    with open(path, "w") as f:
         json.dump(golden, f, indent=1, sort_keys=True)
     print("wrote", os.path.join(HERE, "golden.json"))
 

@@ -1,18 +1,40 @@
-"""Parity at the benchmark's sizes through size-independent properties.
+"""Parity at the benchmark's sizes.
 
-The oracle cannot count scale 24 in test time, so the full-size checks are
+The oracle cannot count scale 24 in test time, so the full-size graphs were
+counted ahead of time on the CPU (tests/golden/make_golden_large.py: the
+oracle's merge counter and its restatement of the reference's loop, on the
+oracle's bit-exact twins of the device generators) and their totals and
+per-vertex digests are golden values here. Beside them, size-independent
 properties every correct count satisfies: the same total under both
 orientations and under any relabelling of the vertices, per-vertex counts
 summing to three times the total, and per-vertex counts of sampled vertices
 (hubs included) equal to the oracle's count of edges among their neighbours.
 """
+import hashlib
+
 import numpy as np
 import pytest
 
 import oracle
 import xxtric_b200 as xt
+from conftest import load_golden_large
 
 pytestmark = pytest.mark.gpu
+
+LARGE = load_golden_large()
+
+
+def digest(pv: np.ndarray) -> str:
+    return hashlib.sha256(np.ascontiguousarray(pv, "<i8").tobytes()).hexdigest()
+
+
+def check_large(name: str, t: int, pv: np.ndarray, n_edges: int) -> None:
+    """Total, per-vertex digest and edge count against the CPU-pinned values."""
+    f = LARGE[name]
+    assert t == f["triangles"]
+    assert n_edges == f["undirected"]
+    assert int(pv.sum()) == f["per_vertex_sum"]
+    assert digest(pv) == f["per_vertex_sha256"]
 
 
 @pytest.fixture(scope="module")
@@ -37,12 +59,14 @@ def test_scale22_orientations_and_sampled_vertices(ctx):
     s, d = rmat_device(ctx, scale)
     g_deg = ctx.graph_from_device_edges(n, len(s), s, d, xt.ORIENT_DEGREE)
     t_deg, pv = g_deg.count(per_vertex=True)
+    g_deg_info = g_deg.info()
     g_deg.free()
     g_id = ctx.graph_from_device_edges(n, len(s), s, d, xt.ORIENT_ID)
     t_id = g_id.count()
     g_id.free()
     assert t_deg == t_id
     assert pv.sum() == 3 * t_deg
+    check_large("rmat22", t_deg, pv, g_deg_info["n_edges"])
     off, tails = oracle.canon_csr(n, s.cpu().numpy().astype(np.int64), d.cpu().numpy().astype(np.int64))
     deg = np.diff(off)
     rng = np.random.default_rng(22)
@@ -62,6 +86,7 @@ def test_scale24_properties(ctx):
     g.free()
     assert pv.sum() == 3 * t
     assert inf["n_edges"] == 260453894
+    check_large("rmat24", t, pv, inf["n_edges"])
     # relabel every vertex by a random permutation: same total, permuted counts
     perm = torch.randperm(n, device="cuda", dtype=torch.int64).to(torch.int32)
     ps, pd = perm[s.long()], perm[d.long()]
@@ -84,6 +109,7 @@ def test_scale24_reference_layout_entry(ctx):
     g = ctx.graph_from_device_edges(n, len(s), s, d)
     t = g.count()
     g.free()
+    assert t == LARGE["rmat22_seed5"]["triangles"]
     off, tails = oracle.canon_csr(n, s.cpu().numpy().astype(np.int64), d.cpu().numpy().astype(np.int64))
     d_off = torch.from_numpy(off).cuda()
     d_t = torch.from_numpy(tails).cuda()
@@ -120,6 +146,7 @@ def test_chunglu_config_properties(ctx):
     t_id, pv_id = g_id.count(per_vertex=True)
     g_id.free()
     assert t_id == t and (pv_id == pv).all()
+    check_large("chunglu_full", t, pv, inf["n_edges"])
     off, tails = oracle.canon_csr(n, s.cpu().numpy().astype(np.int64), d.cpu().numpy().astype(np.int64))
     deg = np.diff(off)
     assert inf["max_degree"] == deg.max() and inf["n_edges"] * 2 == len(tails)

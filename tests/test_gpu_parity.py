@@ -84,6 +84,47 @@ def test_noncanonical_input_is_canonicalised(ctx):
     g.free()
 
 
+@pytest.mark.parametrize("orient", ORIENTS)
+def test_canonical_flag_checks_its_promise(ctx, orient):
+    """XT_CSR_CANONICAL skips the sort, so rows that break the promise (out of
+    order, a repeated id, the row's own id, an edge listed from one end only)
+    are rejected on the device before any build or count kernel uses them,
+    and the context stays usable."""
+    bad = [
+        ([0, 2, 4, 6], [2, 1, 0, 2, 0, 1]),      # row 0 out of order
+        ([0, 3, 5, 7], [1, 1, 2, 0, 2, 0, 1]),   # row 0 repeats 1
+        ([0, 3, 5, 7], [0, 1, 2, 0, 2, 0, 1]),   # row 0 holds 0
+        ([0, 2, 3, 5], [1, 2, 2, 0, 1]),         # row 0 lists 1, row 1 lacks 0
+        ([0, 1, 3, 5], [2, 0, 2, 0, 1]),         # row 1 lists 0, row 0 lacks 1
+    ]
+    for o, t in bad:
+        with pytest.raises(xt.XtError) as e:
+            ctx.graph_from_csr(np.array(o, np.int64), np.array(t, np.int64), canonical=True, orient=orient)
+        assert e.value.status == xt.XT_ERR_INVALID, (o, t)
+        # the same rows through the sorting path are canonicalised and counted
+        g = ctx.graph_from_csr(np.array(o, np.int64), np.array(t, np.int64), canonical=False, orient=orient)
+        assert g.count() == 1
+        g.free()
+    off, tails = canon("k64")
+    g = ctx.graph_from_csr(off, tails, canonical=True, orient=orient)
+    assert g.count() == GOLDEN["k64"]["triangles"]
+    g.free()
+
+
+def test_count_device_rejects_broken_rows(torch_cuda):
+    """The reference-layout launcher (xt_count_device) takes the canonical
+    path too: a row out of order is rejected and the counter keeps its value."""
+    torch = torch_cuda
+    out = torch.full((1,), 5, dtype=torch.int64, device="cuda")
+    with pytest.raises(xt.XtError) as e:
+        xt.count_device(3, torch.tensor([0, 2, 4, 6], dtype=torch.int64, device="cuda"),
+                        torch.tensor([2, 1, 0, 2, 0, 1], dtype=torch.int64, device="cuda"), out,
+                        stream=torch.cuda.current_stream().cuda_stream)
+    assert e.value.status == xt.XT_ERR_INVALID
+    torch.cuda.synchronize()
+    assert int(out.item()) == 5
+
+
 @pytest.mark.parametrize("n", [1024, 4096, 16384, 65536])
 def test_reference_rgg_counts(ctx, n):
     off, tails = xt.generate_rgg(n, 1)

@@ -6,6 +6,7 @@ checks (main.cpp:238-275)."""
 import os
 import re
 import subprocess
+import sys
 
 import numpy as np
 import pytest
@@ -222,17 +223,45 @@ def test_cpp_mirror_compiles_and_reports_no_device(tmp_path):
     assert r.returncode == 3 and r.stdout.startswith("error 9"), r.stdout
 
 
-def test_bench_traffic_comes_from_the_committed_profile():
+def test_bench_roofline_figures_come_from_the_committed_profiles():
     # the bench line's roofline.traffic is the DRAM bytes per full-size
-    # k_count launch recorded in profiles/; it must parse and be of the
-    # size the profile's table states (tens of GB at R-MAT scale 24)
+    # k_count launch recorded in profiles/ (and its issue figure the small-case
+    # capture's); they must parse and agree with the profiles' tables
     import importlib.util
     spec = importlib.util.spec_from_file_location("bench_mod", os.path.join(ROOT, "bench.py"))
     bench = importlib.util.module_from_spec(spec)
     spec.loader.exec_module(bench)
-    t = bench.profiled_traffic("k_count_rmat_s24.md")
-    assert isinstance(t, int) and 1e10 < t < 2e11
+    t = bench.profiled_value("k_count_rmat_s24.md", "dram_bytes_per_launch_full_size")
+    assert t is not None and 1e10 < t < 2e11
     text = open(os.path.join(ROOT, "profiles", "k_count_rmat_s24.md")).read()
     gb = float(re.search(r"dram__bytes_read\.sum \| ([0-9.]+) GB", text).group(1))
     assert abs(t / 1e9 - gb) < 0.1
-    assert bench.profiled_traffic("no_such_profile.md") is None
+    iss = bench.profiled_value("k_count_rmat_s22.md", "issue_slots_busy_frac")
+    assert iss is not None and 0.0 < iss <= 1.0
+    text = open(os.path.join(ROOT, "profiles", "k_count_rmat_s22.md")).read()
+    pct = float(re.search(r"issue slots busy \| ([0-9.]+)%", text).group(1))
+    assert abs(100 * iss - pct) < 0.1
+    assert bench.profiled_value("no_such_profile.md", "dram_bytes_per_launch_full_size") is None
+    # the roofline's basis: DRAM bytes over the kernel time when a capture exists
+    class A:
+        workload, scale = "rmat24", bench.SCALE
+    info = {"alg_bytes": 171_750_000_000, "footprint_bytes": 6_800_000_000, "tail_alg_bytes": 744_750_000_000}
+    r = bench.roofline_fields(A, info, 0.030)
+    assert r["traffic"] == int(t) and abs(r["achieved"] - t / 0.030 / 1e9) < 1e-6
+    assert abs(r["frac"] - r["achieved"] / r["peak"]) < 1e-12 and r["logical_frac"] > r["frac"]
+
+
+def test_bench_reference_arm_loads_nothing_of_the_product(tmp_path):
+    # the reference arm times the reference's own CPU path: it must not load
+    # libxtb200.so (checked in a fresh interpreter, on the rgg sample, which
+    # the oracle builds by itself)
+    code = ("import sys, importlib.util; sys.argv=['bench.py']; "
+            f"spec = importlib.util.spec_from_file_location('b', {os.path.join(ROOT, 'bench.py')!r}); "
+            "b = importlib.util.module_from_spec(spec); spec.loader.exec_module(b); "
+            "wl = b.Workload('rgg'); (off, tails), what, cfg = wl.cpu_sample(); "
+            "import os; maps = open('/proc/self/maps').read(); "
+            "print(len(tails), cfg['workload'][:20], 'libxtb200' in maps, 'xxtric_b200' in sys.modules)")
+    r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, timeout=300, cwd=ROOT)
+    assert r.returncode == 0, r.stderr
+    n, *_, loaded, imported = r.stdout.split()
+    assert int(n) > 0 and loaded == "False" and imported == "False"

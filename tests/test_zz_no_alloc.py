@@ -87,3 +87,35 @@ def test_static_scratch_size_limit_and_bad_input():
     xt.count_device_static(3, off, tails, out, stream=torch.cuda.current_stream().cuda_stream)
     torch.cuda.synchronize()
     assert int(out.item()) == 1
+
+
+def test_static_scratch_asymmetric_rows_leave_the_counter_alone():
+    """An edge listed in one of its two rows only is rejected in either
+    direction, and the output counter keeps its value on every error, in the
+    overwrite and the accumulate forms."""
+    import torch
+    stream = torch.cuda.current_stream().cuda_stream
+    cases = [
+        # row 0 lists 1 (1 > 0) but row 1 lacks 0: the upper-row direction
+        ([0, 2, 3, 5], [1, 2, 2, 0, 1]),
+        # row 1 lists 0 (0 < 1) but row 0 lacks 1: the lower-row direction
+        ([0, 1, 3, 5], [2, 0, 2, 0, 1]),
+    ]
+    for o, t in cases:
+        d_o = torch.tensor(o, dtype=torch.int64, device="cuda")
+        d_t = torch.tensor(t, dtype=torch.int64, device="cuda")
+        for acc in (False, True):
+            out = torch.full((1,), 41, dtype=torch.int64, device="cuda")
+            with pytest.raises(xt.XtError) as e:
+                xt.count_device_static(3, d_o, d_t, out, accumulate=acc, stream=stream)
+            assert e.value.status == xt.XT_ERR_INVALID, (o, t, acc)
+            torch.cuda.synchronize()
+            assert int(out.item()) == 41, (o, t, acc)
+    # a bad row (out of order) leaves the counter alone too
+    out = torch.full((1,), 41, dtype=torch.int64, device="cuda")
+    with pytest.raises(xt.XtError):
+        xt.count_device_static(3, torch.tensor([0, 2, 4, 6], dtype=torch.int64, device="cuda"),
+                               torch.tensor([2, 1, 0, 2, 0, 1], dtype=torch.int64, device="cuda"), out,
+                               accumulate=True, stream=stream)
+    torch.cuda.synchronize()
+    assert int(out.item()) == 41

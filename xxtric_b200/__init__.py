@@ -50,7 +50,7 @@ class GraphInfo(ctypes.Structure):
     _fields_ = [("nv", _i64), ("n_input", _i64), ("n_edges", _i64), ("max_degree", _i64),
                 ("max_out_degree", _i64), ("max_in_degree", _i64), ("wedge_work", _i64),
                 ("stream_work", _i64), ("alg_bytes", _i64), ("tail_alg_bytes", _i64),
-                ("orient", _i32), ("reserved", _i32)]
+                ("orient", _i32), ("reserved", _i32), ("footprint_bytes", _i64)]
 
     def as_dict(self) -> dict:
         return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}

@@ -142,6 +142,38 @@ __global__ void k_csr_tails32(const int64_t *__restrict__ tails, int64_t n, int6
   }
 }
 
+// Canonical CSR input check, a warp per row, run once the offsets and ids have
+// passed k_csr_rows / k_csr_tails32: every row strictly ascending (no
+// repeats), without its own id, and every entry (u,t) listed back in row t
+// (binary search of row t, whose bounds were checked). The canonical path
+// takes each row's upper part as it stands, so a row out of order would
+// reach the count's member sets unsorted and an edge listed from one end
+// only would lose its triangles; either sets bit 4 of *err.
+__global__ void k_csr_check_canonical(const int64_t *__restrict__ off, const int32_t *__restrict__ t32, int64_t nv,
+                                      int *__restrict__ err) {
+  const int lane = threadIdx.x & 31;
+  const int64_t nwarps = (int64_t(gridDim.x) * blockDim.x) >> 5;
+  for (int64_t u = (blockIdx.x * int64_t(blockDim.x) + threadIdx.x) >> 5; u < nv; u += nwarps) {
+    const int64_t e0 = off[u], e1 = off[u + 1];
+    bool bad = false;
+    for (int64_t p = e0 + lane; !bad && p < e1; p += 32) {
+      const int32_t t = t32[p];
+      bad = t == u || (p > e0 && t32[p - 1] >= t);
+      if (!bad) {
+        int64_t lo = off[t], hi = off[t + 1];
+        const int64_t end = hi;
+        while (lo < hi) {
+          const int64_t mid = lo + (hi - lo) / 2;
+          if (t32[mid] < u) lo = mid + 1;
+          else hi = mid;
+        }
+        bad = lo >= end || t32[lo] != u;
+      }
+    }
+    if (__any_sync(0xffffffffu, bad) && lane == 0) atomicOr(err, 4);
+  }
+}
+
 // canonical CSR input: each undirected edge once, as the entry (u,t), u < t;
 // the kept entries stay in (row, column) order
 __global__ void k_csr_lower_keys(const int32_t *__restrict__ rows, const int32_t *__restrict__ tails, int64_t n,
@@ -316,8 +348,11 @@ static xt_status check_err(Ctx *c, const char *what) {
   XT_CUDA(c, cudaStreamSynchronize(c->stream));
   if (h) {
     XT_CUDA(c, cudaMemsetAsync(c->d_err, 0, sizeof(int), c->stream));
-    return set_error(c, XT_ERR_INVALID,
-                     std::string(what) + ((h & 1) ? ": vertex id outside [0,nv)" : ": offsets not monotone in [0,ne]"));
+    const char *why = (h & 1)   ? ": vertex id outside [0,nv)"
+                      : (h & 2) ? ": offsets not monotone in [0,ne]"
+                                : ": a row is out of order, repeats an id or holds its own id, or an edge is "
+                                  "missing from its other end's row (not a canonical CSR)";
+    return set_error(c, XT_ERR_INVALID, std::string(what) + why);
   }
   return XT_OK;
 }
@@ -419,6 +454,7 @@ static xt_status finish_csr(Ctx *c, uint64_t *keys, uint64_t *spare, int64_t m, 
     dfree(c, plen);
     XT_TRY(s);
     XT_TRY(dalloc_n(c, &g->d_colp, size_t(total > 0 ? total : 8)));
+    g->colp_len = total;
     if (total > 0)
       k_pad_fill<<<counted(c, grid_for(m, B, c->sm_count)), B, 0, c->stream>>>(keys, m, b, g->d_off, g->d_poff,
                                                                                g->d_colp);
@@ -556,6 +592,12 @@ xt_status build_from_csr(Ctx *c, int64_t nv, const int64_t *d_off, const int64_t
                                                                                     c->d_err);
     if ((s = cuda_status(c, cudaGetLastError(), "k_csr_rows")) != XT_OK) break;
     if ((s = check_err(c, "csr")) != XT_OK) break;
+    if (canonical) {  // the rows are used as they stand: check the promise first
+      k_csr_check_canonical<<<counted(c, grid_for(nv * 32, B, c->sm_count)), B, 0, c->stream>>>(d_off, t32, nv,
+                                                                                                c->d_err);
+      if ((s = cuda_status(c, cudaGetLastError(), "k_csr_check_canonical")) != XT_OK) break;
+      if ((s = check_err(c, "canonical csr")) != XT_OK) break;
+    }
     if (!canonical) {
       s = build_from_edges(c, nv, ne_in, rows, t32, orient, g);
       if (s == XT_OK) g->n_input = ne_in;

@@ -270,6 +270,7 @@ xt_status xt_graph_get_info(const xt_graph *gr, xt_graph_info *info) {
   info->alg_bytes = 16 * (g.nv + 1) + 20 * g.ne + 4 * g.stream_work;
   info->tail_alg_bytes = 8 * (g.nv + 1) + 4 * g.ne + 16 * g.ne + 4 * g.wedge_work;
   info->orient = g.orient;
+  info->footprint_bytes = 16 * (g.nv + 1) + 20 * g.ne + 4 * g.colp_len;
   return XT_OK;
 }
 

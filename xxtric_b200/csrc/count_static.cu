@@ -23,6 +23,10 @@
 // (for example, issued on two streams at once) race on it and give wrong
 // counts: serialise them.
 //
+// Input: the entry cannot sort, so it checks the rows first (order, repeats,
+// self loops, id range, and that every edge is listed from both ends) and on
+// any failure returns XT_ERR_INVALID and leaves *d_count as it was.
+//
 // Set-up: the first call on a device, with that device current, looks the
 // array's device address up (cudaGetSymbolAddress) and keeps it; make that
 // first call before any stream capture.
@@ -44,7 +48,7 @@ struct Header {
   unsigned long long n_heavy;    // entries of the heavy-head list
   unsigned long long cursor_w;   // next head batch for the warp pass
   unsigned long long cursor_c;   // next heavy head for the CTA pass
-  int err;                       // a row is not symmetric (a neighbour's row lacks the back edge)
+  int err;                       // bit 1: an edge lacks its back edge; bit 2: a row fails the row check
 };
 
 constexpr int kThreads = 256;
@@ -78,22 +82,49 @@ __global__ void k_na_init(Header *hdr) {
   hdr->err = 0;
 }
 
-// Input check, a warp per row: offsets that do not decrease, ids in [0, nv),
-// rows strictly ascending (no repeats) and without the row's own id. A
-// violation sets hdr->err (bit 2) and the passes below do nothing, so an
-// unsorted row or an id past nv cannot steer shared- or global-memory indices.
+// Input check, a warp per row: offsets that are not negative and do not
+// decrease, ids in [0, nv), rows strictly ascending (no repeats) and without
+// the row's own id. A violation sets hdr->err (bit 2) and the passes below do
+// nothing, so an unsorted row or an id past nv cannot steer shared- or
+// global-memory indices.
 __global__ void k_na_check(int64_t nv, const int64_t *__restrict__ off, const int64_t *__restrict__ tails,
                            Header *hdr) {
   const int lane = threadIdx.x & 31;
   const int64_t nwarps = (int64_t(gridDim.x) * blockDim.x) >> 5;
   for (int64_t v = (blockIdx.x * int64_t(blockDim.x) + threadIdx.x) >> 5; v < nv; v += nwarps) {
     const int64_t e0 = off[v], e1 = off[v + 1];
-    bool bad = e1 < e0;
+    bool bad = e0 < 0 || e1 < e0;
     for (int64_t p = e0 + lane; !bad && p < e1; p += 32) {
       const int64_t t = tails[p];
       bad = t < 0 || t >= nv || t == v || (p > e0 && tails[p - 1] >= t);
     }
     if (__any_sync(0xffffffffu, bad) && lane == 0) atomicOr(&hdr->err, 2);
+  }
+}
+
+// Symmetry, a warp per row, once the rows have passed k_na_check: every entry
+// t of row v must have v in row t (binary search of the sorted row t). Both
+// directions of a missing back edge set hdr->err (bit 1): the count reads
+// only the upper parts of the rows and would otherwise drop the triangles
+// of an edge listed on one side.
+__global__ void k_na_back(int64_t nv, const int64_t *__restrict__ off, const int64_t *__restrict__ tails,
+                          Header *hdr) {
+  if (hdr->err) return;
+  const int lane = threadIdx.x & 31;
+  const int64_t nwarps = (int64_t(gridDim.x) * blockDim.x) >> 5;
+  for (int64_t v = (blockIdx.x * int64_t(blockDim.x) + threadIdx.x) >> 5; v < nv; v += nwarps) {
+    bool bad = false;
+    for (int64_t p = off[v] + lane; !bad && p < off[v + 1]; p += 32) {
+      const int64_t t = tails[p];
+      int64_t lo = off[t], hi = off[t + 1];
+      while (lo < hi) {
+        const int64_t mid = lo + (hi - lo) / 2;
+        if (tails[mid] < v) lo = mid + 1;
+        else hi = mid;
+      }
+      bad = lo >= off[t + 1] || tails[lo] != v;
+    }
+    if (__any_sync(0xffffffffu, bad) && lane == 0) atomicOr(&hdr->err, 1);
   }
 }
 
@@ -267,7 +298,9 @@ __global__ void __launch_bounds__(kThreads) k_na_cta(const int64_t *__restrict__
   if (lane == 0 && hits) atomicAdd(&sc.hdr->triangles, (unsigned long long)hits);
 }
 
+// the result, only when every check passed: on an error *out keeps its value
 __global__ void k_na_finish(const Header *hdr, int64_t *out, int accumulate) {
+  if (hdr->err) return;
   const int64_t t = int64_t(hdr->triangles);
   *out = accumulate ? *out + t : t;
 }
@@ -298,6 +331,9 @@ extern "C" xt_status xt_count_device_static(int64_t nv, const int64_t *d_indices
   using namespace xt::nalloc;
   if (nv < 1 || !d_indices || !d_edge_list || !d_count) return XT_ERR_INVALID;
   if (nv > kMaxNv) return XT_ERR_OVERFLOW;  // the fixed scratch holds 8 bytes per vertex
+  // an error left pending by the caller's own earlier work is not this call's:
+  // report it without clearing it, before launching anything
+  if (cudaPeekAtLastError() != cudaSuccess) return XT_ERR_CUDA;
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess) return XT_ERR_NO_DEVICE;
   unsigned char *base = nullptr;
@@ -307,19 +343,23 @@ extern "C" xt_status xt_count_device_static(int64_t nv, const int64_t *d_indices
   }
   cudaStream_t st = static_cast<cudaStream_t>(cuda_stream);
   const Scratch sc = carve(base, nv);
-  int sms = 148;
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  int sms = 0;
+  if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms < 1) {
+    cudaGetLastError();
+    return XT_ERR_CUDA;
+  }
   k_na_init<<<1, 1, 0, st>>>(sc.hdr);
   const int64_t gw = (nv * 32 + kThreads - 1) / kThreads;
-  k_na_check<<<unsigned(gw < int64_t(sms) * 32 ? gw : int64_t(sms) * 32), kThreads, 0, st>>>(nv, d_indices,
-                                                                                             d_edge_list, sc.hdr);
+  const unsigned grid_rows = unsigned(gw < int64_t(sms) * 32 ? gw : int64_t(sms) * 32);
+  k_na_check<<<grid_rows, kThreads, 0, st>>>(nv, d_indices, d_edge_list, sc.hdr);
+  k_na_back<<<grid_rows, kThreads, 0, st>>>(nv, d_indices, d_edge_list, sc.hdr);
   const int64_t gs = (nv + kThreads - 1) / kThreads;
   k_na_split<<<unsigned(gs < int64_t(sms) * 32 ? gs : int64_t(sms) * 32), kThreads, 0, st>>>(nv, d_indices,
                                                                                              d_edge_list, sc);
   k_na_warp<<<unsigned(sms * 8), kThreads, 0, st>>>(nv, d_indices, d_edge_list, sc);
   k_na_cta<<<unsigned(sms * 4), kThreads, 0, st>>>(d_indices, d_edge_list, sc);
   k_na_finish<<<1, 1, 0, st>>>(sc.hdr, d_count, accumulate);
-  if (cudaGetLastError() != cudaSuccess) return XT_ERR_CUDA;
+  if (cudaGetLastError() != cudaSuccess) return XT_ERR_CUDA;  // nothing was pending at entry: these launches
   int err = 0;
   if (cudaMemcpyAsync(&err, &sc.hdr->err, sizeof(int), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
       cudaStreamSynchronize(st) != cudaSuccess) {

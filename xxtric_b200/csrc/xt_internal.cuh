@@ -121,7 +121,8 @@ struct Graph {
   int64_t exec_kernels = 0;  // library kernels inside `exec`, counted per replay
   int64_t *d_res = nullptr;
   int64_t wedge_work = 0;   // sum over oriented (u,v) of d+(v)
-  int64_t stream_work = 0;  // sum over oriented (u,v) of d+(u) = sum_u d+(u)^2
+  int64_t stream_work = 0;  // sum over u of C(d+(u), 2): the suffix columns the count streams
+  int64_t colp_len = 0;     // entries of the padded column array
   Plan *plan = nullptr;
 };
 
