@@ -214,8 +214,20 @@ xt_status xt_graph_set_tuning(xt_graph *g, int64_t block_work, int64_t warp_work
  * automatic (the lane tier is on only for graphs of 2^30 or more
  * candidates), 0 = tier off. Re-plans (and re-captures a captured graph). */
 xt_status xt_graph_set_tiers(xt_graph *g, int64_t lane_work, int64_t warp_work);
-/* Autotuner: a coordinate search of the three thresholds, timing `reps`
- * counts each, keeping the fastest; with cache_path it first looks the
+/* Global count: a bulk L2 prefetch of each in-record's suffix one record
+ * batch ahead (on != 0) or none (0, the default). It pays on graphs whose
+ * suffixes are seldom re-read from L2 (many small graphs in one batch) and
+ * costs issue slots on graphs whose suffixes are; the autotuner tries both.
+ * Re-captures a captured graph. */
+xt_status xt_graph_set_prefetch(xt_graph *g, int on);
+/* Test hook, no counterpart in the reference: caps the eviction chain of the
+ * global count's cuckoo member sets at `iters` steps (negative: the default
+ * of 64). With 0 or 1 nearly every hashed set falls back to linear probing,
+ * which lets a test reach that path; counts are unchanged. */
+xt_status xt_graph_debug_cuckoo_iters(xt_graph *g, int iters);
+/* Autotuner: a coordinate search of the three thresholds, then the suffix
+ * prefetch on and off, timing `reps` counts each, keeping the fastest; with
+ * cache_path it first looks the
  * (GPU, graph class) key up in that text file and appends new results.
  * A JSON report of the trials goes to report (nullable). */
 xt_status xt_graph_autotune(xt_graph *g, int reps, const char *cache_path, char *report, int64_t report_len);

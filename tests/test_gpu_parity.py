@@ -321,6 +321,15 @@ def test_each_tier_alone_vs_oracle(ctx, torch_cuda, kind):
                 t, pv = g.count(per_vertex=True)
                 assert t == expect, (orient, lane_work, warp_work)
                 assert (pv == opv).all(), (orient, lane_work, warp_work)
+                # the global-count kernel: cuckoo member sets, their linear-
+                # probing fallback (chains capped at 0 and 1 evictions) and
+                # the bulk suffix prefetch
+                for iters, pf in ((-1, False), (-1, True), (0, False), (1, True)):
+                    g.debug_cuckoo_iters(iters)
+                    g.set_prefetch(pf)
+                    assert g.count() == expect, (orient, lane_work, warp_work, iters, pf)
+                g.debug_cuckoo_iters(-1)
+                g.set_prefetch(False)
             g.set_tiers(1 << 40, 0)
             g.capture()
             assert g.count_groups()[0] == expect  # the captured replay

@@ -93,6 +93,8 @@ _proto("xt_count_groups_async", _int, _vp, _vp, _vp)
 _proto("xt_graph_capture", _int, _vp)
 _proto("xt_graph_set_tuning", _int, _vp, _i64, _i64, _i64)
 _proto("xt_graph_set_tiers", _int, _vp, _i64, _i64)
+_proto("xt_graph_set_prefetch", _int, _vp, _int)
+_proto("xt_graph_debug_cuckoo_iters", _int, _vp, _int)
 _proto("xt_mem_stats", _int, _vp, _P(_i64), _P(_i64), _int)
 _proto("xt_serve_estimate", _i64, _i64, _i64)
 _proto("xt_serve_open", _int, _int, _vp, _P(_vp))
@@ -121,7 +123,8 @@ EXPORTED = ["xt_strerror", "xt_last_error", "xt_open", "xt_close", "xt_set_strea
             "xt_graph_from_csr", "xt_graph_from_edges", "xt_graph_from_device_edges", "xt_graph_get_info",
             "xt_graph_get_csr", "xt_graph_free", "xt_count", "xt_count_async", "xt_count_edges", "xt_count_edges_async", "xt_count_device",
             "xt_count_device_static", "xt_graph_from_batch", "xt_graph_from_device_batch", "xt_graph_groups",
-            "xt_count_groups", "xt_count_groups_async", "xt_batch_count", "xt_graph_capture", "xt_graph_set_tuning", "xt_graph_set_tiers",
+            "xt_count_groups", "xt_count_groups_async", "xt_batch_count", "xt_graph_capture", "xt_graph_set_tuning", "xt_graph_set_tiers", "xt_graph_set_prefetch",
+            "xt_graph_debug_cuckoo_iters",
             "xt_mem_stats", "xt_serve_estimate", "xt_serve_open", "xt_serve_submit", "xt_serve_poll",
             "xt_serve_wait", "xt_serve_get_stats", "xt_serve_close", "xt_serve_batches", "xt_tsv_read", "xt_tsv_write",
             "xt_graph_autotune", "xt_batch_spec", "xt_gen_batch", "xt_device_free",
@@ -497,6 +500,14 @@ class DeviceGraph:
 
     def set_tuning(self, block_work: int = 0, warp_work: int = 0, bitmap_bits: int = 0) -> None:
         _check(_L.xt_graph_set_tuning(self._h, block_work, warp_work, bitmap_bits), "xt_graph_set_tuning", self.ctx)
+
+    def set_prefetch(self, on: bool) -> None:
+        """Bulk L2 prefetch of each in-record's suffix one batch ahead (global count)."""
+        _check(_L.xt_graph_set_prefetch(self._h, int(on)), "xt_graph_set_prefetch", self.ctx)
+
+    def debug_cuckoo_iters(self, iters: int) -> None:
+        """Test hook: cap the cuckoo member sets' eviction chains (-1: default)."""
+        _check(_L.xt_graph_debug_cuckoo_iters(self._h, iters), "xt_graph_debug_cuckoo_iters", self.ctx)
 
     def set_tiers(self, lane_work: int = -1, warp_work: int = -1) -> None:
         """Tier limits of the schedule: heads with at most lane_work candidates

@@ -450,6 +450,12 @@ xt_status set_tiers(Graph *g, int64_t lane_work, int64_t warp_work) {
   return XT_OK;
 }
 
+xt_status set_prefetch(Graph *g, int on) {
+  g->prefetch_suffix = on ? 1 : 0;
+  if (g->exec) XT_TRY(capture_count(g));  // the launch inside the captured graph changes
+  return XT_OK;
+}
+
 xt_status set_tuning(Graph *g, int64_t block_work, int64_t warp_work, int64_t bitmap_bits) {
   const bool was_captured = g->exec != nullptr;
   g->tune_block_work = block_work > 0 ? block_work : 0;
@@ -499,18 +505,19 @@ static std::string tune_key(const Graph *g) {
   };
   char buf[512];
   // the schedule revision keeps timings of an older kernel from being reused
-  snprintf(buf, sizeof buf, "sched6|%s|sm%d|orient%d|nv2^%d|ne2^%d|work2^%d|groups%lld", p.name, p.multiProcessorCount,
+  snprintf(buf, sizeof buf, "sched7|%s|sm%d|orient%d|nv2^%d|ne2^%d|work2^%d|groups%lld", p.name, p.multiProcessorCount,
            g->orient, lg(g->nv), lg(g->ne), lg(g->stream_work), (long long)g->n_groups);
   for (char *q = buf; *q; q++)
     if (*q == ' ') *q = '_';
   return buf;
 }
 
-// Coordinate search over the schedule thresholds: the CTA task size, the
-// warp-task work limit and the largest member id range kept as a bitmap
-// (beyond it the hash is used), each swept with the others held, the best
-// kept. Results are cached per (GPU, graph class) in a text file when a path
-// is given, so a second run of the same class of graph skips the search.
+// Coordinate search over the schedule: the CTA task size, the warp-task work
+// limit and the largest member id range kept as a bitmap (beyond it the hash
+// is used), each swept with the others held, the best kept; then the bulk
+// suffix prefetch on and off. Results are cached per (GPU, graph class) in a
+// text file when a path is given, so a second run of the same class of graph
+// skips the search.
 xt_status autotune(Graph *g, int reps, const char *cache_path, std::string *report) {
   const std::string key = tune_key(g);
   if (cache_path && *cache_path) {
@@ -519,10 +526,12 @@ xt_status autotune(Graph *g, int reps, const char *cache_path, std::string *repo
       while (fgets(line, sizeof line, f)) {
         char k[300];
         long long bw, ww, bb;
+        int pf;
         double ms;
-        if (sscanf(line, "%299s %lld %lld %lld %lf", k, &bw, &ww, &bb, &ms) == 5 && key == k) {
+        if (sscanf(line, "%299s %lld %lld %lld %d %lf", k, &bw, &ww, &bb, &pf, &ms) == 6 && key == k) {
           fclose(f);
           if (report) *report = "{\"cached\": true, \"key\": \"" + key + "\"}";
+          XT_TRY(set_prefetch(g, pf));
           return set_tuning(g, bw, ww, bb);
         }
       }
@@ -531,6 +540,7 @@ xt_status autotune(Graph *g, int reps, const char *cache_path, std::string *repo
   }
   int64_t best[3] = {0, 0, 0};
   double best_ms = 0;
+  XT_TRY(set_prefetch(g, 0));
   XT_TRY(set_tuning(g, 0, 0, 0));
   XT_TRY(time_count(g, reps, &best_ms));
   std::string rep = "{\"key\": \"" + key + "\", \"trials\": [";
@@ -558,14 +568,30 @@ xt_status autotune(Graph *g, int reps, const char *cache_path, std::string *repo
     }
   }
   XT_TRY(set_tuning(g, best[0], best[1], best[2]));
-  snprintf(buf, sizeof buf, "], \"best\": {\"block_work\": %lld, \"warp_work\": %lld, \"bitmap_bits\": %lld, \"ms\": %.4f}}",
-           (long long)best[0], (long long)best[1], (long long)best[2], best_ms);
+  int best_pf = 0;
+  {
+    XT_TRY(set_prefetch(g, 1));
+    double ms = 0;
+    XT_TRY(time_count(g, reps, &ms));
+    snprintf(buf, sizeof buf, ", {\"block_work\": %lld, \"warp_work\": %lld, \"bitmap_bits\": %lld, \"prefetch\": 1, "
+             "\"ms\": %.4f}", (long long)best[0], (long long)best[1], (long long)best[2], ms);
+    rep += buf;
+    if (ms < best_ms) {
+      best_ms = ms;
+      best_pf = 1;
+    }
+    XT_TRY(set_prefetch(g, best_pf));
+  }
+  snprintf(buf, sizeof buf,
+           "], \"best\": {\"block_work\": %lld, \"warp_work\": %lld, \"bitmap_bits\": %lld, \"prefetch\": %d, "
+           "\"ms\": %.4f}}",
+           (long long)best[0], (long long)best[1], (long long)best[2], best_pf, best_ms);
   rep += buf;
   if (report) *report = rep;
   if (cache_path && *cache_path) {
     if (FILE *f = fopen(cache_path, "a")) {
-      fprintf(f, "%s %lld %lld %lld %.4f\n", key.c_str(), (long long)best[0], (long long)best[1], (long long)best[2],
-              best_ms);
+      fprintf(f, "%s %lld %lld %lld %d %.4f\n", key.c_str(), (long long)best[0], (long long)best[1],
+              (long long)best[2], best_pf, best_ms);
       fclose(f);
     }
   }
@@ -714,6 +740,22 @@ xt_status xt_graph_set_tiers(xt_graph *gr, int64_t lane_work, int64_t warp_work)
   if (!gr) return XT_ERR_INVALID;
   cudaSetDevice(gr->g.ctx->device);
   return set_tiers(&gr->g, lane_work, warp_work);
+}
+
+xt_status xt_graph_debug_cuckoo_iters(xt_graph *gr, int iters) {
+  if (!gr || !gr->g.ctx) return XT_ERR_INVALID;
+  gr->g.cuckoo_iters = iters < 0 ? -1 : iters;
+  if (gr->g.exec) {
+    cudaSetDevice(gr->g.ctx->device);
+    return capture_count(&gr->g);
+  }
+  return XT_OK;
+}
+
+xt_status xt_graph_set_prefetch(xt_graph *gr, int on) {
+  if (!gr || !gr->g.ctx) return XT_ERR_INVALID;
+  cudaSetDevice(gr->g.ctx->device);
+  return set_prefetch(&gr->g, on);
 }
 
 xt_status xt_graph_autotune(xt_graph *gr, int reps, const char *cache_path, char *report, int64_t report_len) {

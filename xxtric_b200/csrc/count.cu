@@ -82,6 +82,21 @@ struct PlanParams {
 #ifndef XT_TINY_WORK
 #define XT_TINY_WORK 32
 #endif
+// global count: warp tasks keep hashed member sets as cuckoo tables (two
+// slots per id, branch-free probes) and reset only the slots they filled
+#ifndef XT_WARP_CUCKOO
+#define XT_WARP_CUCKOO 1
+#endif
+// streaming: L2 prefetch of the pair XT_PF_DIST steps ahead (0: none;
+// measured slower: the kernel is issue-bound, R-MAT s24 28.55 -> 30.4 ms at
+// distance 2)
+#ifndef XT_PF_DIST
+#define XT_PF_DIST 0
+#endif
+#ifndef XT_LANE_LOOP
+#define XT_LANE_LOOP 0
+#endif
+constexpr bool kWarpCuckoo = XT_WARP_CUCKOO != 0;
 constexpr int32_t kEmpty = -1;
 
 // A warp or CTA task: the in-records [k0, k0 + nrec) of head v streamed
@@ -304,6 +319,31 @@ __device__ __forceinline__ uint32_t hash_insert(int32_t *tab, uint32_t mask, int
   }
 }
 
+// Cuckoo table (global-count warp tasks): member x is stored as the key x + 1
+// in one of its two slots h1, h2 (0 marks an empty slot, so an all-zero
+// region is an empty table and an empty bitmap at once). Insertion follows
+// Alcantara et al.'s parallel cuckoo hashing: swap the key into its slot,
+// continue with the key it evicted at that key's other slot; a lane whose
+// chain outlasts kCuckooIters reports failure and the task falls back to
+// linear probing. A probe reads both slots, with no loop and no divergence.
+constexpr uint32_t kCuckooMul1 = 0x9E3779B1u, kCuckooMul2 = 0x7FEB352Du;
+constexpr int kCuckooIters = 64;  // eviction chain limit (a test hook can lower it)
+
+__device__ __forceinline__ uint32_t cuckoo_h1(uint32_t key, int shift) { return (key * kCuckooMul1) >> shift; }
+__device__ __forceinline__ uint32_t cuckoo_h2(uint32_t key, int shift) { return (key * kCuckooMul2) >> shift; }
+
+__device__ __forceinline__ bool cuckoo_insert(int32_t *tab, int shift, uint32_t key, int iters) {
+  uint32_t slot = cuckoo_h1(key, shift);
+  for (int it = 0; it < iters; it++) {
+    const uint32_t old = atomicExch(reinterpret_cast<unsigned int *>(&tab[slot]), key);
+    if (old == 0u) return true;
+    key = old;
+    const uint32_t a = cuckoo_h1(key, shift);
+    slot = (slot == a) ? cuckoo_h2(key, shift) : a;
+  }
+  return false;  // `key` is out of the table
+}
+
 // the slot holding x, or -1
 __device__ __forceinline__ int hash_find(const int32_t *tab, uint32_t mask, int shift, int32_t x) {
   uint32_t h = hash_slot(x, shift);
@@ -327,7 +367,11 @@ struct Members {
   uint32_t mask;    // hash: slots - 1
   int shift;        // hash: 32 - log2(slots)
   bool bitmap;
+  bool cuckoo;      // hash kept as a cuckoo table (global-count warp tasks)
 };
+
+// Member-set kinds, one specialised streaming loop each.
+constexpr int kKindHash = 0, kKindBitmap = 1, kKindCuckoo = 2;
 
 // Chooses the structure for members mem[0, n) (ascending) that fits `words`
 // words (a bitmap only while the members' id range is at most bitmap_bits)
@@ -339,6 +383,7 @@ template <bool PV>
 __device__ __forceinline__ int members_layout(Members &m, const int32_t *mem, int n, int words, int64_t bitmap_bits) {
   m.lo = mem[0];
   m.hi = mem[n - 1];
+  m.cuckoo = false;
   const int64_t range = int64_t(m.hi) - int64_t(m.lo) + 1;
   const int64_t nw = int64_t(m.hi >> 5) - int64_t(m.lo >> 5) + 1;
   m.bitmap = nw + 1 <= int64_t(words) && range <= bitmap_bits;
@@ -386,6 +431,55 @@ __device__ __forceinline__ void members_insert(const Members &m, int32_t x) {
   }
 }
 
+// Global-count warp tasks: the member set in a warp slice that is all zero
+// when the task starts: a bitmap over [min, max] when that fits, else a
+// cuckoo table over every slot. Returns false (warp-uniform) when a cuckoo
+// insert failed; the caller then rebuilds the set by linear probing.
+__device__ __forceinline__ bool warp_set_build(Members &m, const int32_t *mem, int n, int words, int64_t bitmap_bits,
+                                               int iters, int lane) {
+  m.lo = mem[0];
+  m.hi = mem[n - 1];
+  const int64_t range = int64_t(m.hi) - int64_t(m.lo) + 1;
+  const int64_t nw = int64_t(m.hi >> 5) - int64_t(m.lo >> 5) + 1;
+  m.bitmap = nw + 1 <= int64_t(words) && range <= bitmap_bits;
+  m.cuckoo = !m.bitmap;
+  bool ok = true;
+  if (m.bitmap) {
+    m.base = uint32_t(m.lo >> 5);
+    m.nwords = uint32_t(nw);
+    m.mask = 0;
+    m.shift = 0;
+    for (int i = lane; i < n; i += 32) members_insert(m, mem[i]);
+  } else {
+    int lg = 6;
+    while ((2 << lg) <= words) lg++;
+    m.base = m.nwords = 0;
+    m.mask = (1u << lg) - 1;
+    m.shift = 32 - lg;
+    for (int i = lane; i < n; i += 32) ok &= cuckoo_insert(m.words, m.shift, uint32_t(mem[i]) + 1u, iters);
+  }
+  return __all_sync(0xffffffffu, ok);
+}
+
+// Returns a warp slice to all zero: clears the bitmap words or cuckoo slots
+// that members [0, n) took.
+__device__ __forceinline__ void warp_set_reset(const Members &m, const int32_t *mem, int n, int lane) {
+  for (int i = lane; i < n; i += 32) {
+    const int32_t x = mem[i];
+    if (m.bitmap) {
+      m.words[uint32_t(x >> 5) - m.base] = 0;
+    } else {
+      const uint32_t key = uint32_t(x) + 1u, a = cuckoo_h1(key, m.shift);
+      if (uint32_t(m.words[a]) == key) m.words[a] = 0;
+      else m.words[cuckoo_h2(key, m.shift)] = 0;
+    }
+  }
+}
+
+__device__ __forceinline__ void zero_words(int32_t *w, int n, int t, int nt) {
+  for (int i = 4 * t; i < n; i += 4 * nt) *reinterpret_cast<int4 *>(w + i) = make_int4(0, 0, 0, 0);
+}
+
 // ---- streaming the in-record suffixes ----------------------------------------
 //
 // A pair is an aligned 32-byte block of 8 columns (one 256-bit load) of the
@@ -419,6 +513,11 @@ __device__ __forceinline__ void prefetch_l2(const void *p, uint32_t bytes) {
   asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
 }
 
+// Asks L2 for the line holding p (no register result, nothing to wait for).
+__device__ __forceinline__ void prefetch_line_l2(const void *p) {
+  asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
+}
+
 // bitmap membership: bit (w & 31) of word (w >> 5) - base; every w outside
 // the bitmap's words lands on the zero guard word
 __device__ __forceinline__ uint32_t bitmap_test(const Members &m, int32_t w) {
@@ -437,11 +536,24 @@ __device__ __forceinline__ int hash_test(const Members &m, int32_t w) {
   return 1;
 }
 
-template <bool PV, bool BITMAP>
+// cuckoo membership: the key w + 1 in either of its two slots (sentinels and
+// ids outside the set match no stored key)
+__device__ __forceinline__ uint32_t cuckoo_test(const Members &m, int32_t w) {
+  const uint32_t key = uint32_t(w) + 1u;
+  const uint32_t x = uint32_t(m.words[cuckoo_h1(key, m.shift)]);
+  const uint32_t y = uint32_t(m.words[cuckoo_h2(key, m.shift)]);
+  return uint32_t(x == key) | uint32_t(y == key);
+}
+
+template <bool PV, int KIND>
 __device__ __forceinline__ int probe_pair(const int4 a, const int4 b, const Members &m) {
-  if (BITMAP) {
+  if (KIND == kKindBitmap) {
     return int((bitmap_test(m, a.x) + bitmap_test(m, a.y)) + (bitmap_test(m, a.z) + bitmap_test(m, a.w)) +
                (bitmap_test(m, b.x) + bitmap_test(m, b.y)) + (bitmap_test(m, b.z) + bitmap_test(m, b.w)));
+  }
+  if (KIND == kKindCuckoo) {
+    return int((cuckoo_test(m, a.x) + cuckoo_test(m, a.y)) + (cuckoo_test(m, a.z) + cuckoo_test(m, a.w)) +
+               (cuckoo_test(m, b.x) + cuckoo_test(m, b.y)) + (cuckoo_test(m, b.z) + cuckoo_test(m, b.w)));
   }
   return hash_test<PV>(m, a.x) + hash_test<PV>(m, a.y) + hash_test<PV>(m, a.z) + hash_test<PV>(m, a.w) +
          hash_test<PV>(m, b.x) + hash_test<PV>(m, b.y) + hash_test<PV>(m, b.z) + hash_test<PV>(m, b.w);
@@ -451,9 +563,9 @@ __device__ __forceinline__ int probe_pair(const int4 a, const int4 b, const Memb
 // the member's index is the word's first index plus the set bits below;
 // hash: the index kept beside its slot) and, per edge, the edge u->w at
 // column position pos
-template <int MODE, bool BITMAP>
+template <int MODE, int KIND>
 __device__ __forceinline__ int probe_one(const Members &m, int32_t w, unsigned int *__restrict__ es, int64_t pos) {
-  if (BITMAP) {
+  if (KIND == kKindBitmap) {
     uint32_t i = uint32_t(w >> 5) - m.base;
     i = i < m.nwords ? i : m.nwords;
     const uint32_t x = uint32_t(m.words[i]);
@@ -467,13 +579,13 @@ __device__ __forceinline__ int probe_one(const Members &m, int32_t w, unsigned i
   return 1;
 }
 
-template <int MODE, bool BITMAP>
+template <int MODE, int KIND>
 __device__ __forceinline__ int probe_pair_counted(const int4 a, const int4 b, const Members &m,
                                                   unsigned int *__restrict__ es, int64_t pos0) {
-  return probe_one<MODE, BITMAP>(m, a.x, es, pos0) + probe_one<MODE, BITMAP>(m, a.y, es, pos0 + 1) +
-         probe_one<MODE, BITMAP>(m, a.z, es, pos0 + 2) + probe_one<MODE, BITMAP>(m, a.w, es, pos0 + 3) +
-         probe_one<MODE, BITMAP>(m, b.x, es, pos0 + 4) + probe_one<MODE, BITMAP>(m, b.y, es, pos0 + 5) +
-         probe_one<MODE, BITMAP>(m, b.z, es, pos0 + 6) + probe_one<MODE, BITMAP>(m, b.w, es, pos0 + 7);
+  return probe_one<MODE, KIND>(m, a.x, es, pos0) + probe_one<MODE, KIND>(m, a.y, es, pos0 + 1) +
+         probe_one<MODE, KIND>(m, a.z, es, pos0 + 2) + probe_one<MODE, KIND>(m, a.w, es, pos0 + 3) +
+         probe_one<MODE, KIND>(m, b.x, es, pos0 + 4) + probe_one<MODE, KIND>(m, b.y, es, pos0 + 5) +
+         probe_one<MODE, KIND>(m, b.z, es, pos0 + 6) + probe_one<MODE, KIND>(m, b.w, es, pos0 + 7);
 }
 
 // Streams the suffixes of in-records [k0, kend) through the member set with
@@ -482,7 +594,12 @@ __device__ __forceinline__ int probe_pair_counted(const int4 a, const int4 b, co
 // hits. Per-vertex mode (MODE 1) credits each record's hits to its owner u;
 // per-edge mode (MODE 2) credits them to the record's own edge u->v and each
 // hit to the edge u->w at the candidate's column.
-template <int MODE, bool BITMAP>
+// PF: a bulk L2 prefetch of each record's suffix one batch ahead (one per
+// record, by the record's first lane): it pays where little of the graph is
+// re-read from L2 (the 4,096-graph batch: 40.3 -> 34.6 ms) and costs issue
+// slots where much is (R-MAT s24: 28.55 -> 30.4 ms), so it is chosen per
+// graph (xt_graph_set_prefetch, the autotuner)
+template <int MODE, int KIND, bool PF>
 __device__ __forceinline__ int64_t stream_kind(const InRec *__restrict__ rec, const int32_t *__restrict__ colp,
                                                int64_t k0, int64_t kend, int lg_s, int *cursor, const Members &m,
                                                int64_t *__restrict__ pv, unsigned int *__restrict__ es,
@@ -521,6 +638,13 @@ __device__ __forceinline__ int64_t stream_kind(const InRec *__restrict__ rec, co
   while (kb < nrec) {  // warp-uniform
     const int32_t nnkb = claim();
     const int4 nn4 = fetch(nnkb);
+    if (PF && k == 0 && n4.z > 0) {
+      // the next batch's suffix into L2 while this batch streams (its record
+      // arrived a batch ago): one bulk prefetch per record, at most 64 KB
+      const int64_t ns = int64_t(uint32_t(n4.x)) | (int64_t(n4.y) << 32);
+      const int64_t nb = int64_t((int32_t(ns & 7) + n4.z + 7) >> 3) * 32;
+      prefetch_l2(colp + (ns & ~int64_t(7)), uint32_t(nb < 65536 ? nb : 65536));
+    }
     const int64_t s = int64_t(uint32_t(r4.x)) | (int64_t(r4.y) << 32);
     const int32_t np = r4.z > 0 ? (int32_t(s & 7) + r4.z + 7) >> 3 : 0;  // pairs of the suffix
     const int32_t cnt = np > k ? ((np - k + S - 1) >> lg_s) : 0;            // this lane's
@@ -531,6 +655,18 @@ __device__ __forceinline__ int64_t stream_kind(const InRec *__restrict__ rec, co
     int4 xa = sent, xb = sent;
     if (cnt > 0) load_pair(colp, P, xa, xb);
     int h = 0;
+#if XT_LANE_LOOP
+    // each lane runs its own pairs and leaves the loop after its last one
+    for (int32_t it = 0; it < cnt; it++) {
+      const int4 a = xa, b = xb;
+      const int64_t pa = P;  // the pair in a, b
+      P += S;
+      if (it + 1 < cnt) load_pair(colp, P, xa, xb);  // next step's pair in flight during the probes
+      if (PV) h += probe_pair_counted<MODE, KIND>(a, b, m, es, 8 * pa + dpos);
+      else h += probe_pair<false, KIND>(a, b, m);
+    }
+    (void)steps;
+#else
     // a lane past its last pair probes sentinels
     for (int32_t it = 0; it < steps; it++) {
       const int4 a = xa, b = xb;
@@ -538,13 +674,17 @@ __device__ __forceinline__ int64_t stream_kind(const InRec *__restrict__ rec, co
       P += S;
       if (it + 1 < cnt) {
         load_pair(colp, P, xa, xb);  // next step's pair in flight during the probes
+#if XT_PF_DIST > 1
+        if (it + XT_PF_DIST < cnt) prefetch_line_l2(colp + 8 * (P + int64_t(XT_PF_DIST - 1) * S));
+#endif
       } else {
         xa = sent;
         xb = sent;
       }
-      if (PV) h += probe_pair_counted<MODE, BITMAP>(a, b, m, es, 8 * pa + dpos);
-      else h += probe_pair<false, BITMAP>(a, b, m);
+      if (PV) h += probe_pair_counted<MODE, KIND>(a, b, m, es, 8 * pa + dpos);
+      else h += probe_pair<false, KIND>(a, b, m);
     }
+#endif
     if (PV) {
       int hr = h;
 #pragma unroll
@@ -563,15 +703,18 @@ __device__ __forceinline__ int64_t stream_kind(const InRec *__restrict__ rec, co
   return hits;
 }
 
-template <int MODE>
+template <int MODE, bool PF>
 __device__ __forceinline__ int64_t stream_suffixes(const InRec *__restrict__ rec, const int32_t *__restrict__ colp,
                                                    int64_t k0, int64_t kend, int lg_s, int *cursor, const Members &m,
                                                    int64_t *__restrict__ pv, unsigned int *__restrict__ es,
                                                    const int64_t *__restrict__ off, const int64_t *__restrict__ poff,
                                                    int lane) {
   // the membership kind is fixed per task: one specialised loop each
-  if (m.bitmap) return stream_kind<MODE, true>(rec, colp, k0, kend, lg_s, cursor, m, pv, es, off, poff, lane);
-  return stream_kind<MODE, false>(rec, colp, k0, kend, lg_s, cursor, m, pv, es, off, poff, lane);
+  if (m.bitmap)
+    return stream_kind<MODE, kKindBitmap, PF>(rec, colp, k0, kend, lg_s, cursor, m, pv, es, off, poff, lane);
+  if (MODE == 0 && kWarpCuckoo && m.cuckoo)
+    return stream_kind<MODE, kKindCuckoo, PF>(rec, colp, k0, kend, lg_s, cursor, m, pv, es, off, poff, lane);
+  return stream_kind<MODE, kKindHash, PF>(rec, colp, k0, kend, lg_s, cursor, m, pv, es, off, poff, lane);
 }
 
 // ---- the count kernel ---------------------------------------------------------
@@ -596,6 +739,7 @@ struct CountArgs {
   const int32_t *group;           // head -> group (a graph of a batch), or null
   unsigned long long *group_out;  // per-group counts when group != null
   int64_t bitmap_bits;            // largest member id range kept as a bitmap
+  int cuckoo_iters;               // cuckoo eviction chain limit
 };
 
 // adds a warp's hits of one task to the task head's group
@@ -655,8 +799,9 @@ __device__ __forceinline__ void clear_members(const Members &m, int nclear, int 
   for (int i = t; i < nclear; i += nt) m.words[i] = m.bitmap ? 0 : kEmpty;
 }
 
-// MODE 0: global count; 1: and per-vertex counts; 2: and per-edge counts
-template <int MODE>
+// MODE 0: global count; 1: and per-vertex counts; 2: and per-edge counts.
+// PF: bulk suffix prefetch (see stream_kind).
+template <int MODE, bool PF>
 // (the per-vertex and per-edge modes hold 56 KB of shared memory, so three
 // of their CTAs fit an SM: their register budget is sized for three)
 __global__ void __launch_bounds__(kThreads, MODE == 0 ? kMinBlocks : 3) k_count(const CountArgs a) {
@@ -704,10 +849,28 @@ __global__ void __launch_bounds__(kThreads, MODE == 0 ? kMinBlocks : 3) k_count(
     m.idx = bidx;
     m.mcnt = bmcnt;
     const int nclear = members_layout<PV>(m, mem, t.nmem, kBlockWords, a.bitmap_bits);
-    clear_members<PV>(m, nclear, tid, kThreads);
-    __syncthreads();
-    for (int i = tid; i < t.nmem; i += kThreads) members_insert_at<PV>(m, mem, i);
-    __syncthreads();
+    if (MODE == 0 && kWarpCuckoo && !m.bitmap) {
+      // a hashed set as a cuckoo table over every slot (load <= 1/4); if a
+      // chain runs too long anywhere, the task falls back to linear probing
+      m.cuckoo = true;
+      zero_words(bwords, nclear, tid, kThreads);
+      __syncthreads();
+      bool ok = true;
+      for (int i = tid; i < t.nmem; i += kThreads)
+        ok &= cuckoo_insert(m.words, m.shift, uint32_t(mem[i]) + 1u, a.cuckoo_iters);
+      if (__syncthreads_or(!ok)) {
+        m.cuckoo = false;
+        clear_members<PV>(m, nclear, tid, kThreads);
+        __syncthreads();
+        for (int i = tid; i < t.nmem; i += kThreads) members_insert_at<PV>(m, mem, i);
+        __syncthreads();
+      }
+    } else {
+      clear_members<PV>(m, nclear, tid, kThreads);
+      __syncthreads();
+      for (int i = tid; i < t.nmem; i += kThreads) members_insert_at<PV>(m, mem, i);
+      __syncthreads();
+    }
     if (warp == 0) {  // stage is free again: bring in the next task
       const Task tn = claim_task(&cursor[0], a.bt, a.n_bt, lane);
       const int so = stage_task(s_stage, col, rec, tn, lane);
@@ -716,7 +879,7 @@ __global__ void __launch_bounds__(kThreads, MODE == 0 ? kMinBlocks : 3) k_count(
         s_soff[cur ^ 1] = so;
       }
     }
-    int64_t h = stream_suffixes<MODE>(rec, a.colp, t.k0, t.k0 + t.nrec, t.lg_s, &s_batch, m, pv, es, off, a.poff,
+    int64_t h = stream_suffixes<MODE, PF>(rec, a.colp, t.k0, t.k0 + t.nrec, t.lg_s, &s_batch, m, pv, es, off, a.poff,
                                       lane);
     acc += h;
     if (a.group) credit_group(a, t.v, h, lane);
@@ -742,7 +905,54 @@ __global__ void __launch_bounds__(kThreads, MODE == 0 ? kMinBlocks : 3) k_count(
   }
 
   // ---- warp tasks: the CTA region split among the warps ----
-  {
+  if (MODE == 0 && kWarpCuckoo) {
+    // The slice holds the CTA tasks' last set: zero it once. A task then
+    // builds its bitmap or cuckoo table into the zeroed slice and, when done,
+    // clears only the words or slots its members took, instead of clearing
+    // the whole 1,024-word slice per task.
+    int32_t *wstage = s_stage + warp * kStageWarp;
+    int32_t *words = bwords + warp * kWarpWords;
+    Task t = claim_task(&cursor[1], a.wt, a.n_wt, lane);
+    int so = stage_task(wstage, col, rec, t, lane);
+    zero_words(words, kWarpWords, lane, 32);
+    while (true) {
+      cp_async_wait_all();
+      __syncwarp();
+      if (t.nrec < 0) break;
+      const int32_t *mem = wstage + so;
+      Members m;
+      m.words = words;
+      m.idx = nullptr;
+      m.mcnt = nullptr;
+      const bool ok = warp_set_build(m, mem, t.nmem, kWarpWords, a.bitmap_bits, a.cuckoo_iters, lane);
+      __syncwarp();
+      const Task tn = claim_task(&cursor[1], a.wt, a.n_wt, lane);  // read after the stream
+      int64_t h;
+      if (ok) {
+        h = stream_suffixes<MODE, PF>(rec, a.colp, t.k0, t.k0 + t.nrec, t.lg_s, nullptr, m, pv, es, off, a.poff, lane);
+        __syncwarp();
+        warp_set_reset(m, mem, t.nmem, lane);
+      } else {
+        // a cuckoo chain ran too long (rare): the same members by linear
+        // probing over the whole slice, which is zeroed again afterwards
+        zero_words(words, kWarpWords, lane, 32);
+        __syncwarp();
+        const int nclear = members_layout<false>(m, mem, t.nmem, kWarpWords, a.bitmap_bits);
+        clear_members<false>(m, nclear, lane, 32);
+        __syncwarp();
+        for (int i = lane; i < t.nmem; i += 32) members_insert_at<false>(m, mem, i);
+        __syncwarp();
+        h = stream_suffixes<MODE, PF>(rec, a.colp, t.k0, t.k0 + t.nrec, t.lg_s, nullptr, m, pv, es, off, a.poff, lane);
+        __syncwarp();
+        zero_words(words, kWarpWords, lane, 32);
+      }
+      acc += h;
+      if (a.group) credit_group(a, t.v, h, lane);
+      __syncwarp();
+      so = stage_task(wstage, col, rec, tn, lane);
+      t = tn;
+    }
+  } else {
     int32_t *wstage = s_stage + warp * kStageWarp;
     Task t = claim_task(&cursor[1], a.wt, a.n_wt, lane);
     int so = stage_task(wstage, col, rec, t, lane);
@@ -761,7 +971,7 @@ __global__ void __launch_bounds__(kThreads, MODE == 0 ? kMinBlocks : 3) k_count(
       for (int i = lane; i < t.nmem; i += 32) members_insert_at<PV>(m, mem, i);
       __syncwarp();
       const Task tn = claim_task(&cursor[1], a.wt, a.n_wt, lane);  // read after the stream
-      int64_t h = stream_suffixes<MODE>(rec, a.colp, t.k0, t.k0 + t.nrec, t.lg_s, nullptr, m, pv, es, off, a.poff,
+      int64_t h = stream_suffixes<MODE, PF>(rec, a.colp, t.k0, t.k0 + t.nrec, t.lg_s, nullptr, m, pv, es, off, a.poff,
                                         lane);
       acc += h;
       if (a.group) credit_group(a, t.v, h, lane);
@@ -914,12 +1124,15 @@ xt_status make_plan(Graph *g) {
     // persistent grids: every CTA that fits on the device at once
     int occ[3] = {0, 0, 0};
     for (int mode = 0; mode < 3 && s == XT_OK; mode++) {
-      auto fn = mode == 0 ? k_count<0> : (mode == 1 ? k_count<1> : k_count<2>);
+      auto fn = mode == 0 ? k_count<0, false> : (mode == 1 ? k_count<1, false> : k_count<2, false>);
       const size_t bytes = count_smem_bytes(mode != 0);
       s = cuda_status(c, cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes)), "attr");
       if (s == XT_OK)
         s = cuda_status(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ[mode], fn, kThreads, bytes), "occ");
     }
+    if (s == XT_OK)
+      s = cuda_status(c, cudaFuncSetAttribute(k_count<0, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                              int(count_smem_bytes(false))), "attr");
     if (s != XT_OK) break;
     pl->grid_global = c->sm_count * (occ[0] > 0 ? occ[0] : 1);
     pl->grid_pv = c->sm_count * (occ[1] > 0 ? occ[1] : 1);
@@ -1084,13 +1297,16 @@ xt_status count_graph(Graph *g, int64_t *d_global, int64_t *d_pv, int64_t *d_gro
   a.group = d_groups ? g->d_group : nullptr;
   a.group_out = reinterpret_cast<unsigned long long *>(d_groups);
   a.bitmap_bits = pl->bitmap_bits;
+  a.cuckoo_iters = g->cuckoo_iters >= 0 ? g->cuckoo_iters : kCuckooIters;
   if (g->ne > 0) {
     if (d_support)
-      k_count<2><<<counted(c, pl->grid_es), kThreads, count_smem_bytes(true), c->stream>>>(a);
+      k_count<2, false><<<counted(c, pl->grid_es), kThreads, count_smem_bytes(true), c->stream>>>(a);
     else if (d_pv)
-      k_count<1><<<counted(c, pl->grid_pv), kThreads, count_smem_bytes(true), c->stream>>>(a);
+      k_count<1, false><<<counted(c, pl->grid_pv), kThreads, count_smem_bytes(true), c->stream>>>(a);
+    else if (g->prefetch_suffix > 0)
+      k_count<0, true><<<counted(c, pl->grid_global), kThreads, count_smem_bytes(false), c->stream>>>(a);
     else
-      k_count<0><<<counted(c, pl->grid_global), kThreads, count_smem_bytes(false), c->stream>>>(a);
+      k_count<0, false><<<counted(c, pl->grid_global), kThreads, count_smem_bytes(false), c->stream>>>(a);
   }
   if (d_support && g->ne > 0)
     k_widen<<<counted(c, grid_for(g->ne, 256, c->sm_count)), 256, 0, c->stream>>>(es, g->ne, d_support);

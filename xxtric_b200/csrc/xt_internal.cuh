@@ -111,6 +111,8 @@ struct Graph {
   int64_t tune_block_work = 0;  // schedule overrides (0: choose automatically)
   int64_t tune_warp_work = 0;
   int64_t tune_bitmap_bits = 0;
+  int prefetch_suffix = 0;      // global count: bulk L2 prefetch of each record's suffix (1) or not (0)
+  int cuckoo_iters = -1;        // test hook: cuckoo eviction chain limit (-1: the default)
   int64_t tier_lane_work = -1;  // tier limits (-1: automatic, 0: tier off)
   int64_t tier_warp_work = -1;
   int32_t *d_group = nullptr;   // internal id -> group (graph of a batch), or null
