@@ -447,6 +447,11 @@ def run_xtric(args) -> None:
             line["cpu_sample_on_gpu"] = sample_on_gpu(ctx, stream, torch, cb)
         except Exception as e:
             line["cpu_baseline"] = {"value": None, "unavailable": str(e)[:200]}
+    if rank == 0 and world == 1 and not args.no_cpu_baseline and args.workload == "rmat24":
+        try:
+            line["reference_gpu"] = reference_gpu_leg(ctx, stream, torch)
+        except Exception as e:
+            line["reference_gpu"] = {"unavailable": str(e)[:200]}
     if not args.no_forms and args.workload == "rmat24":
         # the batching and serving forms, summarised (the full lines: --workload batch|serve)
         line["batch"] = measure_batch(ctx, stream, torch, steps=5, warmup=3, e2e_steps=2)["summary"]
@@ -535,6 +540,54 @@ def roofline_fields(args, info: dict, t_kernel: float) -> dict:
             r["issue_frac"] = iss
             r["issue_source"] = f"profiles/{small} (ncu --set full, R-MAT scale 22: sm__inst_issued / issue slots)"
     return r
+
+
+def reference_gpu_leg(ctx, stream, torch) -> dict:
+    """The reference's own single-GPU engine (oracle/_ref/tric_gpu:
+    TriangleCountingSingle over single_gpu_count, xxtric-gpu.hpp:27-270,
+    counting.cu:537-638, built for sm_100a) and this library's count on the
+    same graphs, on this GPU: R-MAT scales 16 and 18 of the workload's
+    generator and the reference's random geometric graph of config 1. The
+    reference's time is its main()'s timing of count() (the kernel, its
+    synchronisation and the 8-byte read), best of 3 runs; this library's is
+    the count kernel's CUDA-event time. Larger R-MAT scales are left out: the
+    reference's warp-per-vertex loop over a hub's neighbour pairs runs for
+    minutes there."""
+    import oracle
+    if not os.path.exists(oracle.REF_TRIC_GPU):
+        return {"unavailable": "oracle/_ref/tric_gpu is not built (it is built where the reference tree exists)"}
+    graphs = []
+    for sc in (16, 18):
+        src, dst = oracle.rmat_edges(sc, EDGE_FACTOR << sc, SEED)
+        graphs.append((f"R-MAT scale {sc} of the workload's generator", oracle.canon_csr(1 << sc, src, dst)))
+    rgg = Workload("rgg")
+    graphs.append(("the reference's random geometric graph, n=65,536, r=sqrt(16/(pi n)), two strip ranks",
+                   oracle.ref_rgg(RGG_N, RGG_RANKS, rgg.radius)))
+    out = []
+    for name, (off, tails) in graphs:
+        path = write_vite(off, tails)
+        try:
+            runs = [oracle.run_ref(["-f", path], gpu=True, timeout=300) for _ in range(3)]
+        finally:
+            os.unlink(path)
+        bad = [r for r in runs if r["rc"] != 0 or "t_count" not in r]
+        if bad:
+            out.append({"graph": name, "unavailable": "reference GPU run failed: " + bad[0]["stdout"][-200:]})
+            continue
+        t_ref = min(r["t_count"] for r in runs)
+        g = ctx.graph_from_csr(off, tails, canonical=True)
+        d = torch.zeros(1, dtype=torch.int64, device="cuda")
+        g.count_async(d)
+        torch.cuda.synchronize()
+        tri = int(d.item())
+        t = time_counts(g, stream, torch, 20)
+        ne = g.info()["n_edges"]
+        g.free()
+        out.append({"graph": name, "oriented_edges": ne, "triangles": tri,
+                    "reference_triangles": runs[0].get("triangles"),
+                    "reference_ms": 1e3 * t_ref, "xtric_ms": 1e3 * t, "speedup": t_ref / t})
+    return {"binary": "oracle/_ref/tric_gpu (reference main.cpp + xxtric-gpu.hpp + counting.cu, "
+                      "-DUSE_CUDA -DUSE_SINGLE_DEVICE, sm_100a)", "graphs": out}
 
 
 def sample_on_gpu(ctx, stream, torch, cb: dict) -> dict:
@@ -659,6 +712,7 @@ def measure_batch(ctx, stream, torch, steps: int, warmup: int, e2e_steps: int) -
         "e2e_graphs_per_s": round(ng / t_e2e, 1), "plain_e2e_graphs_per_s": round(ng / plain_e2e_s, 1),
         "e2e_speedup_vs_plain": round(plain_e2e_s / t_e2e, 3),
         "per_graph_counts_equal_plain": bool(plain_ok), "triangles": total, "ms_per_batch_count": 1e3 * t_batch / steps,
+        "autotune_best": tune.get("best", tune),
         "note": "count: device time of one captured launch over all graphs vs the sum of per-graph count times; "
                 "e2e: host edge lists in, per-graph counts out, vs building and counting each graph alone",
     }

@@ -1,6 +1,7 @@
 """The oracle: a CPU restatement of sg0/xxtric's counting path and of this
-library's deterministic generators (xtoracle.c), plus the reference's own CPU
-binary built from its sources (oracle/_ref/, see the Makefile).
+library's deterministic generators (xtoracle.c), plus the reference's own
+binaries built from its sources (oracle/_ref/, see the Makefile): its CPU
+count and its single-GPU engine.
 
 TEST INFRASTRUCTURE ONLY. It is loaded by tests/, by __graft_entry__.smoke()
 and by bench.py's CPU-baseline leg, always as the checker or the timed CPU
@@ -19,6 +20,7 @@ LIB = os.path.join(HERE, "liboracle.so")
 REF_DIR = os.path.join(HERE, "_ref")
 REF_TRIC = os.path.join(REF_DIR, "tric")
 REF_TRIC_OMP = os.path.join(REF_DIR, "tric_omp")
+REF_TRIC_GPU = os.path.join(REF_DIR, "tric_gpu")
 REFERENCE_TREE = "/root/reference"
 
 _i64p = np.ctypeslib.ndpointer(np.int64, flags="C")
@@ -27,10 +29,13 @@ _L = None
 
 
 def build(ref: bool = True) -> None:
-    """Compile liboracle.so, and oracle/_ref/ when the reference tree exists."""
+    """Compile liboracle.so, and oracle/_ref/ when the reference tree exists
+    (the CPU binaries, and the single-GPU binary when nvcc is present)."""
     subprocess.run(["make", "-s", "-C", HERE, "all"], check=True)
     if ref and os.path.isdir(REFERENCE_TREE):
         subprocess.run(["make", "-s", "-C", HERE, "ref", f"REF={REFERENCE_TREE}"], check=True)
+        if os.path.exists("/usr/local/cuda/bin/nvcc"):
+            subprocess.run(["make", "-s", "-C", HERE, "refgpu", f"REF={REFERENCE_TREE}"], check=True)
 
 
 def lib() -> ctypes.CDLL:
@@ -184,14 +189,20 @@ def ref_rgg(nv: int, nprocs: int = 1, radius: float = 0.0):
         cap = -m
 
 
-def run_ref(args: list[str], omp: bool = False, threads: int | None = None, timeout: float = 3600) -> dict:
-    """Run the reference's own CPU binary and parse its output lines (main.cpp:129-190)."""
-    exe = REF_TRIC_OMP if omp else REF_TRIC
+def run_ref(args: list[str], omp: bool = False, threads: int | None = None, timeout: float = 3600,
+            gpu: bool = False) -> dict:
+    """Run the reference's own binary (CPU, or its single-GPU engine with
+    gpu=True) and parse its output lines (main.cpp:129-190)."""
+    exe = REF_TRIC_GPU if gpu else (REF_TRIC_OMP if omp else REF_TRIC)
     if not os.path.exists(exe):
         raise FileNotFoundError(exe)
     env = dict(os.environ)
     if threads:
         env["OMP_NUM_THREADS"] = str(threads)
+    if gpu:
+        # modules load with the context (in the constructor), so the timed
+        # count() holds the kernel, its synchronisation and the 8-byte read
+        env["CUDA_MODULE_LOADING"] = "EAGER"
     r = subprocess.run([exe] + args, capture_output=True, text=True, timeout=timeout, env=env)
     out = {"rc": r.returncode, "stdout": r.stdout}
     for line in r.stdout.splitlines():
