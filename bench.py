@@ -485,12 +485,18 @@ def run_e2e(args, ctx, stream, torch, n, ne, src, dst, g, counts, info) -> dict:
     replicas.barrier()
     torch.cuda.synchronize()
     marks = [torch.cuda.Event(enable_timing=True) for _ in range(args.e2e_steps + 1)]
+    host = []  # per step, host wall ms of the build call, the count call and the free
     marks[0].record(stream)
     for i in range(args.e2e_steps):
+        h0 = time.perf_counter()
         g2 = ctx.graph_from_edges(n, hs, hd, xt.ORIENT_DEGREE)  # H2D + build + orient + plan
+        h1 = time.perf_counter()
         e2e_counts.append(g2.count())                          # count + D2H of the result
+        h2 = time.perf_counter()
         g2.free()
         marks[i + 1].record(stream)
+        h3 = time.perf_counter()
+        host.append([round(1e3 * (h1 - h0), 2), round(1e3 * (h2 - h1), 2), round(1e3 * (h3 - h2), 2)])
     torch.cuda.synchronize()
     t_e2e = marks[0].elapsed_time(marks[-1]) / 1e3
     e2e_step_ms = [marks[i].elapsed_time(marks[i + 1]) for i in range(args.e2e_steps)]
@@ -501,7 +507,8 @@ def run_e2e(args, ctx, stream, torch, n, ne, src, dst, g, counts, info) -> dict:
     return {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 2 * 4 * ne, "d2h_bytes_per_step": 8,
             "ms_per_step": 1e3 * t_e2e / args.e2e_steps, "steps": args.e2e_steps,
             "step_ms": [round(x, 2) for x in e2e_step_ms],
-            "median_step_ms": round(statistics.median(e2e_step_ms), 2)}
+            "median_step_ms": round(statistics.median(e2e_step_ms), 2),
+            "host_build_count_free_ms": host}
 
 
 def roofline_fields(args, info: dict, t_kernel: float) -> dict:

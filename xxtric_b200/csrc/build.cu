@@ -70,19 +70,22 @@ __global__ void k_unique_flags(const uint64_t *__restrict__ keys, int64_t n, int
   }
 }
 
-// (degree, id) sort keys of every vertex
-__global__ void k_rank_keys(const int32_t *__restrict__ deg, int64_t nv, uint64_t *__restrict__ vk) {
-  XT_GRID_STRIDE(x, nv) vk[x] = (uint64_t(uint32_t(deg[x])) << 32) | uint64_t(x);
+// every vertex's id (the values of the rank sort, keyed by degree) and the
+// largest degree (how many key bits the sort needs)
+__global__ void k_rank_ids(const int32_t *__restrict__ deg, int64_t nv, int32_t *__restrict__ ids,
+                           unsigned int *__restrict__ dmax) {
+  unsigned int mx = 0;
+  XT_GRID_STRIDE(x, nv) {
+    ids[x] = int32_t(x);
+    mx = max(mx, unsigned(deg[x]));
+  }
+  for (int o = 16; o; o >>= 1) mx = max(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+  if ((threadIdx.x & 31) == 0 && mx) atomicMax(dmax, mx);
 }
 
-// sorted (degree, id) keys -> internal->input and input->internal maps
-__global__ void k_rank_perm(const uint64_t *__restrict__ vk, int64_t nv, int32_t *__restrict__ n2o,
-                            int32_t *__restrict__ o2n) {
-  XT_GRID_STRIDE(r, nv) {
-    const int32_t old = int32_t(vk[r] & 0xffffffffu);
-    n2o[r] = old;
-    o2n[old] = int32_t(r);
-  }
+// ids in (degree, id) order -> input->internal map
+__global__ void k_rank_perm(const int32_t *__restrict__ n2o, int64_t nv, int32_t *__restrict__ o2n) {
+  XT_GRID_STRIDE(r, nv) o2n[n2o[r]] = int32_t(r);
 }
 
 // (lo,hi) in input ids -> (src<<b|dst) in internal ids, src <= dst
@@ -225,14 +228,14 @@ __device__ __forceinline__ uint32_t len_class_desc(int64_t len) {
   return 127u - (c < 127u ? c : 127u);
 }
 
-// (head << lb | length class) sort key and position value for every
-// out-CSR position, and the position's in-record written in position order
-// (rows ascend with positions, so these reads are near sequential): lb
-// (0..7) bits of the class fit beside the head in 31 bits
-template <class V>
+// (head << lb | length class) sort key for every out-CSR position, and the
+// position's in-record, both written in position order (rows ascend with
+// positions, so the row reads are near sequential): lb (0..7) bits of the
+// class fit beside the head in 31 bits. The records then travel through the
+// sort as its values, so no gather from random positions follows.
 __global__ void k_in_keys(const uint64_t *__restrict__ keys, int b, const int64_t *__restrict__ off,
                           const int64_t *__restrict__ poff, int64_t m, int lb, uint32_t *__restrict__ ik,
-                          V *__restrict__ iv, InRec *__restrict__ recp) {
+                          InRec *__restrict__ recp) {
   const uint64_t mask = (uint64_t(1) << b) - 1;
   XT_GRID_STRIDE(p, m) {
     const uint64_t e = keys[p];  // the out-CSR entry at position p: its row and column
@@ -241,20 +244,12 @@ __global__ void k_in_keys(const uint64_t *__restrict__ keys, int b, const int64_
     uint32_t k = uint32_t(e & mask) << lb;
     if (lb > 0) k |= len_class_desc(len) >> (7 - lb);
     ik[p] = k;
-    iv[p] = V(p);
     InRec r;
     r.s = poff[u] + (p - a) + 1;  // the suffix, in the padded column array
     r.len = int32_t(len);
     r.u = u;
     recp[p] = r;
   }
-}
-
-// positions sorted by (head, class) -> in-records grouped by head
-template <class V>
-__global__ void k_in_records(const V *__restrict__ pos, int64_t m, const InRec *__restrict__ recp,
-                             InRec *__restrict__ rec) {
-  XT_GRID_STRIDE(i, m) rec[i] = recp[int64_t(pos[i])];
 }
 
 // ---------------------------------------------------------------------------
@@ -295,17 +290,23 @@ static xt_status select_flagged(Ctx *c, const uint64_t *in, const uint8_t *flags
   return XT_OK;
 }
 
-// radix sort of (key, value) pairs on the low end_bit bits of 32-bit keys
+// Stable radix sort of (32-bit key, value) pairs on the low end_bit bits,
+// ping-ponging between the caller's two buffers of each (no scratch copies of
+// the data); *k_sorted / *v_sorted say which buffer holds the result.
 template <class V>
-static xt_status sort_pairs32(Ctx *c, const uint32_t *kin, uint32_t *kout, const V *vin, V *vout, int64_t n,
-                              int end_bit) {
+static xt_status sort_pairs_db(Ctx *c, uint32_t *k0, uint32_t *k1, V *v0, V *v1, int64_t n, int end_bit,
+                               uint32_t **k_sorted, V **v_sorted) {
+  cub::DoubleBuffer<uint32_t> dk(k0, k1);
+  cub::DoubleBuffer<V> dv(v0, v1);
   size_t bytes = 0;
-  XT_CUDA(c, cub::DeviceRadixSort::SortPairs(nullptr, bytes, kin, kout, vin, vout, n, 0, end_bit, c->stream));
+  XT_CUDA(c, cub::DeviceRadixSort::SortPairs(nullptr, bytes, dk, dv, n, 0, end_bit, c->stream));
   void *tmp = nullptr;
   XT_TRY(dalloc(c, &tmp, bytes));
-  cudaError_t e = cub::DeviceRadixSort::SortPairs(tmp, bytes, kin, kout, vin, vout, n, 0, end_bit, c->stream);
+  cudaError_t e = cub::DeviceRadixSort::SortPairs(tmp, bytes, dk, dv, n, 0, end_bit, c->stream);
   dfree(c, tmp);
   XT_CUDA(c, e);
+  *k_sorted = dk.Current();
+  *v_sorted = dv.Current();
   return XT_OK;
 }
 
@@ -359,71 +360,80 @@ static xt_status check_err(Ctx *c, const char *what) {
 
 // Degree orientation: ranks the vertices by (deg, id) into g->d_perm
 // (internal -> input id) and relabels n keys (lo << b | hi, input ids) in
-// place to (low rank << b | high rank).
-static xt_status rank_and_relabel(Ctx *c, const int32_t *deg, int64_t nv, int b, uint64_t *keys, int64_t n,
-                                  Graph *g) {
+// place to (low rank << b | high rank). The rank is a stable sort of the
+// ids keyed by degree alone (the ids enter in ascending order, so ties keep
+// id order), on as many key bits as the largest degree needs.
+static xt_status rank_and_relabel(Ctx *c, int32_t *deg, int64_t nv, int b, uint64_t *keys, int64_t n, Graph *g) {
   const int B = 256;
-  uint64_t *vk = nullptr, *vk2 = nullptr;
-  int32_t *o2n = nullptr;
-  xt_status s = dalloc_n(c, &vk, size_t(nv));
-  if (s == XT_OK) s = dalloc_n(c, &vk2, size_t(nv));
+  int32_t *ids = nullptr, *o2n = nullptr, *dalt = nullptr;
+  unsigned int *d_dmax = nullptr;
+  xt_status s = dalloc_n(c, &ids, size_t(nv));
+  if (s == XT_OK) s = dalloc_n(c, &dalt, size_t(nv));
   if (s == XT_OK) s = dalloc_n(c, &o2n, size_t(nv));
   if (s == XT_OK) s = dalloc_n(c, &g->d_perm, size_t(nv));
+  if (s == XT_OK) s = dalloc_n(c, &d_dmax, 1);
+  unsigned int dmax = 0;
+  if (s == XT_OK) s = cuda_status(c, cudaMemsetAsync(d_dmax, 0, sizeof(unsigned int), c->stream), "memset");
   if (s == XT_OK) {
-    k_rank_keys<<<counted(c, grid_for(nv, B, c->sm_count)), B, 0, c->stream>>>(deg, nv, vk);
-    s = sort_keys(c, vk, vk2, nv, 32 + b);
+    k_rank_ids<<<counted(c, grid_for(nv, B, c->sm_count)), B, 0, c->stream>>>(deg, nv, ids, d_dmax);
+    s = cuda_status(c, cudaMemcpyAsync(&dmax, d_dmax, sizeof(unsigned int), cudaMemcpyDeviceToHost, c->stream),
+                    "D2H");
   }
+  if (s == XT_OK) s = cuda_status(c, cudaStreamSynchronize(c->stream), "sync");
+  uint32_t *dk = nullptr;
+  int32_t *perm = nullptr;
   if (s == XT_OK) {
-    k_rank_perm<<<counted(c, grid_for(nv, B, c->sm_count)), B, 0, c->stream>>>(vk2, nv, g->d_perm, o2n);
+    int bits = 1;
+    while (bits < 32 && (uint64_t(1) << bits) <= dmax) bits++;
+    // keys: the degrees (deg is consumed); values: the ids
+    s = sort_pairs_db<int32_t>(c, reinterpret_cast<uint32_t *>(deg), reinterpret_cast<uint32_t *>(dalt), ids,
+                               g->d_perm, nv, bits, &dk, &perm);
+  }
+  if (s == XT_OK && perm != g->d_perm)
+    s = cuda_status(c, cudaMemcpyAsync(g->d_perm, perm, sizeof(int32_t) * nv, cudaMemcpyDeviceToDevice, c->stream),
+                    "perm");
+  if (s == XT_OK) {
+    k_rank_perm<<<counted(c, grid_for(nv, B, c->sm_count)), B, 0, c->stream>>>(g->d_perm, nv, o2n);
     if (n > 0) k_relabel_edges<<<counted(c, grid_for(n, B, c->sm_count)), B, 0, c->stream>>>(keys, n, b, o2n);
     s = cuda_status(c, cudaGetLastError(), "relabel");
   }
-  dfree(c, vk);
-  dfree(c, vk2);
+  dfree(c, ids);
+  dfree(c, dalt);
   dfree(c, o2n);
+  dfree(c, d_dmax);
   return s;
 }
 
 // In-records grouped by head (d_ioff, d_irec), longest suffix first, from the
 // out-CSR. keys: the out-CSR's m sorted keys (row << b | col), read here and
-// then overwritten; spare: a free buffer of at least m 8-byte entries.
-template <class V>
+// then overwritten; spare: a free buffer of at least m 8-byte entries. The
+// 4-byte sort keys of both sides fit in spare; the records are sorted as
+// values between two record arrays, one of which becomes d_irec.
 static xt_status build_in_records(Ctx *c, uint64_t *keys, uint64_t *spare, int64_t m, int64_t nv, int b, Graph *g) {
   const int B = 256;
   const int lb = b + 7 <= 31 ? 7 : 31 - b;  // key = head << lb | class, 31 bits at most
-  // 4-byte values: keys and values of one side fit one 8-byte buffer
-  uint32_t *kin = reinterpret_cast<uint32_t *>(spare), *kout = reinterpret_cast<uint32_t *>(keys);
-  V *vin = nullptr, *vout = nullptr, *own_in = nullptr, *own_out = nullptr;
-  InRec *recp = nullptr;  // in-records in out-position order
-  xt_status s = XT_OK;
-  if (sizeof(V) == 4) {
-    vin = reinterpret_cast<V *>(kin + m);
-    vout = reinterpret_cast<V *>(kout + m);
-  } else {
-    s = dalloc_n(c, &own_in, size_t(m));
-    if (s == XT_OK) s = dalloc_n(c, &own_out, size_t(m));
-    vin = own_in;
-    vout = own_out;
-  }
-  if (s == XT_OK) s = dalloc_n(c, &recp, size_t(m));
+  uint32_t *kin = reinterpret_cast<uint32_t *>(spare), *kalt = kin + m;
+  InRec *r0 = nullptr, *r1 = nullptr;
+  xt_status s = dalloc_n(c, &r0, size_t(m));
+  if (s == XT_OK) s = dalloc_n(c, &r1, size_t(m));
   if (s == XT_OK) {
     // the sorted keys still hold each position's row and column
-    k_in_keys<V><<<counted(c, grid_for(m, B, c->sm_count)), B, 0, c->stream>>>(keys, b, g->d_off, g->d_poff, m, lb,
-                                                                               kin, vin, recp);
+    k_in_keys<<<counted(c, grid_for(m, B, c->sm_count)), B, 0, c->stream>>>(keys, b, g->d_off, g->d_poff, m, lb,
+                                                                            kin, r0);
     s = cuda_status(c, cudaGetLastError(), "in-keys");
   }
   // stable: records of one (head, class) stay in position order
-  if (s == XT_OK) s = sort_pairs32<V>(c, kin, kout, vin, vout, m, b + lb);
-  if (s == XT_OK) s = keys_to_csr<uint32_t>(c, kout, m, nv, lb, g->d_ioff, nullptr);
-  // the records' own array comes after the sort, when its scratch is free
-  if (s == XT_OK) s = dalloc_n(c, &g->d_irec, size_t(m));
+  uint32_t *ks = nullptr;
+  InRec *rs = nullptr;
+  if (s == XT_OK) s = sort_pairs_db<InRec>(c, kin, kalt, r0, r1, m, b + lb, &ks, &rs);
+  if (s == XT_OK) s = keys_to_csr<uint32_t>(c, ks, m, nv, lb, g->d_ioff, nullptr);
   if (s == XT_OK) {
-    k_in_records<V><<<counted(c, grid_for(m, B, c->sm_count)), B, 0, c->stream>>>(vout, m, recp, g->d_irec);
-    s = cuda_status(c, cudaGetLastError(), "in-records");
+    g->d_irec = rs;
+    dfree(c, rs == r0 ? r1 : r0);
+  } else {
+    dfree(c, r0);
+    dfree(c, r1);
   }
-  dfree(c, recp);
-  dfree(c, own_in);
-  dfree(c, own_out);
   return s;
 }
 
@@ -466,8 +476,7 @@ static xt_status finish_csr(Ctx *c, uint64_t *keys, uint64_t *spare, int64_t m, 
     XT_CUDA(c, cudaMemsetAsync(g->d_ioff, 0, sizeof(int64_t) * (nv + 1), c->stream));
     return XT_OK;
   }
-  if (m < (int64_t(1) << 31)) return build_in_records<uint32_t>(c, keys, spare, m, nv, b, g);
-  return build_in_records<uint64_t>(c, keys, spare, m, nv, b, g);
+  return build_in_records(c, keys, spare, m, nv, b, g);
 }
 
 // Copies the host rows into d_src/d_dst in chunks on the copy stream; the
