@@ -114,6 +114,15 @@ xt_status xt_graph_from_edges(xt_ctx *ctx, int64_t nv, int64_t ne, const int32_t
 /* the same from int32 edge lists already in device memory (not freed) */
 xt_status xt_graph_from_device_edges(xt_ctx *ctx, int64_t nv, int64_t ne, const int32_t *d_src,
                                      const int32_t *d_dst, int orient, xt_graph **out);
+/* Replaces BinaryEdgeList::read (graph.hpp:294-395) followed by the
+ * TriangleCountingSingle constructor: the vite file at path (elem_bytes 8, or
+ * 4 for USE_32_BIT_GRAPH) is streamed through pinned staging buffers to the
+ * device, whose kernels take the tails out of the {tail, weight} records, and
+ * built like xt_graph_from_csr (flags: XT_CSR_CANONICAL or 0). The host never
+ * touches a record. XT_ERR_IO for a file whose size does not match its header
+ * or whose offsets do not start at 0 and end at ne. */
+xt_status xt_graph_from_vite(xt_ctx *ctx, const char *path, int elem_bytes, int flags, int orient,
+                             xt_graph **out);
 xt_status xt_graph_get_info(const xt_graph *g, xt_graph_info *info);
 /* copy the oriented CSR out (host buffers of nv+1 and n_edges entries), in
  * the library's internal numbering: vertices renumbered by orientation rank,
@@ -331,6 +340,21 @@ xt_status xt_gen_chunglu(xt_ctx *ctx, int64_t n, const uint64_t *cdf, int64_t ne
 int64_t xt_chunglu_cdf(int64_t n, double gamma, double mean_deg, double max_deg, uint64_t *cdf);
 /* Erdos-Renyi G(n, ne): uniform ordered pairs */
 xt_status xt_gen_er(xt_ctx *ctx, int64_t n, int64_t ne, uint64_t seed, int32_t *d_src, int32_t *d_dst);
+/* Replaces the loops of GenerateRGG(nv).generate (graph.hpp:745-1364) and
+ * its LCG (utils.hpp:245-430) for the -n path without random edges (-p 0):
+ * the reference's random geometric graph as nprocs strip ranks build it,
+ * generated on the device, bit for bit the edge set of xt_rgg_generate.
+ * radius <= 0 selects the reference's r(n) (graph.hpp:788-791). Writes each
+ * undirected edge once, as (a, b) with a < b, into d_src/d_dst (device
+ * int32 arrays of cap rows) and its count into *n_pairs; with d_src == NULL
+ * only *n_pairs is filled (sizing call). XT_ERR_OVERFLOW when cap is short. */
+xt_status xt_gen_rgg(xt_ctx *ctx, int64_t nv, int nprocs, double radius, int64_t cap, int64_t *n_pairs,
+                     int32_t *d_src, int32_t *d_dst);
+/* The same graph generated and built on the device in one call (the -n path
+ * of main.cpp:90-91 followed by the TriangleCountingSingle constructor); the
+ * library holds every buffer. n_input of its info is the reference's
+ * directed entry count, twice the pairs. */
+xt_status xt_graph_from_rgg(xt_ctx *ctx, int64_t nv, int nprocs, double radius, int orient, xt_graph **out);
 
 /* ---- host-side graph input (no device needed) ------------------------------ */
 

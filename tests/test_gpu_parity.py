@@ -136,6 +136,71 @@ def test_reference_rgg_counts(ctx, n):
         g.free()
 
 
+@pytest.mark.parametrize("elem", [8, 4])
+@pytest.mark.parametrize("name", ["k4", "iso_tail", "k64", "er0", "rmat14", "chunglu14", "amazon0302"])
+def test_vite_file_through_the_device(ctx, tmp_path, name, elem):
+    """xt_graph_from_vite: the reference's vite file streamed to the device and
+    parsed there counts the same as the golden count, canonical or not, and
+    a file whose size or offsets contradict its header is XT_ERR_IO."""
+    off, tails = canon(name)
+    p = str(tmp_path / f"{name}_{elem}.bin")
+    xt.write_vite(p, off, tails, elem)
+    for canonical in (True, False):
+        for orient in ORIENTS:
+            g = ctx.graph_from_vite(p, elem, canonical=canonical, orient=orient)
+            assert g.count() == GOLDEN[name]["triangles"]
+            assert g.info()["n_input"] == len(tails)
+            g.free()
+    raw = open(p, "rb").read()
+    with open(p, "wb") as f:  # one record short of its header
+        f.write(raw[:-2 * elem])
+    with pytest.raises(xt.XtError) as e:
+        ctx.graph_from_vite(p, elem)
+    assert e.value.status == xt.XT_ERR_IO
+    if len(tails) > 1:  # the header and the size agree, but offsets[nv] says fewer records
+        o2 = off.copy()
+        o2[-1] -= 1
+        hdr = np.array([len(off) - 1, len(tails)], np.int64 if elem == 8 else np.int32).tobytes()
+        body = o2.astype(np.int64 if elem == 8 else np.int32).tobytes()
+        with open(p, "wb") as f:
+            f.write(hdr + body + raw[len(hdr) + len(body):])
+        with pytest.raises(xt.XtError) as e:
+            ctx.graph_from_vite(p, elem)
+        assert e.value.status == xt.XT_ERR_IO
+    # the context stays usable
+    g = ctx.graph_from_csr(off, tails, canonical=True)
+    assert g.count() == GOLDEN[name]["triangles"]
+    g.free()
+
+
+@pytest.mark.parametrize("n,nprocs,config_radius", [(1024, 1, False), (4096, 1, False), (16384, 1, False),
+                                                     (65536, 1, False), (65536, 2, False), (65536, 2, True),
+                                                     (65536, 4, True), (1 << 20, 2, True)])
+def test_device_rgg_is_the_reference_graph(ctx, n, nprocs, config_radius):
+    """xt_gen_rgg builds the reference's random geometric graph on the device:
+    its edge set equals the host restatement's (itself pinned to the
+    reference binary's rgg fixtures) edge for edge, and its count equals the
+    golden count where the reference ran it (one rank, the reference's r)."""
+    radius = float(np.sqrt(16.0 / (np.pi * n))) if config_radius else 0.0
+    m, s, d = ctx.gen_rgg(n, nprocs, radius)
+    off_h, tails_h = xt.generate_rgg(n, nprocs, radius)
+    assert 2 * m == len(tails_h)
+    s_np, d_np = s.cpu().numpy().astype(np.int64), d.cpu().numpy().astype(np.int64)
+    assert (s_np < d_np).all()
+    off_d, tails_d = oracle.canon_csr(n, s_np, d_np)
+    assert (off_d == off_h).all() and (tails_d == tails_h).all()
+    g = ctx.graph_from_device_edges(n, m, s, d)
+    t = g.count()
+    g.free()
+    g = ctx.graph_from_rgg(n, nprocs, radius)  # generated and built in one call
+    assert g.count() == t and g.info()["n_input"] == len(tails_h)
+    g.free()
+    if nprocs == 1 and not config_radius:
+        assert t == GOLDEN[f"rgg{n}"]["triangles"]
+    elif n <= 65536:
+        assert t == oracle.count_merge(off_h, tails_h)
+
+
 def test_rgg_two_ranks_and_config_radius(ctx):
     # mpiexec -n 2 graph and the r = sqrt(16/(pi n)) variant: oracle counts
     n = 65536

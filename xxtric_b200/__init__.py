@@ -94,6 +94,9 @@ _proto("xt_graph_capture", _int, _vp)
 _proto("xt_graph_set_tuning", _int, _vp, _i64, _i64, _i64)
 _proto("xt_graph_set_tiers", _int, _vp, _i64, _i64)
 _proto("xt_graph_set_prefetch", _int, _vp, _int)
+_proto("xt_gen_rgg", _int, _vp, _i64, _int, _dbl, _i64, _P(_i64), _vp, _vp)
+_proto("xt_graph_from_vite", _int, _vp, ctypes.c_char_p, _int, _int, _int, _P(_vp))
+_proto("xt_graph_from_rgg", _int, _vp, _i64, _int, _dbl, _int, _P(_vp))
 _proto("xt_graph_debug_cuckoo_iters", _int, _vp, _int)
 _proto("xt_mem_stats", _int, _vp, _P(_i64), _P(_i64), _int)
 _proto("xt_serve_estimate", _i64, _i64, _i64)
@@ -128,7 +131,8 @@ EXPORTED = ["xt_strerror", "xt_last_error", "xt_open", "xt_close", "xt_set_strea
             "xt_mem_stats", "xt_serve_estimate", "xt_serve_open", "xt_serve_submit", "xt_serve_poll",
             "xt_serve_wait", "xt_serve_get_stats", "xt_serve_close", "xt_serve_batches", "xt_tsv_read", "xt_tsv_write",
             "xt_graph_autotune", "xt_batch_spec", "xt_gen_batch", "xt_device_free",
-            "xt_gen_rmat", "xt_gen_chunglu", "xt_chunglu_cdf", "xt_gen_er", "xt_vite_read", "xt_vite_write",
+            "xt_gen_rmat", "xt_gen_chunglu", "xt_chunglu_cdf", "xt_gen_er", "xt_gen_rgg", "xt_graph_from_vite",
+            "xt_graph_from_rgg", "xt_vite_read", "xt_vite_write",
             "xt_rgg_generate"]
 
 
@@ -305,6 +309,21 @@ class Context:
         return live.value, peak.value
 
     # -- graphs --
+    def graph_from_vite(self, path: str, elem_bytes: int = 8, canonical: bool = False,
+                        orient: int = ORIENT_DEGREE) -> "DeviceGraph":
+        """A vite binary file read through the device (xt_graph_from_vite)."""
+        h = _vp()
+        _check(_L.xt_graph_from_vite(self._h, path.encode(), elem_bytes, CSR_CANONICAL if canonical else 0, orient,
+                                     ctypes.byref(h)), "xt_graph_from_vite", self)
+        return DeviceGraph(self, h.value)
+
+    def graph_from_rgg(self, nv: int, nprocs: int = 1, radius: float = 0.0,
+                       orient: int = ORIENT_DEGREE) -> "DeviceGraph":
+        """The reference's random geometric graph generated and built on the device."""
+        h = _vp()
+        _check(_L.xt_graph_from_rgg(self._h, nv, nprocs, radius, orient, ctypes.byref(h)), "xt_graph_from_rgg", self)
+        return DeviceGraph(self, h.value)
+
     def graph_from_csr(self, offsets: np.ndarray, tails: np.ndarray, canonical: bool = False,
                        orient: int = ORIENT_DEGREE) -> "DeviceGraph":
         off = np.ascontiguousarray(offsets, np.int64)
@@ -394,6 +413,20 @@ class Context:
                "xt_gen_chunglu", self)
         if sync:
             self.synchronize()
+
+    def gen_rgg(self, nv: int, nprocs: int = 1, radius: float = 0.0):
+        """The reference's random geometric graph (as nprocs strip ranks build
+        it) generated on the device: (n_pairs, src, dst), int32 torch tensors
+        on this context's device holding each undirected edge once (a < b)."""
+        import torch
+        n = ctypes.c_int64(0)
+        _check(_L.xt_gen_rgg(self._h, nv, nprocs, radius, 0, ctypes.byref(n), None, None), "xt_gen_rgg", self)
+        src = torch.empty(max(1, n.value), dtype=torch.int32, device=f"cuda:{self.device}")
+        dst = torch.empty_like(src)
+        _check(_L.xt_gen_rgg(self._h, nv, nprocs, radius, n.value, ctypes.byref(n), _ptr(src), _ptr(dst)),
+               "xt_gen_rgg", self)
+        self.synchronize()
+        return n.value, src[:n.value], dst[:n.value]
 
     def gen_er(self, n: int, ne: int, seed: int, d_src, d_dst, sync: bool = True) -> None:
         _check(_L.xt_gen_er(self._h, n, ne, seed, _ptr(d_src), _ptr(d_dst)), "xt_gen_er", self)

@@ -24,8 +24,8 @@ BUILD = os.path.join(ROOT, "_build")
 LIB = os.path.join(PKG, "libxtb200.so")
 CLI = os.path.join(PKG, "xtric")
 
-CUDA_SOURCES = ["csrc/capi.cu", "csrc/build.cu", "csrc/count.cu", "csrc/gen.cu", "csrc/count_static.cu",
-                "csrc/batch.cu", "csrc/serve.cu"]
+CUDA_SOURCES = ["csrc/capi.cu", "csrc/build.cu", "csrc/count.cu", "csrc/gen.cu", "csrc/rgg.cu",
+                "csrc/vite.cu", "csrc/count_static.cu", "csrc/batch.cu", "csrc/serve.cu"]
 HOST_SOURCES = ["host/host_io.cpp"]
 CLI_SOURCES = ["host/xtric_main.cpp"]
 HEADERS = ["csrc/xt_internal.cuh", "csrc/xt_rng.cuh", "../include/xtric.h", "host/xtric_host.hpp"]

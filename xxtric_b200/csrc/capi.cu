@@ -16,6 +16,8 @@ xt_status gen_rmat(Ctx *c, int scale, int64_t ne, uint64_t seed, int a16, int b1
 xt_status gen_chunglu(Ctx *c, int64_t n, const uint64_t *cdf, int64_t ne, uint64_t seed, int permute,
                       int32_t *d_src, int32_t *d_dst);
 xt_status gen_er(Ctx *c, int64_t n, int64_t ne, uint64_t seed, int32_t *d_src, int32_t *d_dst);
+xt_status gen_rgg(Ctx *c, int64_t nv, int nprocs, double radius, int64_t cap, int64_t *n_pairs, int32_t *d_src,
+                  int32_t *d_dst);
 
 xt_status set_error(Ctx *c, xt_status s, const std::string &msg) {
   if (c) c->last_error = msg;
@@ -255,6 +257,18 @@ xt_status xt_graph_from_csr(xt_ctx *ctx, int64_t nv, const int64_t *offsets, con
   return s;
 }
 
+xt_status xt_graph_from_vite(xt_ctx *ctx, const char *path, int elem_bytes, int flags, int orient,
+                             xt_graph **out) {
+  if (!ctx || !out || !path) return XT_ERR_INVALID;
+  *out = nullptr;
+  Ctx *c = &ctx->c;
+  cudaSetDevice(c->device);
+  xt_graph *gr = new (std::nothrow) xt_graph();
+  if (!gr) return XT_ERR_OOM;
+  xt_status s = build_from_vite(c, path, elem_bytes, (flags & XT_CSR_CANONICAL) != 0, orient, &gr->g);
+  return finish_build(ctx, gr, s, out);
+}
+
 xt_status xt_graph_get_info(const xt_graph *gr, xt_graph_info *info) {
   if (!gr || !info) return XT_ERR_INVALID;
   const Graph &g = gr->g;
@@ -422,6 +436,40 @@ xt_status xt_gen_er(xt_ctx *ctx, int64_t n, int64_t ne, uint64_t seed, int32_t *
   if (!ctx) return XT_ERR_INVALID;
   cudaSetDevice(ctx->c.device);
   return gen_er(&ctx->c, n, ne, seed, d_src, d_dst);
+}
+
+xt_status xt_gen_rgg(xt_ctx *ctx, int64_t nv, int nprocs, double radius, int64_t cap, int64_t *n_pairs,
+                     int32_t *d_src, int32_t *d_dst) {
+  if (!ctx) return XT_ERR_INVALID;
+  cudaSetDevice(ctx->c.device);
+  return gen_rgg(&ctx->c, nv, nprocs, radius, cap, n_pairs, d_src, d_dst);
+}
+
+xt_status xt_graph_from_rgg(xt_ctx *ctx, int64_t nv, int nprocs, double radius, int orient, xt_graph **out) {
+  if (!ctx || !out) return XT_ERR_INVALID;
+  *out = nullptr;
+  Ctx *c = &ctx->c;
+  cudaSetDevice(c->device);
+  int64_t m = 0;
+  XT_TRY(gen_rgg(c, nv, nprocs, radius, 0, &m, nullptr, nullptr));
+  int32_t *ds = nullptr, *dd = nullptr;
+  XT_TRY(dalloc_n(c, &ds, size_t(m > 0 ? m : 1)));
+  xt_status s = dalloc_n(c, &dd, size_t(m > 0 ? m : 1));
+  if (s == XT_OK && m > 0) s = gen_rgg(c, nv, nprocs, radius, m, &m, ds, dd);
+  xt_graph *gr = nullptr;
+  if (s == XT_OK) {
+    gr = new (std::nothrow) xt_graph();
+    if (!gr) s = XT_ERR_OOM;
+  }
+  if (s == XT_OK) {
+    s = build_from_edges(c, nv, m, ds, dd, orient, &gr->g);
+    if (s == XT_OK) gr->g.n_input = 2 * m;  // the reference's directed entries
+    s = finish_build(ctx, gr, s, out);
+  }
+  dfree(c, ds);
+  dfree(c, dd);
+  cudaStreamSynchronize(c->stream);
+  return s;
 }
 
 int64_t xt_chunglu_cdf(int64_t n, double gamma, double mean_deg, double max_deg, uint64_t *cdf) {

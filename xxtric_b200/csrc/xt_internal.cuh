@@ -145,6 +145,9 @@ xt_status build_from_edges(Ctx *c, int64_t nv, int64_t ne, const int32_t *d_src,
 xt_status build_from_csr(Ctx *c, int64_t nv, const int64_t *d_off, const int64_t *d_tails, bool canonical,
                          int orient, Graph *g);
 void free_graph_device(Graph *g);
+// Reads a vite binary file (8- or 4-byte fields) through pinned staging
+// buffers into a device CSR and builds from it (vite.cu).
+xt_status build_from_vite(Ctx *c, const char *path, int elem_bytes, bool canonical, int orient, Graph *g);
 
 // Builds the disjoint union of ng graphs (host offset tables, device edge
 // rows with graph-local ids) as one graph with a per-vertex group map.
@@ -164,6 +167,10 @@ xt_status count_graph(Graph *g, int64_t *d_global, int64_t *d_pv, int64_t *d_gro
                       int64_t *d_support = nullptr);
 
 }  // namespace xt
+
+// The host set-up of the reference's random geometric graph (host_io.cpp):
+// radius, each strip rank's first LCG value and its strip [lo, lo + range).
+xt_status xt_rgg_setup(int64_t nv, int nprocs, double radius, double *rn, int64_t *x0, double *lo, double *range);
 
 struct xt_ctx {
   xt::Ctx c;

@@ -254,10 +254,19 @@ xt_status xt_tsv_write(const char *path, int64_t ne, const int32_t *src, const i
 // uninitialised when nrande < nprocs (graph.hpp:1108-1113), zero here.
 // Rows are sorted like the reference's (graph.hpp:1306-1341); duplicates that
 // the random step can create are kept, as the reference keeps them.
-xt_status xt_rgg_generate(int64_t nv, int nprocs, double radius, double random_edge_pct, uint64_t seed,
-                          int64_t cap, int64_t *ne, int64_t *offsets, int64_t *tails) {
-  if (!ne || nv <= 0 || nprocs <= 0 || (nprocs & (nprocs - 1)) || nv % nprocs) return XT_ERR_INVALID;
-  if (random_edge_pct < 0.0 || random_edge_pct >= 100.0) return XT_ERR_INVALID;
+}  // extern "C"
+
+// The reference's set-up of its random geometric graph for P strip ranks
+// (the host part of graph.hpp:745-1364 and utils.hpp:245-430): the radius
+// r(n) with PI = 3.14159 (deftypes.hpp:7, graph.hpp:788-791) unless radius >
+// 0 is given; the LCG seed std::seed_seq({1}) (utils.hpp:37-44, 261); each
+// rank's first LCG value, jumped ahead by a hypercube prefix of 2x2 matrix
+// powers computed without modulus in wrapping int64 (utils.hpp:272-348);
+// each rank's strip [lo, lo + range) (utils.hpp:399-421). Shared by the host
+// generator below and the device generator (csrc/rgg.cu).
+xt_status xt_rgg_setup(int64_t nv, int nprocs, double radius, double *rn_out, int64_t *x0, double *lo,
+                       double *range) {
+  if (nv <= 0 || nprocs <= 0 || (nprocs & (nprocs - 1)) || nv % nprocs) return XT_ERR_INVALID;
   const int P = nprocs;
   const int64_t n = nv / P, nl = 2 * n;
   const int64_t MLCG = 2147483647LL;
@@ -270,7 +279,6 @@ xt_status xt_rgg_generate(int64_t nv, int nprocs, double radius, double random_e
     rn = (rc + rt) / double(2.0);
   }
   if (!((1.0 / double(P)) > rn)) return XT_ERR_INVALID;
-
   // LCG jump-ahead prefix, wrapping int64 like the reference's unmodded
   // 2x2 products
   auto mat2 = [](int64_t c[4], const int64_t a[4], const int64_t b[4]) {
@@ -302,18 +310,40 @@ xt_status xt_rgg_generate(int64_t nv, int nprocs, double radius, double random_e
   std::seed_seq seq({1u});
   uint32_t x0w = 0;
   seq.generate(&x0w, &x0w + 1);
-  const int64_t x0 = int64_t(x0w);
+  const int64_t xs = int64_t(x0w);
+  const double rec_np = double(1.0 / double(P));
+  for (int r = 0; r < P; r++) {
+    x0[r] = (r == 0) ? xs : int64_t(uint64_t(xs) * uint64_t(Pf[r][0]) + uint64_t(Pf[r][2])) % MLCG;
+    lo[r] = r * rec_np;
+  }
+  *range = 1.0 / double(P);
+  *rn_out = rn;
+  return XT_OK;
+}
+
+extern "C" {
+
+xt_status xt_rgg_generate(int64_t nv, int nprocs, double radius, double random_edge_pct, uint64_t seed,
+                          int64_t cap, int64_t *ne, int64_t *offsets, int64_t *tails) {
+  if (!ne || nv <= 0 || nprocs <= 0 || (nprocs & (nprocs - 1)) || nv % nprocs) return XT_ERR_INVALID;
+  if (random_edge_pct < 0.0 || random_edge_pct >= 100.0) return XT_ERR_INVALID;
+  const int P = nprocs;
+  const int64_t n = nv / P, nl = 2 * n;
+  const int64_t MLCG = 2147483647LL;
+  double rn = 0, range = 0;
+  std::vector<int64_t> x0s(P);
+  std::vector<double> los(P);
+  if (xt_rgg_setup(nv, P, radius, &rn, x0s.data(), los.data(), &range) != XT_OK) return XT_ERR_INVALID;
   std::vector<double> X(size_t(n) * P), Y(size_t(n) * P);
   {
     std::vector<int64_t> rnum(nl);
     const double mult = 1.0 / double(1.0 + double(MLCG - 1));
-    const double rec_np = double(1.0 / double(P));
     std::vector<double> drand(nl);
     for (int r = 0; r < P; r++) {
-      rnum[0] = (r == 0) ? x0 : int64_t(uint64_t(x0) * uint64_t(Pf[r][0]) + uint64_t(Pf[r][2])) % MLCG;
+      rnum[0] = x0s[r];
       for (int64_t i = 1; i < nl; i++) rnum[i] = (rnum[i - 1] * 16807 + 0) % MLCG;
       for (int64_t i = 0; i < nl; i++) drand[i] = double(double(std::fabs(double(rnum[i]))) * mult);
-      const double lo = r * rec_np, range = 1.0 / double(P);
+      const double lo = los[r];
       for (int64_t i = 0; i < n; i++) {
         X[size_t(r) * n + i] = drand[i];
         Y[size_t(r) * n + i] = lo + double(range * drand[n + i]);

@@ -59,7 +59,8 @@ class Graph {
   int get_owner(GraphElem) const { return 0; }
 
   // the statistics block of graph.hpp:230-264 for one process
-  void print_dist_stats() const {
+  void print_dist_stats() const { print_dist_stats(nv_, ne_); }
+  static void print_dist_stats(GraphElem nv_, GraphElem ne_) {
     const double average = double(ne_), avg_sq = double(ne_) * double(ne_);
     const double var = std::fabs(avg_sq - average * average), stddev = std::sqrt(var);
     std::cout << "\n-------------------------------------------------------\n"
@@ -132,15 +133,22 @@ class GenerateRGG {
 // device count, clear() releases the device memory.
 class TriangleCountingSingle {
  public:
-  explicit TriangleCountingSingle(Graph *g, int orient = XT_ORIENT_DEGREE, int device = 0) : g_(g) {
+  explicit TriangleCountingSingle(Graph *g, int orient = XT_ORIENT_DEGREE, int device = 0) {
     check(xt_open(device, &ctx_), "opening the CUDA device");
-    xt_status s = xt_graph_from_csr(ctx_, g->get_nv(), g->edge_indices_.data(), g->tails_.data(), 0, orient, &dg_);
-    if (s != XT_OK) {
-      std::string msg = std::string("building the device graph: ") + xt_strerror(s) + " (" + xt_last_error(ctx_) + ")";
-      xt_close(ctx_);
-      ctx_ = nullptr;
-      throw Error(s, msg);
-    }
+    built(xt_graph_from_csr(ctx_, g->get_nv(), g->edge_indices_.data(), g->tails_.data(), 0, orient, &dg_));
+  }
+  // A vite file (BinaryEdgeList's format, elem_bytes 8 or 4) streamed to the
+  // device and parsed there: the host holds no copy of the graph.
+  TriangleCountingSingle(const std::string &vite_path, int elem_bytes, int orient = XT_ORIENT_DEGREE,
+                         int device = 0) {
+    check(xt_open(device, &ctx_), "opening the CUDA device");
+    built(xt_graph_from_vite(ctx_, vite_path.c_str(), elem_bytes, 0, orient, &dg_));
+  }
+  // The reference's random geometric graph (no random edges) generated and
+  // built on the device, as nprocs strip ranks make it.
+  TriangleCountingSingle(GraphElem nv, int nprocs, double radius, int orient = XT_ORIENT_DEGREE, int device = 0) {
+    check(xt_open(device, &ctx_), "opening the CUDA device");
+    built(xt_graph_from_rgg(ctx_, nv, nprocs, radius, orient, &dg_));
   }
   ~TriangleCountingSingle() { clear(); }
   TriangleCountingSingle(const TriangleCountingSingle &) = delete;
@@ -153,7 +161,7 @@ class TriangleCountingSingle {
   }
   // per-vertex counts (each triangle credits its three corners)
   GraphElem count(std::vector<GraphElem> &per_vertex) {
-    per_vertex.assign(size_t(g_->get_nv()), 0);
+    per_vertex.assign(size_t(info().nv), 0);
     int64_t t = 0;
     check(xt_count(dg_, &t, per_vertex.data()), "counting", ctx_);
     return t;
@@ -179,7 +187,14 @@ class TriangleCountingSingle {
   }
 
  private:
-  Graph *g_;
+  void built(xt_status s) {
+    if (s != XT_OK) {
+      std::string msg = std::string("building the device graph: ") + xt_strerror(s) + " (" + xt_last_error(ctx_) + ")";
+      xt_close(ctx_);
+      ctx_ = nullptr;
+      throw Error(s, msg);
+    }
+  }
   xt_ctx *ctx_ = nullptr;
   xt_graph *dg_ = nullptr;
 };

@@ -3,7 +3,9 @@
 //   xtric -f graph.bin [-b|-d] [-r n] [-s bufsize]
 //   xtric -n N [-l] [-p pct]
 // -b/-d/-r/-s shape the reference's multi-rank partitioning and buffers and
-// are accepted and ignored with a notice. Extra long options:
+// are accepted and ignored with a notice. The -f file is streamed to the
+// device and parsed there, and the -n graph (without -p random edges) is
+// generated on the device. Extra long options:
 //   --orient id|degree   orientation of the device CSR (default degree)
 //   --nprocs P           strip ranks the -n graph is generated for (default 1)
 //   --radius R           RGG radius instead of the reference's r(n)
@@ -18,6 +20,7 @@
 #include <cstdlib>
 #include <fstream>
 #include <iostream>
+#include <memory>
 #include <string>
 
 #include "xtric_host.hpp"
@@ -110,26 +113,41 @@ void parseCommandLine(int argc, char *const argv[]) {
 
 int main(int argc, char *argv[]) {
   parseCommandLine(argc, argv);
+  // -f and -n without random edges are read or generated on the device (the
+  // host never holds the graph); -n with -p > 0 generates on the host, as
+  // its random edges come from a host RNG
+  const bool on_device = !generateGraph || randomEdgePercent <= 0.0;
+  if (generateGraph && (nprocsRGG <= 0 || (nprocsRGG & (nprocsRGG - 1)))) {
+    std::cout << "Error: random geometric graph generation require power-of-2 #processes." << std::endl;
+    abort_run();
+  }
+  if (generateGraph && !randomNumberLCG)
+    std::cerr << "*Warning*: coordinates are always drawn from the reference's LCG (-l); the reference's "
+                 "std::random_device path is not reproducible."
+              << std::endl;
   Graph *g = nullptr;
+  std::unique_ptr<TriangleCountingSingle> tr;
+  GraphElem nv = 0, ne = 0;
   const double td0 = now();
   try {
-    if (generateGraph) {
-      if (nprocsRGG <= 0 || (nprocsRGG & (nprocsRGG - 1))) {
-        std::cout << "Error: random geometric graph generation require power-of-2 #processes." << std::endl;
-        abort_run();
-      }
-      GenerateRGG gr(nvRGG, nprocsRGG, radius, seed);
-      g = gr.generate(randomNumberLCG, true, randomEdgePercent);
+    if (on_device) {
+      if (generateGraph) tr.reset(new TriangleCountingSingle(nvRGG, nprocsRGG, radius, orient));
+      else tr.reset(new TriangleCountingSingle(inputFileName, elemBytes, orient));
+      const xt_graph_info inf = tr->info();
+      nv = inf.nv;
+      ne = inf.n_input;
     } else {
-      BinaryEdgeList rm(elemBytes);
-      g = rm.read(0, 1, ranksPerNode, inputFileName);
+      GenerateRGG gr(nvRGG, nprocsRGG, radius, seed);
+      g = gr.generate(true, true, randomEdgePercent);
+      nv = g->get_nv();
+      ne = g->get_ne();
     }
   } catch (const Error &e) {
-    std::cout << " Error opening file! " << std::endl;
+    if (!generateGraph) std::cout << " Error opening file! " << std::endl;
     std::cerr << e.what() << std::endl;
     abort_run();
   }
-  g->print_dist_stats();
+  Graph::print_dist_stats(nv, ne);
   const double tdt = now() - td0;
   if (!generateGraph)
     std::cout << "Time to read input file and create distributed graph (secs.): " << tdt << std::endl;
@@ -137,20 +155,20 @@ int main(int argc, char *argv[]) {
     std::cout << "Time to generate distributed graph of " << nvRGG << " vertices (secs.): " << tdt << std::endl;
 
   try {
-    TriangleCountingSingle tr(g, orient);
+    if (!tr) tr.reset(new TriangleCountingSingle(g, orient));
     std::vector<GraphElem> pv;
     const double t0 = now();
-    const GraphElem ntris = perVertexFile.empty() ? tr.count() : tr.count(pv);
+    const GraphElem ntris = perVertexFile.empty() ? tr->count() : tr->count(pv);
     const double t = now() - t0;
     std::cout << "Avg/Min/Max execution time (secs.) for triangle counting on 1 processes: " << t << ", " << t
               << ", " << t << std::endl;
     std::cout << "Number of triangles: " << ntris << std::endl;
-    std::cout << "TEPS: " << double(g->get_ne()) / t << std::endl;
+    std::cout << "TEPS: " << double(ne) / t << std::endl;
     if (!perVertexFile.empty()) {
       std::ofstream f(perVertexFile);
       for (GraphElem c : pv) f << c << "\n";
     }
-    tr.clear();
+    tr->clear();
   } catch (const Error &e) {
     std::cerr << e.what() << std::endl;
     delete g;
