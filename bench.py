@@ -348,14 +348,22 @@ def run_reference_arm(args) -> None:
 # the product arm
 # ---------------------------------------------------------------------------
 
-def time_counts(g, stream, torch, steps: int, per_vertex=None) -> float:
-    """Mean device seconds of one count (CUDA events on the launching stream)."""
+def time_counts(g, stream, torch, steps: int, per_vertex=None, support=None) -> float:
+    """Mean device seconds of one count (CUDA events on the launching stream):
+    the global count, or with per-vertex (per_vertex) or per-edge (support)
+    counts into the given device arrays."""
     d = torch.zeros(1, dtype=torch.int64, device="cuda")
     a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    g.count_async(d, per_vertex)  # warm
+
+    def one():
+        if support is not None:
+            g.count_edges_async(d, support)
+        else:
+            g.count_async(d, per_vertex)
+    one()  # warm
     a.record(stream)
     for _ in range(steps):
-        g.count_async(d, per_vertex)
+        one()
     b.record(stream)
     torch.cuda.synchronize()
     return a.elapsed_time(b) / 1e3 / steps
@@ -379,10 +387,20 @@ def run_xtric(args) -> None:
     g = ctx.graph_from_device_edges(n, ne, src, dst, xt.ORIENT_DEGREE)
     info = g.info()
     d_count = torch.zeros(1, dtype=torch.int64, device="cuda")
+    # --mode per-vertex / per-edge: the timed step is the count with those
+    # outputs (the kernels k_count<1> / k_count<2>), for profiling them
+    d_pv = torch.zeros(n, dtype=torch.int64, device="cuda") if args.mode == "per-vertex" else None
+    d_sup = torch.zeros(max(1, info["n_edges"]), dtype=torch.int64, device="cuda") if args.mode == "per-edge" else None
+
+    def count_step():
+        if d_sup is not None:
+            g.count_edges_async(d_count, d_sup)
+        else:
+            g.count_async(d_count, d_pv)
 
     counts = []
     for _ in range(args.warmup):
-        g.count_async(d_count)
+        count_step()
         counts.append(int(d_count.item()))
 
     replicas.barrier()
@@ -397,7 +415,7 @@ def run_xtric(args) -> None:
     start.record(stream)
     for k in range(args.steps):
         ev[k][0].record(stream)
-        g.count_async(d_count)
+        count_step()
         ev[k][1].record(stream)
     end.record(stream)
     torch.cuda.synchronize()
@@ -411,7 +429,16 @@ def run_xtric(args) -> None:
         raise RuntimeError(f"count changed between steps: {counts}")
     value, total_edges, t_max = replicas.aggregate(info["n_edges"] * args.steps, t_total)
 
-    extra = {}
+    extra = {"mode": args.mode}
+    del d_pv, d_sup
+    if args.workload == "rmat24" and args.mode == "global" and not args.no_forms:
+        # the per-vertex and per-edge kernels on the same graph
+        pv = torch.zeros(n, dtype=torch.int64, device="cuda")
+        extra["per_vertex_ms"] = 1e3 * time_counts(g, stream, torch, 3, pv)
+        del pv
+        sup = torch.zeros(max(1, info["n_edges"]), dtype=torch.int64, device="cuda")
+        extra["per_edge_ms"] = 1e3 * time_counts(g, stream, torch, 3, support=sup)
+        del sup
     if args.workload == "chunglu":
         # the per-vertex kernel and the reference's id orientation on the same graph
         pv = torch.zeros(n, dtype=torch.int64, device="cuda")
@@ -522,10 +549,13 @@ def roofline_fields(args, info: dict, t_kernel: float) -> dict:
     peaks = measured_peaks()
     peak = peaks["hbm_gbs"]
     name = {"rmat24": "k_count_rmat_s24.md", "chunglu": "k_count_chunglu.md"}.get(args.workload)
+    if getattr(args, "mode", "global") != "global":
+        name = None  # the committed DRAM capture is the global count's
     dram = profiled_value(name, "dram_bytes_per_launch_full_size") if name and args.scale == SCALE else None
     logical = info["alg_bytes"] / t_kernel / 1e9
     r = {"bound": "hbm", "peak": peak, "unit": "GB/s", "peak_source": peaks["source"],
-         "kernel": "k_count<0>", "kernel_ms": 1e3 * t_kernel}
+         "kernel": {"global": "k_count<0>", "per-vertex": "k_count<1>",
+                    "per-edge": "k_count<2>"}[getattr(args, "mode", "global")], "kernel_ms": 1e3 * t_kernel}
     if dram:
         a = dram / t_kernel / 1e9
         r.update({"achieved": a, "frac": a / peak, "traffic": int(dram),
@@ -941,6 +971,9 @@ def main() -> None:
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-forms", action="store_true",
                     help="leave the batching and serving summaries out of the default line")
+    ap.add_argument("--mode", choices=["global", "per-vertex", "per-edge"], default="global",
+                    help="the count the timed step runs: the global count (the headline), or with per-vertex or "
+                         "per-edge counts into device memory")
     ap.add_argument("--no-e2e", action="store_true",
                     help="skip the end-to-end leg (profiler captures of the count kernel)")
     args = ap.parse_args()

@@ -709,7 +709,7 @@ xt_status xt_count_groups(xt_graph *gr, int64_t *total, int64_t *per_group) {
     XT_CUDA(c, cudaMemcpyAsync(per_group, g.d_res + 1, sizeof(int64_t) * g.n_groups, cudaMemcpyDeviceToHost,
                                c->stream));
   XT_CUDA(c, cudaStreamSynchronize(c->stream));
-  return XT_OK;
+  return count_status(c);
 }
 
 int64_t xt_graph_groups(const xt_graph *gr) { return gr ? gr->g.n_groups : -1; }

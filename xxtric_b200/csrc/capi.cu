@@ -352,6 +352,7 @@ xt_status xt_count(xt_graph *gr, int64_t *global, int64_t *per_vertex) {
                     "D2H");
   dfree(c, d);
   if (s == XT_OK) s = cuda_status(c, cudaStreamSynchronize(c->stream), "count");
+  if (s == XT_OK) s = count_status(c);
   return s;
 }
 
@@ -370,6 +371,7 @@ xt_status xt_count_edges(xt_graph *gr, int64_t *global, int64_t *support) {
                     "D2H");
   dfree(c, d);
   if (s == XT_OK) s = cuda_status(c, cudaStreamSynchronize(c->stream), "count");
+  if (s == XT_OK) s = count_status(c);
   return s;
 }
 

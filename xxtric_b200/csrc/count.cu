@@ -97,6 +97,8 @@ struct PlanParams {
 #define XT_LANE_LOOP 0
 #endif
 constexpr bool kWarpCuckoo = XT_WARP_CUCKOO != 0;
+// bit of the context's error word set when a bounded staging wait gave up
+constexpr int kErrStageTimeout = 8;
 constexpr int32_t kEmpty = -1;
 
 // A warp or CTA task: the in-records [k0, k0 + nrec) of head v streamed
@@ -740,6 +742,7 @@ struct CountArgs {
   unsigned long long *group_out;  // per-group counts when group != null
   int64_t bitmap_bits;            // largest member id range kept as a bitmap
   int cuckoo_iters;               // cuckoo eviction chain limit
+  int *err;                       // error word: kErrStageTimeout when a staging wait gave up
 };
 
 // adds a warp's hits of one task to the task head's group
@@ -754,6 +757,48 @@ __device__ __forceinline__ void cp_async16(void *smem_dst, const void *gsrc) {
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
+// CTA-task staging by one bulk copy (global -> this CTA's shared memory, no
+// multicast) completed on an mbarrier that counts its bytes.
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t *bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
+  uint32_t done;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+      : "=r"(done)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return done != 0;
+}
+// waits for phase `parity` of the barrier, at most kStageWaitLimit tries
+constexpr uint32_t kStageWaitLimit = 1u << 22;
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity) {
+  for (uint32_t it = 0; it < kStageWaitLimit; it++)
+    if (mbar_try_wait(bar, parity)) return true;
+  return false;
+}
+__device__ __forceinline__ void bulk_copy_g2s(void *dst, const void *src, uint32_t bytes, uint64_t *bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                   smem_u32(dst)),
+               "l"(src), "r"(bytes), "r"(smem_u32(bar))
+               : "memory");
+}
+// the generic-proxy reads of the staging buffer are ordered before the next
+// bulk copy (async proxy) overwrites it
+__device__ __forceinline__ void fence_proxy_async_smem() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
 
 // Task staging: the next task's descriptor is claimed and its members copied
 // into shared memory (cp.async) and its in-records sent to L2 while the
@@ -793,6 +838,32 @@ __device__ __forceinline__ int stage_task(int32_t *stage, const int32_t *__restr
   return int(t.r0 - a0);
 }
 
+// CTA tasks: one lane copies the task's members into stage with one bulk
+// copy on the barrier (a plain arrival when there is no task, so the phase
+// still completes), and warp 0's lanes send its in-records to L2; returns
+// where the members start in stage
+__device__ __forceinline__ int stage_task_bulk(int32_t *stage, uint64_t *bar, const int32_t *__restrict__ col,
+                                               const InRec *__restrict__ rec, const Task &t, int lane) {
+  if (lane == 0) {
+    if (t.nrec < 0) {
+      mbar_arrive(bar);
+    } else {
+      // from r0 rounded down to 4 columns (the column array is 256-byte
+      // aligned), whole 16-byte chunks: reads stay inside the column padding
+      const int64_t a0 = t.r0 & ~int64_t(3);
+      const uint32_t bytes = uint32_t((t.r0 + t.nmem - a0 + 3) >> 2) * 16u;
+      fence_proxy_async_smem();
+      mbar_arrive_expect_tx(bar, bytes);
+      bulk_copy_g2s(stage, col + a0, bytes, bar);
+    }
+  }
+  if (t.nrec < 0) return 0;
+  const int64_t bytes = int64_t(t.nrec) * int64_t(sizeof(InRec));
+  for (int64_t q = int64_t(lane) << 16; q < bytes; q += int64_t(32) << 16)
+    prefetch_l2(reinterpret_cast<const char *>(rec + t.k0) + q, uint32_t(bytes - q < 65536 ? bytes - q : 65536));
+  return int(t.r0 & 3);
+}
+
 // clears the first nclear words of the member set (thread t of nt)
 template <bool PV>
 __device__ __forceinline__ void clear_members(const Members &m, int nclear, int t, int nt) {
@@ -820,6 +891,7 @@ __global__ void __launch_bounds__(kThreads, MODE == 0 ? kMinBlocks : 3) k_count(
   uint16_t *bidx = reinterpret_cast<uint16_t *>(smem + kBlockWords);
   int32_t *bmcnt = smem + kBlockWords + kBlockWords / 2;
   __shared__ __align__(16) int32_t s_stage[kStageInts];
+  __shared__ __align__(8) uint64_t s_stage_bar;  // completes when a CTA task's members have landed
   __shared__ Task s_task[2];
   __shared__ int s_soff[2];
   __shared__ int s_batch;  // next in-record batch of the current CTA task
@@ -829,18 +901,27 @@ __global__ void __launch_bounds__(kThreads, MODE == 0 ? kMinBlocks : 3) k_count(
   int64_t acc = 0;
 
   // ---- CTA tasks ----
+  if (tid == 0) mbar_init(&s_stage_bar, 1);
+  __syncthreads();
+  uint32_t stage_parity = 0;
   if (warp == 0) {
     const Task t0 = claim_task(&cursor[0], a.bt, a.n_bt, lane);
-    const int so = stage_task(s_stage, col, rec, t0, lane);
+    const int so = stage_task_bulk(s_stage, &s_stage_bar, col, rec, t0, lane);
     if (lane == 0) {
       s_task[0] = t0;
       s_soff[0] = so;
     }
   }
   for (int cur = 0;; cur ^= 1) {
-    if (warp == 0) cp_async_wait_all();
+    // every thread waits for the staged members (bounded: on a timeout the
+    // CTA leaves its task loop and reports it through the error word)
+    const bool landed = mbar_wait_bounded(&s_stage_bar, stage_parity);
+    stage_parity ^= 1u;
     if (tid == 0) s_batch = 0;
-    __syncthreads();
+    if (__syncthreads_or(!landed)) {
+      if (tid == 0 && a.err) atomicOr(a.err, kErrStageTimeout);
+      break;
+    }
     const Task t = s_task[cur];
     if (t.nrec < 0) break;
     const int32_t *mem = s_stage + s_soff[cur];
@@ -873,7 +954,7 @@ __global__ void __launch_bounds__(kThreads, MODE == 0 ? kMinBlocks : 3) k_count(
     }
     if (warp == 0) {  // stage is free again: bring in the next task
       const Task tn = claim_task(&cursor[0], a.bt, a.n_bt, lane);
-      const int so = stage_task(s_stage, col, rec, tn, lane);
+      const int so = stage_task_bulk(s_stage, &s_stage_bar, col, rec, tn, lane);
       if (lane == 0) {
         s_task[cur ^ 1] = tn;
         s_soff[cur ^ 1] = so;
@@ -1248,6 +1329,20 @@ xt_status make_plan(Graph *g) {
   return s;
 }
 
+// After a count has finished on the context stream: XT_ERR_TIMEOUT if a
+// CTA's bounded wait for its staged members gave up (the count is then
+// incomplete), which clears the flag; XT_OK otherwise.
+xt_status count_status(Ctx *c) {
+  int h = 0;
+  XT_CUDA(c, cudaMemcpyAsync(&h, c->d_err, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  XT_CUDA(c, cudaStreamSynchronize(c->stream));
+  if (h & kErrStageTimeout) {
+    XT_CUDA(c, cudaMemsetAsync(c->d_err, 0, sizeof(int), c->stream));
+    return set_error(c, XT_ERR_TIMEOUT, "count: a CTA's wait for its staged member list timed out");
+  }
+  return XT_OK;
+}
+
 __global__ void k_widen(const unsigned int *__restrict__ in, int64_t n, int64_t *__restrict__ out) {
   XT_GRID_STRIDE(i, n) out[i] = int64_t(in[i]);
 }
@@ -1298,6 +1393,7 @@ xt_status count_graph(Graph *g, int64_t *d_global, int64_t *d_pv, int64_t *d_gro
   a.group_out = reinterpret_cast<unsigned long long *>(d_groups);
   a.bitmap_bits = pl->bitmap_bits;
   a.cuckoo_iters = g->cuckoo_iters >= 0 ? g->cuckoo_iters : kCuckooIters;
+  a.err = c->d_err;
   if (g->ne > 0) {
     if (d_support)
       k_count<2, false><<<counted(c, pl->grid_es), kThreads, count_smem_bytes(true), c->stream>>>(a);

@@ -165,6 +165,9 @@ void free_plan(Graph *g);
 // (nullable; not together with d_pv).
 xt_status count_graph(Graph *g, int64_t *d_global, int64_t *d_pv, int64_t *d_groups = nullptr,
                       int64_t *d_support = nullptr);
+// Synchronises the context stream and reports a count whose bounded device
+// wait gave up (XT_ERR_TIMEOUT); the synchronous count calls end with it.
+xt_status count_status(Ctx *c);
 
 }  // namespace xt
 
