@@ -93,6 +93,10 @@ struct PlanParams {
 #ifndef XT_PF_DIST
 #define XT_PF_DIST 0
 #endif
+// per-vertex mode: bitmap hits credited without a branch
+#ifndef XT_PV_PRED
+#define XT_PV_PRED 1
+#endif
 #ifndef XT_LANE_LOOP
 #define XT_LANE_LOOP 0
 #endif
@@ -565,8 +569,38 @@ __device__ __forceinline__ int probe_pair(const int4 a, const int4 b, const Memb
 // the member's index is the word's first index plus the set bits below;
 // hash: the index kept beside its slot) and, per edge, the edge u->w at
 // column position pos
+// the shared-window address of a shared-memory pointer
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+// atomic add of 1 to a shared counter when pred != 0: the instruction is
+// predicated, so lanes that do not add take no branch (the address may be
+// garbage when pred == 0; it is not accessed)
+__device__ __forceinline__ void red_shared_add1_if(uint32_t saddr, uint32_t pred) {
+  asm volatile("{\n .reg .pred q;\n setp.ne.u32 q, %1, 0;\n @q red.shared.add.u32 [%0], 1;\n}" ::"r"(saddr),
+               "r"(pred)
+               : "memory");
+}
+
 template <int MODE, int KIND>
 __device__ __forceinline__ int probe_one(const Members &m, int32_t w, unsigned int *__restrict__ es, int64_t pos) {
+  if (XT_PV_PRED && MODE == 1 && KIND == kKindBitmap) {
+    // per-vertex mode, branch-free: every candidate finds the counter its
+    // member would have (the word's first member index plus the set bits
+    // below; idx of a word without members, or of the guard word, is stale
+    // and then unused) and the increment is predicated on the hit. R-MAT s24
+    // 63.8 -> 60.4 ms; the per-edge mode keeps its branch (its predicated
+    // global increments measured 97.0 -> 98.8 ms)
+    uint32_t i = uint32_t(w >> 5) - m.base;
+    i = i < m.nwords ? i : m.nwords;
+    const uint32_t x = uint32_t(m.words[i]);
+    const uint32_t bit = uint32_t(w) & 31u;
+    const uint32_t hit = (x >> bit) & 1u;
+    const uint32_t k = uint32_t(m.idx[i]) + uint32_t(__popc(x & ((1u << bit) - 1u)));
+    red_shared_add1_if(smem_u32(m.mcnt) + 4u * k, hit);
+    return int(hit);
+  }
   if (KIND == kKindBitmap) {
     uint32_t i = uint32_t(w >> 5) - m.base;
     i = i < m.nwords ? i : m.nwords;
@@ -760,9 +794,6 @@ __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wai
 
 // CTA-task staging by one bulk copy (global -> this CTA's shared memory, no
 // multicast) completed on an mbarrier that counts its bytes.
-__device__ __forceinline__ uint32_t smem_u32(const void *p) {
-  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
-}
 __device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
   asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
 }
