@@ -505,7 +505,7 @@ static std::string tune_key(const Graph *g) {
   };
   char buf[512];
   // the schedule revision keeps timings of an older kernel from being reused
-  snprintf(buf, sizeof buf, "sched7|%s|sm%d|orient%d|nv2^%d|ne2^%d|work2^%d|groups%lld", p.name, p.multiProcessorCount,
+  snprintf(buf, sizeof buf, "sched8|%s|sm%d|orient%d|nv2^%d|ne2^%d|work2^%d|groups%lld", p.name, p.multiProcessorCount,
            g->orient, lg(g->nv), lg(g->ne), lg(g->stream_work), (long long)g->n_groups);
   for (char *q = buf; *q; q++)
     if (*q == ' ') *q = '_';
@@ -548,8 +548,8 @@ xt_status autotune(Graph *g, int reps, const char *cache_path, std::string *repo
   snprintf(buf, sizeof buf, "{\"block_work\": 0, \"warp_work\": 0, \"bitmap_bits\": 0, \"ms\": %.4f}", best_ms);
   rep += buf;
   const std::vector<int64_t> options[3] = {
-      {int64_t(1) << 14, int64_t(1) << 16, int64_t(1) << 18, int64_t(1) << 20},
-      {1024, 4096, 16384},
+      {int64_t(1) << 14, int64_t(1) << 16, int64_t(1) << 17, int64_t(1) << 18, int64_t(1) << 20},
+      {1024, 4096, 8192, 16384},
       {int64_t(1) << 13, int64_t(1) << 16, int64_t(1) << 18}};
   for (int dim = 0; dim < 3; dim++) {
     for (int64_t opt : options[dim]) {

@@ -37,11 +37,15 @@ namespace xt {
 #ifndef XT_THREADS
 #define XT_THREADS 256
 #endif
+// CTA tasks of up to 2^17 candidates, warp tasks of up to 8,192: swept
+// with the cuckoo member sets (R-MAT s24 / s22 / Chung-Lu 27.32 / 4.70 /
+// 7.99 ms against 28.09 / 4.99 / 8.39 at 2^16 and 4,096; 2^18 28.52 ms at
+// s24; 16,384 4.78 ms at s22; 32,768 9.49 ms on Chung-Lu)
 #ifndef XT_BLOCK_WORK_LOG2
-#define XT_BLOCK_WORK_LOG2 16
+#define XT_BLOCK_WORK_LOG2 17
 #endif
 #ifndef XT_WARP_WORK
-#define XT_WARP_WORK 4096
+#define XT_WARP_WORK 8192
 #endif
 constexpr int kThreads = XT_THREADS;
 constexpr int kWarps = kThreads / 32;
@@ -49,9 +53,10 @@ constexpr int kWarps = kThreads / 32;
 #define XT_MIN_BLOCKS 4
 #endif
 // CTAs per SM the register budget is sized for: 4 x 256 threads leave 64
-// registers a thread (no spills). Swept with the task size at R-MAT s24:
-// 3 CTAs/SM with 2^17-candidate tasks 34.2 ms, 4 with 2^17 33.8 ms, 4 with
-// 2^16 32.1 ms, 4 with 2^15 35.1 ms, 5 (spilling) 53.9 ms
+// registers a thread (no spills). Swept with the task size at R-MAT s24
+// (before the cuckoo sets): 3 CTAs/SM with 2^17-candidate tasks 34.2 ms, 4
+// with 2^17 33.8 ms, 4 with 2^16 32.1 ms, 4 with 2^15 35.1 ms, 5 (spilling)
+// 53.9 ms
 constexpr int kMinBlocks = XT_MIN_BLOCKS;
 constexpr int kBlockWords = 8192;  // CTA region: 8192-slot hash or 2^18-bit bitmap
 // warp tasks run after the CTA tasks and split the CTA region among the warps
