@@ -81,6 +81,12 @@ struct PlanParams {
 #ifndef XT_BATCHES_PER_WARP
 #define XT_BATCHES_PER_WARP 4
 #endif
+// graphs of 2^34 or more candidates: more, smaller record batches per CTA
+// task (R-MAT s24 27.26 ms with 4, 26.47 with 5, 26.79 with 6, 27.59 with 8;
+// at 6, s22 and Chung-Lu were 0.5% slower, so smaller graphs keep 4)
+#ifndef XT_BATCHES_PER_WARP_LARGE
+#define XT_BATCHES_PER_WARP_LARGE 5
+#endif
 #ifndef XT_LANE_PAIRS
 #define XT_LANE_PAIRS 2
 #endif
@@ -1265,7 +1271,7 @@ xt_status make_plan(Graph *g) {
     // tail) for throughput: only graphs with plenty of other work use them
     pp.tiny_work = total_work >= (int64_t(1) << 30) ? XT_TINY_WORK : 0;
     if (g->tier_lane_work >= 0) pp.tiny_work = g->tier_lane_work;
-    pp.batches_per_warp = XT_BATCHES_PER_WARP;
+    pp.batches_per_warp = total_work >= (int64_t(1) << 34) ? XT_BATCHES_PER_WARP_LARGE : XT_BATCHES_PER_WARP;
     pp.lane_pairs = XT_LANE_PAIRS;
     pp.warp_work = g->tune_warp_work > 0 ? g->tune_warp_work : kWarpWork;
     if (g->tier_warp_work >= 0) pp.warp_work = g->tier_warp_work;
