@@ -107,3 +107,32 @@ def test_edge_support_consistent_with_vertex_counts():
     at_v = np.zeros(n, np.int64)
     np.add.at(at_v, np.repeat(np.arange(n), np.diff(off)), es)
     assert (at_v == 2 * pv).all()
+
+
+def test_full_size_pins_are_consistent():
+    """The full-size pins (tests/golden/make_golden_large.py): every entry was
+    counted by both oracle counters, its per-vertex counts sum to three times
+    its total, and where the reference's own binary counted it, its printed
+    total agrees: exactly for the single-threaded build, modulo 2^32 (read as
+    a signed 32-bit int) for the OpenMP build, whose total is summed by
+    std::accumulate with an int initial value (xxtric.hpp:147)."""
+    import json
+    import os
+    from conftest import GOLDEN_DIR
+    with open(os.path.join(GOLDEN_DIR, "golden.json")) as f:
+        large = json.load(f)["large"]
+    assert {"rmat24", "rmat22", "rmat22_seed5", "chunglu_full"} <= set(large)
+    for name, f in large.items():
+        assert f["per_vertex_sum"] == 3 * f["triangles"], name
+        assert set(f["counted_by"]) == {"oracle xo_count_merge", "oracle xo_count_xxtric"}, name
+        for key, r in f.items():
+            if not key.startswith("reference_") or not r.get("finished"):
+                continue
+            if r["binary"] == "tric":
+                assert r["triangles"] == f["triangles"], (name, key)
+            else:
+                wrapped = ((f["triangles"] + (1 << 31)) % (1 << 32)) - (1 << 31)
+                assert r["triangles"] == wrapped, (name, key)
+    # the headline: the reference's own serial build gave the same count
+    assert large["rmat24"]["reference_degree_relabelled_serial"]["triangles"] == 10182539214
+    assert large["rmat24"]["triangles"] == 10182539214
