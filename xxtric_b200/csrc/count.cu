@@ -37,15 +37,21 @@ namespace xt {
 #ifndef XT_THREADS
 #define XT_THREADS 256
 #endif
-// CTA tasks of up to 2^17 candidates, warp tasks of up to 8,192: swept
-// with the cuckoo member sets (R-MAT s24 / s22 / Chung-Lu 27.32 / 4.70 /
-// 7.99 ms against 28.09 / 4.99 / 8.39 at 2^16 and 4,096; 2^18 28.52 ms at
-// s24; 16,384 4.78 ms at s22; 32,768 9.49 ms on Chung-Lu)
+// CTA tasks of up to 2^17 candidates, warp tasks of up to 4,096 (8,192 on
+// graphs of 2^34 or more candidates): swept with the cuckoo member sets
+// (R-MAT s24 / s22 / Chung-Lu 27.32 / 4.70 / 7.99 ms at 2^17 and 8,192
+// against 28.09 / 4.99 / 8.39 at 2^16 and 4,096; at 2^17, 4,096 gave 27.69 /
+// 4.72 / 7.97; 2^18 28.52 ms at s24; 32,768 9.49 ms on Chung-Lu). On small
+// graphs the larger warp limit moves heads onto warp tasks, which run last
+// and leave a tail: R-MAT s18 0.195 -> 0.35 ms with 8,192.
 #ifndef XT_BLOCK_WORK_LOG2
 #define XT_BLOCK_WORK_LOG2 17
 #endif
 #ifndef XT_WARP_WORK
-#define XT_WARP_WORK 8192
+#define XT_WARP_WORK 4096
+#endif
+#ifndef XT_WARP_WORK_LARGE
+#define XT_WARP_WORK_LARGE 8192
 #endif
 constexpr int kThreads = XT_THREADS;
 constexpr int kWarps = kThreads / 32;
@@ -1267,13 +1273,16 @@ xt_status make_plan(Graph *g) {
     if ((s = cuda_status(c, cudaStreamSynchronize(c->stream), "sync")) != XT_OK) break;
     PlanParams pp;
     pp.warp_dmax = kWarpDmax;
+    // graphs of 2^34 or more candidates (R-MAT s24 has 2^35.3) take larger
+    // warp tasks and more record batches per warp
+    const bool large = total_work >= (int64_t(1) << 34);
     // lane tasks trade latency (a lane's dependent loads set the kernel's
     // tail) for throughput: only graphs with plenty of other work use them
     pp.tiny_work = total_work >= (int64_t(1) << 30) ? XT_TINY_WORK : 0;
     if (g->tier_lane_work >= 0) pp.tiny_work = g->tier_lane_work;
-    pp.batches_per_warp = total_work >= (int64_t(1) << 34) ? XT_BATCHES_PER_WARP_LARGE : XT_BATCHES_PER_WARP;
+    pp.batches_per_warp = large ? XT_BATCHES_PER_WARP_LARGE : XT_BATCHES_PER_WARP;
     pp.lane_pairs = XT_LANE_PAIRS;
-    pp.warp_work = g->tune_warp_work > 0 ? g->tune_warp_work : kWarpWork;
+    pp.warp_work = g->tune_warp_work > 0 ? g->tune_warp_work : (large ? XT_WARP_WORK_LARGE : kWarpWork);
     if (g->tier_warp_work >= 0) pp.warp_work = g->tier_warp_work;
     if (g->tune_block_work > 0) {
       pp.block_work = g->tune_block_work;
