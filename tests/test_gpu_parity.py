@@ -269,6 +269,49 @@ def test_chunglu_skewed_counts_vs_oracle(ctx, torch_cuda):
         g.free()
 
 
+def test_builder_rows_of_every_tier(ctx):
+    # Rows of 1 to ~70,000 entries, each edge repeated in either direction
+    # one time in five, and self loops: under the id orientation the hub's
+    # row (69,999 entries) takes the device-sort tier, the long random rows
+    # the CTA tier, the rest the warp (K = 1..32) and thread tiers. The
+    # emitted out-CSR must be the oracle's canonical edge set, each row
+    # ascending and above its own id.
+    rng = np.random.default_rng(7)
+    n = 70000
+    src = [np.zeros(n - 1, np.int64)]
+    dst = [np.arange(1, n, dtype=np.int64)]
+    lens = np.exp(rng.uniform(0, np.log(3000), 4000)).astype(np.int64)
+    for i, L in enumerate(lens, start=1):
+        src.append(np.full(L, i, np.int64))
+        dst.append(rng.integers(0, n, L))
+    src.append(rng.integers(0, n, 200000))
+    dst.append(rng.integers(0, n, 200000))
+    s, d = np.concatenate(src), np.concatenate(dst)
+    rep = rng.random(len(s)) < 0.2
+    flip = rng.random(int(rep.sum())) < 0.5
+    rs, rd = s[rep], d[rep]
+    loops = rng.integers(0, n, 1000)
+    s = np.concatenate([s, np.where(flip, rd, rs), loops])
+    d = np.concatenate([d, np.where(flip, rs, rd), loops])
+    off, tails = oracle.canon_csr(n, s, d)
+    rows = np.repeat(np.arange(n, dtype=np.int64), np.diff(off))
+    up = tails > rows
+    expect = rows[up] * n + tails[up]
+    expect_t = oracle.count_merge(off, tails)
+    for orient in ORIENTS:
+        g = ctx.graph_from_edges(n, s.astype(np.int32), d.astype(np.int32), orient)
+        goff, gcol = g.csr()
+        perm = g.perm().astype(np.int64)
+        grow = np.repeat(np.arange(n, dtype=np.int64), np.diff(goff))
+        assert (gcol > grow).all(), orient
+        same = grow[1:] == grow[:-1]
+        assert (np.diff(gcol.astype(np.int64))[same] > 0).all(), orient
+        a, b = perm[grow], perm[gcol.astype(np.int64)]
+        assert np.array_equal(np.sort(np.minimum(a, b) * n + np.maximum(a, b)), expect), orient
+        assert g.count() == expect_t, orient
+        g.free()
+
+
 def test_count_device_reference_layout(ctx, torch_cuda):
     torch = torch_cuda
     off, tails = canon("amazon0302")

@@ -16,6 +16,7 @@
 #include <cub/cub.cuh>
 
 #include <algorithm>
+#include <vector>
 
 #include "xt_internal.cuh"
 
@@ -38,13 +39,14 @@ static unsigned grid_for(int64_t n, int block, int sm_count) {
 #define XT_GRID_STRIDE(i, n) \
   for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < (n); i += int64_t(gridDim.x) * blockDim.x)
 
-// key = (min << b) | max; self loops keep min == max and are dropped later.
-// With deg != null, every non-loop row also counts one for each end: the
-// degree with repeated rows counted again, which orders the vertices as well
-// as the true degree does (any total order gives the same triangle count).
+// (lo[i], hi[i]) = (min, max) of row i's ends; self loops keep lo == hi and
+// are dropped later. With deg != null, every non-loop row also counts one
+// for each end: the degree with repeated rows counted again, which orders
+// the vertices as well as the true degree does (any total order gives the
+// same triangle count).
 __global__ void k_edge_keys(const int32_t *__restrict__ src, const int32_t *__restrict__ dst, int64_t ne,
-                            int64_t nv, int b, uint64_t *__restrict__ keys, int32_t *__restrict__ deg,
-                            int *__restrict__ err) {
+                            int64_t nv, uint32_t *__restrict__ lo, uint32_t *__restrict__ hi,
+                            int32_t *__restrict__ deg, int *__restrict__ err) {
   XT_GRID_STRIDE(i, ne) {
     int64_t s = src[i], d = dst[i];
     if (s < 0 || d < 0 || s >= nv || d >= nv) {
@@ -52,11 +54,12 @@ __global__ void k_edge_keys(const int32_t *__restrict__ src, const int32_t *__re
       s = 0;
       d = 0;
     }
-    uint64_t lo = uint64_t(s < d ? s : d), hi = uint64_t(s < d ? d : s);
-    keys[i] = (lo << b) | hi;
-    if (deg && lo != hi) {
-      atomicAdd(&deg[lo], 1);
-      atomicAdd(&deg[hi], 1);
+    const uint32_t l = uint32_t(s < d ? s : d), h = uint32_t(s < d ? d : s);
+    lo[i] = l;
+    hi[i] = h;
+    if (deg && l != h) {
+      atomicAdd(&deg[l], 1);
+      atomicAdd(&deg[h], 1);
     }
   }
 }
@@ -95,6 +98,303 @@ __global__ void k_relabel_edges(uint64_t *__restrict__ keys, int64_t m, int b, c
     const uint64_t k = keys[i];
     const uint64_t a = uint64_t(o2n[k >> b]), c = uint64_t(o2n[k & mask]);
     keys[i] = a < c ? ((a << b) | c) : ((c << b) | a);
+  }
+}
+
+// (lo, hi) in input ids -> (row, col) = (low rank, high rank), in place
+__global__ void k_relabel_split(uint32_t *__restrict__ lo, uint32_t *__restrict__ hi, int64_t m,
+                                const int32_t *__restrict__ o2n) {
+  XT_GRID_STRIDE(i, m) {
+    const uint32_t a = uint32_t(o2n[lo[i]]), c = uint32_t(o2n[hi[i]]);
+    lo[i] = a < c ? a : c;
+    hi[i] = a < c ? c : a;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Row buckets. After the rows are sorted by their low end alone, bucket r =
+// bk[rstart[r] .. rstart[r + 1]) holds the high ends of row r in input order,
+// repeats and self loops (the value r) included. Each bucket is then sorted
+// and made unique in place by the tier its length L picks: a thread's
+// registers for L <= 16, a warp's registers for L <= 1,024, a CTA's shared
+// memory for L <= 32,768, one device radix sort per row above that. ulen[r]
+// = the row's unique length; its first ulen[r] entries are the row's
+// columns, ascending.
+
+constexpr int kRowThreadMax = 16;
+constexpr int kRowWarpMax = 1024;
+constexpr int kRowCtaMax = 32768;
+constexpr int kRowCtaThreads = 1024;
+constexpr uint32_t kNoCol = 0xffffffffu;  // above every column (columns are below 2^31)
+
+// compare-exchange toward ascending (asc) or descending order
+__device__ __forceinline__ void cmpx(uint32_t &x, uint32_t &y, bool asc) {
+  const uint32_t lo = min(x, y), hi = max(x, y);
+  x = asc ? lo : hi;
+  y = asc ? hi : lo;
+}
+
+// bitonic sorting network over N registers, ascending
+template <int N>
+__device__ __forceinline__ void net_sort(uint32_t (&v)[N]) {
+#pragma unroll
+  for (int size = 2; size <= N; size <<= 1)
+#pragma unroll
+    for (int stride = size >> 1; stride > 0; stride >>= 1)
+#pragma unroll
+      for (int i = 0; i < N; i++)
+        if ((i & stride) == 0) cmpx(v[i], v[i | stride], (i & size) == 0);
+}
+
+// one row of L <= N entries in a thread's registers: sort, drop repeats and
+// the self loop, write back in place
+template <int N>
+__device__ __forceinline__ int64_t thread_row(uint32_t *__restrict__ bk, int64_t a, int L, uint32_t r) {
+  uint32_t v[N];
+#pragma unroll
+  for (int j = 0; j < N; j++) v[j] = j < L ? bk[a + j] : kNoCol;
+  net_sort<N>(v);
+  int64_t q = 0;
+  uint32_t prev = kNoCol;
+#pragma unroll
+  for (int j = 0; j < N; j++) {
+    if (j < L && v[j] != prev && v[j] != r) bk[a + q++] = v[j];
+    prev = v[j];
+  }
+  return q;
+}
+
+// The lists of rows the thread tier passes on: the warp tier by K (entries
+// per lane: 1, 2, 4, 8, 16, 32), the CTA tier and the device tier. List t
+// starts at lists + base[t] and holds cap[t] rows at most (a row of list t
+// has more than kListMin[t] entries, so n / (kListMin[t] + 1) + 1 bound it).
+constexpr int kLists = 8;
+constexpr int64_t kListMin[kLists] = {16, 32, 64, 128, 256, 512, kRowWarpMax, kRowCtaMax};
+struct RowLists {
+  int64_t base[kLists];
+};
+
+__device__ __forceinline__ int row_list(int64_t L) {
+  if (L <= kRowThreadMax) return -1;
+  if (L <= kRowWarpMax) {
+    int t = 0;
+    while (L > (int64_t(32) << t)) t++;
+    return t;  // K = 1 << t
+  }
+  return L <= kRowCtaMax ? 6 : 7;
+}
+
+// Every row with L <= kRowThreadMax, a thread each; longer rows go to their
+// list (warp-aggregated appends; nl[t] counts list t, nl[kLists] takes the
+// longest row of the CTA list). A warp takes 32 consecutive rows.
+__global__ void k_rows_thread(const int64_t *__restrict__ rstart, int64_t nv, uint32_t *__restrict__ bk,
+                              int64_t *__restrict__ ulen, int32_t *__restrict__ lists, RowLists rl,
+                              unsigned long long *__restrict__ nl) {
+  const int lane = threadIdx.x & 31;
+  const int64_t w0 = (blockIdx.x * int64_t(blockDim.x) + threadIdx.x) >> 5;
+  const int64_t nw = (int64_t(gridDim.x) * blockDim.x) >> 5;
+  for (int64_t base = w0 * 32; base < nv; base += nw * 32) {
+    const int64_t r = base + lane;
+    const bool in = r < nv;
+    const int64_t a = in ? rstart[r] : 0, L = in ? rstart[r + 1] - a : 0;
+    if (in && L <= kRowThreadMax) {
+      int64_t q;
+      if (L <= 1) q = (L == 1 && bk[a] != uint32_t(r)) ? 1 : 0;
+      else if (L <= 4) q = thread_row<4>(bk, a, int(L), uint32_t(r));
+      else if (L <= 8) q = thread_row<8>(bk, a, int(L), uint32_t(r));
+      else q = thread_row<16>(bk, a, int(L), uint32_t(r));
+      ulen[r] = q;
+    }
+    const int tier = in ? row_list(L) : -1;
+    const unsigned any = __ballot_sync(0xffffffffu, tier >= 0);
+    if (!any) continue;
+    if (tier == 6) atomicMax(&nl[kLists], (unsigned long long)L);
+#pragma unroll
+    for (int t = 0; t < kLists; t++) {
+      const unsigned m = __ballot_sync(0xffffffffu, tier == t);
+      if (!m) continue;
+      const int leader = __ffs(m) - 1;
+      unsigned long long at = 0;
+      if (lane == leader) at = atomicAdd(&nl[t], (unsigned long long)__popc(m));
+      at = __shfl_sync(0xffffffffu, at, leader);
+      if (tier == t) lists[rl.base[t] + int64_t(at) + __popc(m & ((1u << lane) - 1u))] = int32_t(r);
+    }
+  }
+}
+
+// One row of 32 K entries at most in a warp's registers, striped (entry e =
+// k * 32 + lane in v[k], so loads and stores coalesce): bitonic sort (pairs
+// at distance below 32 across lanes by shuffle, farther ones inside a lane),
+// then the unique entries compacted in place by ballot.
+template <int K>
+__device__ __forceinline__ void warp_row(uint32_t *__restrict__ bk, int64_t a, int L, uint32_t r,
+                                         int64_t *__restrict__ ulen_r, int lane) {
+  uint32_t v[K];
+#pragma unroll
+  for (int k = 0; k < K; k++) v[k] = k * 32 + lane < L ? bk[a + k * 32 + lane] : kNoCol;
+#pragma unroll
+  for (int size = 2; size <= 32 * K; size <<= 1) {
+#pragma unroll
+    for (int stride = size >> 1; stride > 0; stride >>= 1) {
+      if (stride >= 32) {
+        const int ks = stride >> 5;
+#pragma unroll
+        for (int k = 0; k < K; k++)
+          if ((k & ks) == 0) cmpx(v[k], v[k | ks], ((k * 32) & size) == 0);
+      } else {
+        const bool lower = (lane & stride) == 0;
+#pragma unroll
+        for (int k = 0; k < K; k++) {
+          const uint32_t o = __shfl_xor_sync(0xffffffffu, v[k], stride);
+          const bool asc = ((k * 32 + lane) & size) == 0;
+          v[k] = (lower == asc) ? min(v[k], o) : max(v[k], o);
+        }
+      }
+    }
+  }
+  int64_t q = 0;
+  uint32_t last = kNoCol;  // the entry before this k's lane 0
+  const unsigned below = (1u << lane) - 1u;
+#pragma unroll
+  for (int k = 0; k < K; k++) {
+    uint32_t p = __shfl_up_sync(0xffffffffu, v[k], 1);
+    if (lane == 0) p = last;
+    const bool uq = k * 32 + lane < L && v[k] != p && v[k] != r;
+    const unsigned m = __ballot_sync(0xffffffffu, uq);
+    if (uq) bk[a + q + __popc(m & below)] = v[k];
+    q += __popc(m);
+    last = __shfl_sync(0xffffffffu, v[k], 31);
+  }
+  if (lane == 0) *ulen_r = q;
+}
+
+// warp list K: a warp per row
+template <int K>
+__global__ void k_rows_warp(const int32_t *__restrict__ list, const unsigned long long *__restrict__ n,
+                            const int64_t *__restrict__ rstart, uint32_t *__restrict__ bk,
+                            int64_t *__restrict__ ulen) {
+  const int lane = threadIdx.x & 31;
+  const int64_t nw = (int64_t(gridDim.x) * blockDim.x) >> 5;
+  const int64_t cnt = int64_t(*n);
+  for (int64_t i = (blockIdx.x * int64_t(blockDim.x) + threadIdx.x) >> 5; i < cnt; i += nw) {
+    const int32_t r = list[i];
+    const int64_t a = rstart[r];
+    warp_row<K>(bk, a, int(rstart[r + 1] - a), uint32_t(r), &ulen[r], lane);
+  }
+}
+
+// A sorted row of L entries (src) -> its unique entries without the self
+// loop, compacted into dst, which may be src itself: a chunk's entries are
+// all read before the scan's barrier, and an entry moves only down, so no
+// write reaches an entry a later chunk still reads. All kRowCtaThreads
+// threads of the CTA call it; returns the unique length.
+__device__ int64_t cta_unique(const uint32_t *src, int64_t L, uint32_t r, uint32_t *dst) {
+  using Scan = cub::BlockScan<int, kRowCtaThreads>;
+  __shared__ typename Scan::TempStorage ts;
+  int64_t q = 0;
+  for (int64_t c0 = 0; c0 < L; c0 += kRowCtaThreads) {
+    const int64_t e = c0 + threadIdx.x;
+    const uint32_t x = e < L ? src[e] : kNoCol;
+    const uint32_t p = (e > 0 && e < L) ? src[e - 1] : kNoCol;
+    const int uq = (e < L && x != p && x != r) ? 1 : 0;
+    int pos, tot;
+    Scan(ts).ExclusiveSum(uq, pos, tot);
+    if (uq) dst[q + pos] = x;
+    q += tot;
+    __syncthreads();  // ts is reused by the next chunk
+  }
+  return q;
+}
+
+// the CTA list: a CTA per row, bitonic sort in shared memory (the launch
+// gives as many entries as the list's longest row needs, a power of two)
+__global__ void __launch_bounds__(kRowCtaThreads) k_rows_cta(const int32_t *__restrict__ list,
+                                                             const unsigned long long *__restrict__ n,
+                                                             const int64_t *__restrict__ rstart,
+                                                             uint32_t *__restrict__ bk, int64_t *__restrict__ ulen) {
+  extern __shared__ uint32_t srow[];
+  const int64_t cnt = int64_t(*n);
+  for (int64_t i = blockIdx.x; i < cnt; i += gridDim.x) {
+    const int32_t r = list[i];
+    const int64_t a = rstart[r];
+    const int L = int(rstart[r + 1] - a);
+    int N = 2;
+    while (N < L) N <<= 1;
+    for (int e = threadIdx.x; e < N; e += kRowCtaThreads) srow[e] = e < L ? bk[a + e] : kNoCol;
+    __syncthreads();
+    for (int size = 2; size <= N; size <<= 1)
+      for (int stride = size >> 1; stride > 0; stride >>= 1) {
+        for (int j = threadIdx.x; j < N / 2; j += kRowCtaThreads) {
+          const int x = ((j & ~(stride - 1)) << 1) | (j & (stride - 1)), y = x + stride;
+          uint32_t u = srow[x], w = srow[y];
+          cmpx(u, w, (x & size) == 0);
+          srow[x] = u;
+          srow[y] = w;
+        }
+        __syncthreads();
+      }
+    const int64_t q = cta_unique(srow, L, uint32_t(r), bk + a);
+    if (threadIdx.x == 0) ulen[r] = q;
+    __syncthreads();  // srow is refilled by the next row
+  }
+}
+
+// the device list's {row, start, length} into spans (4 fields a row; the
+// host adds the fourth)
+__global__ void k_rows_spans(const int32_t *__restrict__ list, int64_t nd, const int64_t *__restrict__ rstart,
+                             int64_t *__restrict__ spans) {
+  XT_GRID_STRIDE(i, nd) {
+    const int32_t r = list[i];
+    spans[4 * i] = r;
+    spans[4 * i + 1] = rstart[r];
+    spans[4 * i + 2] = rstart[r + 1] - rstart[r];
+  }
+}
+
+// The device list's rows (spans[i] = {row, start, length, offset}, offset =
+// the entries of the rows before it) into one key array, (i << 32 | column),
+// so a single device radix sort orders every row at once; back again after
+// it.
+__global__ void k_rows_gather(const int64_t *__restrict__ spans, int64_t nd, const uint32_t *__restrict__ bk,
+                              uint64_t *__restrict__ keys) {
+  for (int64_t i = blockIdx.x; i < nd; i += gridDim.x) {
+    const int64_t a = spans[4 * i + 1], L = spans[4 * i + 2], o = spans[4 * i + 3];
+    for (int64_t j = threadIdx.x; j < L; j += blockDim.x) keys[o + j] = (uint64_t(i) << 32) | bk[a + j];
+  }
+}
+__global__ void __launch_bounds__(kRowCtaThreads) k_rows_scatter_unique(const int64_t *__restrict__ spans,
+                                                                        int64_t nd, const uint64_t *__restrict__ keys,
+                                                                        uint32_t *bk, int64_t *__restrict__ ulen) {
+  for (int64_t i = blockIdx.x; i < nd; i += gridDim.x) {
+    const int64_t r = spans[4 * i], a = spans[4 * i + 1], L = spans[4 * i + 2], o = spans[4 * i + 3];
+    for (int64_t j = threadIdx.x; j < L; j += blockDim.x) bk[a + j] = uint32_t(keys[o + j]);
+    __syncthreads();
+    const int64_t q = cta_unique(bk + a, L, uint32_t(r), bk + a);
+    if (threadIdx.x == 0) ulen[r] = q;
+  }
+}
+
+// Unique rows -> the out-CSR: a group of G lanes per row copies its ulen
+// columns to col[off[r]..], keys[off[r]..] (row << b | col) and
+// colp[poff[r]..], and fills the rest of its padded span with kPadSentinel.
+template <int G>
+__global__ void k_rows_emit(const int64_t *__restrict__ rstart, const uint32_t *__restrict__ bk, int64_t nv, int b,
+                            const int64_t *__restrict__ off, const int64_t *__restrict__ poff,
+                            int32_t *__restrict__ col, int32_t *__restrict__ colp, uint64_t *__restrict__ keys) {
+  const int t = threadIdx.x & (G - 1);
+  const int64_t groups = int64_t(gridDim.x) * (blockDim.x / G);
+  for (int64_t r = (blockIdx.x * int64_t(blockDim.x) + threadIdx.x) / G; r < nv; r += groups) {
+    const int64_t a = rstart[r], o = off[r], len = off[r + 1] - o, p = poff[r], plen = poff[r + 1] - p;
+    for (int64_t j = t; j < plen; j += G) {
+      if (j < len) {
+        const uint32_t x = bk[a + j];
+        col[o + j] = int32_t(x);
+        colp[p + j] = int32_t(x);
+        keys[o + j] = (uint64_t(r) << b) | x;
+      } else {
+        colp[p + j] = kPadSentinel;
+      }
+    }
   }
 }
 
@@ -359,11 +659,13 @@ static xt_status check_err(Ctx *c, const char *what) {
 }
 
 // Degree orientation: ranks the vertices by (deg, id) into g->d_perm
-// (internal -> input id) and relabels n keys (lo << b | hi, input ids) in
-// place to (low rank << b | high rank). The rank is a stable sort of the
-// ids keyed by degree alone (the ids enter in ascending order, so ties keep
-// id order), on as many key bits as the largest degree needs.
-static xt_status rank_and_relabel(Ctx *c, int32_t *deg, int64_t nv, int b, uint64_t *keys, int64_t n, Graph *g) {
+// (internal -> input id) and relabels n rows in place: packed keys (lo << b
+// | hi, input ids) to (low rank << b | high rank), or, with keys == null,
+// the split ends lo[] / hi[] to (low rank, high rank). The rank is a stable
+// sort of the ids keyed by degree alone (the ids enter in ascending order,
+// so ties keep id order), on as many key bits as the largest degree needs.
+static xt_status rank_and_relabel(Ctx *c, int32_t *deg, int64_t nv, int b, uint64_t *keys, int64_t n, Graph *g,
+                                  uint32_t *lo = nullptr, uint32_t *hi = nullptr) {
   const int B = 256;
   int32_t *ids = nullptr, *o2n = nullptr, *dalt = nullptr;
   unsigned int *d_dmax = nullptr;
@@ -394,7 +696,8 @@ static xt_status rank_and_relabel(Ctx *c, int32_t *deg, int64_t nv, int b, uint6
                     "perm");
   if (s == XT_OK) {
     k_rank_perm<<<counted(c, grid_for(nv, B, c->sm_count)), B, 0, c->stream>>>(g->d_perm, nv, o2n);
-    if (n > 0) k_relabel_edges<<<counted(c, grid_for(n, B, c->sm_count)), B, 0, c->stream>>>(keys, n, b, o2n);
+    if (n > 0 && keys) k_relabel_edges<<<counted(c, grid_for(n, B, c->sm_count)), B, 0, c->stream>>>(keys, n, b, o2n);
+    if (n > 0 && !keys) k_relabel_split<<<counted(c, grid_for(n, B, c->sm_count)), B, 0, c->stream>>>(lo, hi, n, o2n);
     s = cuda_status(c, cudaGetLastError(), "relabel");
   }
   dfree(c, ids);
@@ -479,11 +782,159 @@ static xt_status finish_csr(Ctx *c, uint64_t *keys, uint64_t *spare, int64_t m, 
   return build_in_records(c, keys, spare, m, nv, b, g);
 }
 
+// The out-CSR and the in-records from n rows grouped by their low end:
+// rows_s (the low ends, ascending) and cols_s (the high ends, in any order
+// within a row; repeats and self loops allowed). kbuf: n 8-byte entries
+// disjoint from cols_s, which take the sorted unique keys (row << b | col)
+// the in-records start from. spare: n 8-byte entries (holding cols_s), the
+// in-record sort's scratch once the out-CSR is written.
+static xt_status rows_to_csr(Ctx *c, const uint32_t *rows_s, uint32_t *cols_s, int64_t n, int64_t nv, int b,
+                             uint64_t *kbuf, uint64_t *spare, Graph *g) {
+  const int B = 256;
+  int64_t *rstart = nullptr, *ulen = nullptr, *spans = nullptr;
+  int32_t *lists = nullptr;
+  unsigned long long *nl = nullptr;
+  uint64_t *hk = nullptr;
+  void *tmp = nullptr;
+  xt_status s = XT_OK;
+  do {
+    // bucket bounds: the runs of the sorted low ends
+    if ((s = dalloc_n(c, &rstart, size_t(nv + 1))) != XT_OK) break;
+    if ((s = keys_to_csr<uint32_t>(c, rows_s, n, nv, 0, rstart, nullptr)) != XT_OK) break;
+    if ((s = dalloc_n(c, &ulen, size_t(nv + 1))) != XT_OK) break;
+    RowLists rl;
+    int64_t ltot = 0;
+    for (int t = 0; t < kLists; t++) {
+      rl.base[t] = ltot;
+      ltot += n / (kListMin[t] + 1) + 1;
+    }
+    if ((s = dalloc_n(c, &lists, size_t(ltot))) != XT_OK) break;
+    if ((s = dalloc_n(c, &nl, kLists + 1)) != XT_OK) break;
+    if ((s = cuda_status(c, cudaMemsetAsync(nl, 0, (kLists + 1) * sizeof(*nl), c->stream), "memset")) != XT_OK) break;
+    if ((s = cuda_status(c, cudaMemsetAsync(ulen + nv, 0, sizeof(int64_t), c->stream), "memset")) != XT_OK) break;
+    // each bucket sorted and made unique in place by its tier
+    k_rows_thread<<<counted(c, grid_for(nv, B, c->sm_count)), B, 0, c->stream>>>(rstart, nv, cols_s, ulen, lists, rl,
+                                                                                 nl);
+    if ((s = cuda_status(c, cudaGetLastError(), "row sort")) != XT_OK) break;
+    unsigned long long hn[kLists + 1];
+    if ((s = cuda_status(c, cudaMemcpyAsync(hn, nl, sizeof(hn), cudaMemcpyDeviceToHost, c->stream), "D2H")) != XT_OK)
+      break;
+    if ((s = cuda_status(c, cudaStreamSynchronize(c->stream), "sync")) != XT_OK) break;
+    using WarpFn = void (*)(const int32_t *, const unsigned long long *, const int64_t *, uint32_t *, int64_t *);
+    const WarpFn wfn[6] = {k_rows_warp<1>, k_rows_warp<2>, k_rows_warp<4>,
+                           k_rows_warp<8>, k_rows_warp<16>, k_rows_warp<32>};
+    for (int t = 0; t < 6 && s == XT_OK; t++) {
+      if (!hn[t]) continue;
+      const int64_t blocks = std::min<int64_t>((int64_t(hn[t]) + 7) / 8, int64_t(c->sm_count) * 16);
+      wfn[t]<<<counted(c, dim3(unsigned(blocks))), B, 0, c->stream>>>(lists + rl.base[t], nl + t, rstart, cols_s,
+                                                                      ulen);
+      s = cuda_status(c, cudaGetLastError(), "row sort");
+    }
+    if (s != XT_OK) break;
+    if (hn[6]) {
+      int N = 2;
+      while (uint64_t(N) < hn[kLists]) N <<= 1;
+      const int smem = N * int(sizeof(uint32_t));
+      if ((s = cuda_status(c, cudaFuncSetAttribute(k_rows_cta, cudaFuncAttributeMaxDynamicSharedMemorySize, smem),
+                           "attr")) != XT_OK)
+        break;
+      const int64_t blocks = std::min<int64_t>(int64_t(hn[6]), int64_t(c->sm_count) * 2);
+      k_rows_cta<<<counted(c, dim3(unsigned(blocks))), kRowCtaThreads, smem, c->stream>>>(
+          lists + rl.base[6], nl + 6, rstart, cols_s, ulen);
+      if ((s = cuda_status(c, cudaGetLastError(), "row sort")) != XT_OK) break;
+    }
+    const int64_t nd = int64_t(hn[7]);
+    if (nd > 0) {  // rows above kRowCtaMax entries: one device radix sort of them all
+      std::vector<int64_t> h(4 * nd);
+      if ((s = dalloc_n(c, &spans, size_t(4 * nd))) != XT_OK) break;
+      k_rows_spans<<<counted(c, grid_for(nd, B, c->sm_count)), B, 0, c->stream>>>(lists + rl.base[7], nd, rstart,
+                                                                                 spans);
+      if ((s = cuda_status(c, cudaMemcpyAsync(h.data(), spans, sizeof(int64_t) * 4 * nd, cudaMemcpyDeviceToHost,
+                                              c->stream), "D2H")) != XT_OK)
+        break;
+      if ((s = cuda_status(c, cudaStreamSynchronize(c->stream), "sync")) != XT_OK) break;
+      int64_t H = 0;
+      for (int64_t i = 0; i < nd; i++) {
+        h[4 * i + 3] = H;
+        H += h[4 * i + 2];
+      }
+      if ((s = cuda_status(c, cudaMemcpyAsync(spans, h.data(), sizeof(int64_t) * 4 * nd, cudaMemcpyHostToDevice,
+                                              c->stream), "H2D")) != XT_OK)
+        break;
+      if ((s = dalloc_n(c, &hk, size_t(2 * H))) != XT_OK) break;
+      const unsigned gb = unsigned(std::min<int64_t>(nd, int64_t(c->sm_count) * 4));
+      k_rows_gather<<<counted(c, dim3(gb)), B, 0, c->stream>>>(spans, nd, cols_s, hk);
+      if ((s = cuda_status(c, cudaGetLastError(), "row gather")) != XT_OK) break;
+      int ib = 1;
+      while ((int64_t(1) << ib) < nd) ib++;
+      cub::DoubleBuffer<uint64_t> db(hk, hk + H);
+      size_t bytes = 0;
+      if ((s = cuda_status(c, cub::DeviceRadixSort::SortKeys(nullptr, bytes, db, H, 0, 32 + ib, c->stream),
+                           "row radix sort")) != XT_OK)
+        break;
+      if ((s = dalloc(c, &tmp, bytes)) != XT_OK) break;
+      if ((s = cuda_status(c, cub::DeviceRadixSort::SortKeys(tmp, bytes, db, H, 0, 32 + ib, c->stream),
+                           "row radix sort")) != XT_OK)
+        break;
+      k_rows_scatter_unique<<<counted(c, dim3(gb)), kRowCtaThreads, 0, c->stream>>>(spans, nd, db.Current(), cols_s,
+                                                                                     ulen);
+      if ((s = cuda_status(c, cudaGetLastError(), "row unique")) != XT_OK) break;
+    }
+    // offsets of the unique rows, then the padded offsets
+    if ((s = dalloc_n(c, &g->d_off, size_t(nv + 1))) != XT_OK) break;
+    if ((s = exclusive_scan_i64(c, ulen, g->d_off, nv + 1)) != XT_OK) break;
+    int64_t m = 0;
+    if ((s = cuda_status(c, cudaMemcpyAsync(&m, g->d_off + nv, sizeof(int64_t), cudaMemcpyDeviceToHost, c->stream),
+                         "D2H")) != XT_OK)
+      break;
+    if ((s = cuda_status(c, cudaStreamSynchronize(c->stream), "sync")) != XT_OK) break;
+    g->ne = m;
+    // Columns are read as aligned 32-byte pairs: pad so the last pair of the
+    // last row stays inside the allocation.
+    if ((s = dalloc_n(c, &g->d_col, size_t(m) + kColPad)) != XT_OK) break;
+    if ((s = cuda_status(c, cudaMemsetAsync(g->d_col + m, 0xff, sizeof(int32_t) * kColPad, c->stream), "memset")) !=
+        XT_OK)
+      break;
+    int64_t *plen = ulen;  // the unique lengths live on in d_off
+    if ((s = dalloc_n(c, &g->d_poff, size_t(nv + 1))) != XT_OK) break;
+    k_pad_len<<<counted(c, grid_for(nv, B, c->sm_count)), B, 0, c->stream>>>(g->d_off, nv, plen);
+    if ((s = cuda_status(c, cudaMemsetAsync(plen + nv, 0, sizeof(int64_t), c->stream), "memset")) != XT_OK) break;
+    if ((s = exclusive_scan_i64(c, plen, g->d_poff, nv + 1)) != XT_OK) break;
+    int64_t total = 0;
+    if ((s = cuda_status(c, cudaMemcpyAsync(&total, g->d_poff + nv, sizeof(int64_t), cudaMemcpyDeviceToHost,
+                                            c->stream), "D2H")) != XT_OK)
+      break;
+    if ((s = cuda_status(c, cudaStreamSynchronize(c->stream), "sync")) != XT_OK) break;
+    if ((s = dalloc_n(c, &g->d_colp, size_t(total > 0 ? total : 8))) != XT_OK) break;
+    g->colp_len = total;
+    constexpr int G = 8;
+    k_rows_emit<G><<<counted(c, grid_for(nv * G, B, c->sm_count)), B, 0, c->stream>>>(
+        rstart, cols_s, nv, b, g->d_off, g->d_poff, g->d_col, g->d_colp, kbuf);
+    if ((s = cuda_status(c, cudaGetLastError(), "row emit")) != XT_OK) break;
+    if ((s = dalloc_n(c, &g->d_ioff, size_t(nv + 1))) != XT_OK) break;
+    if (m == 0) {
+      if ((s = dalloc_n(c, &g->d_irec, 1)) != XT_OK) break;
+      s = cuda_status(c, cudaMemsetAsync(g->d_ioff, 0, sizeof(int64_t) * (nv + 1), c->stream), "memset");
+      break;
+    }
+    // the buckets in spare are dead: it becomes the in-record sort's scratch
+    s = build_in_records(c, kbuf, spare, m, nv, b, g);
+  } while (0);
+  dfree(c, rstart);
+  dfree(c, ulen);
+  dfree(c, spans);
+  dfree(c, lists);
+  dfree(c, nl);
+  dfree(c, hk);
+  dfree(c, tmp);
+  return s;
+}
+
 // Copies the host rows into d_src/d_dst in chunks on the copy stream; the
 // context stream turns each chunk into keys (and degree counts) once it has
 // landed.
 static xt_status upload_and_key(Ctx *c, const HostRows &up, int64_t nv, int64_t ne, int32_t *d_src, int32_t *d_dst,
-                                int b, uint64_t *keys, int32_t *deg) {
+                                uint32_t *lo, uint32_t *hi, int32_t *deg) {
   constexpr int kChunks = 8;
   const int B = 256;
   if (!c->copy_stream) XT_CUDA(c, cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking));
@@ -506,8 +957,8 @@ static xt_status upload_and_key(Ctx *c, const HostRows &up, int64_t nv, int64_t 
     if (s == XT_OK) s = cuda_status(c, cudaEventRecord(ev[i], c->copy_stream), "event");
     if (s == XT_OK) s = cuda_status(c, cudaStreamWaitEvent(c->stream, ev[i], 0), "event");
     if (s == XT_OK) {
-      k_edge_keys<<<counted(c, grid_for(n, B, c->sm_count)), B, 0, c->stream>>>(d_src + a, d_dst + a, n, nv, b,
-                                                                               keys + a, deg, c->d_err);
+      k_edge_keys<<<counted(c, grid_for(n, B, c->sm_count)), B, 0, c->stream>>>(d_src + a, d_dst + a, n, nv,
+                                                                               lo + a, hi + a, deg, c->d_err);
       s = cuda_status(c, cudaGetLastError(), "k_edge_keys");
     }
   }
@@ -529,51 +980,47 @@ xt_status build_from_edges(Ctx *c, int64_t nv, int64_t ne, const int32_t *d_src,
   g->orient = orient;
   const int b = bits_for(nv);
   const int B = 256;
+  // k0 = the rows' low ends then their high ends (4 bytes each); k1 = the
+  // same for the sort's other buffers
   uint64_t *k0 = nullptr, *k1 = nullptr;
-  uint8_t *flags = nullptr;
   int32_t *deg = nullptr;
-  int64_t m = 0;
   xt_status s = XT_OK;
   const size_t n1 = size_t(ne > 0 ? ne : 1);
   do {
     if ((s = dalloc_n(c, &k0, n1)) != XT_OK) break;
     if ((s = dalloc_n(c, &k1, n1)) != XT_OK) break;
+    uint32_t *lo = reinterpret_cast<uint32_t *>(k0), *hi = lo + ne;
+    uint32_t *lo2 = reinterpret_cast<uint32_t *>(k1), *hi2 = lo2 + ne;
     if (orient == XT_ORIENT_DEGREE) {
       if ((s = dalloc_n(c, &deg, size_t(nv))) != XT_OK) break;
       if ((s = cuda_status(c, cudaMemsetAsync(deg, 0, sizeof(int32_t) * nv, c->stream), "memset")) != XT_OK) break;
     }
     if (ne > 0) {
       if (upload) {
-        s = upload_and_key(c, *upload, nv, ne, const_cast<int32_t *>(d_src), const_cast<int32_t *>(d_dst), b, k0,
+        s = upload_and_key(c, *upload, nv, ne, const_cast<int32_t *>(d_src), const_cast<int32_t *>(d_dst), lo, hi,
                            deg);
         if (s != XT_OK) break;
       } else {
-        k_edge_keys<<<counted(c, grid_for(ne, B, c->sm_count)), B, 0, c->stream>>>(d_src, d_dst, ne, nv, b, k0,
+        k_edge_keys<<<counted(c, grid_for(ne, B, c->sm_count)), B, 0, c->stream>>>(d_src, d_dst, ne, nv, lo, hi,
                                                                                    deg, c->d_err);
         if ((s = cuda_status(c, cudaGetLastError(), "k_edge_keys")) != XT_OK) break;
       }
       if ((s = check_err(c, "edge list")) != XT_OK) break;
     }
-    // rank, then relabel every row: one sort of the rows in internal ids
+    // rank, then relabel every row in place
     if (orient == XT_ORIENT_DEGREE) {
-      if ((s = rank_and_relabel(c, deg, nv, b, k0, ne, g)) != XT_OK) break;
+      if ((s = rank_and_relabel(c, deg, nv, b, nullptr, ne, g, lo, hi)) != XT_OK) break;
       dfree(c, deg);
       deg = nullptr;
     }
-    if (ne > 0) {
-      if ((s = dalloc_n(c, &flags, n1)) != XT_OK) break;
-      if ((s = sort_keys(c, k0, k1, ne, 2 * b)) != XT_OK) break;
-      k_unique_flags<<<counted(c, grid_for(ne, B, c->sm_count)), B, 0, c->stream>>>(k1, ne, b, flags);
-      if ((s = select_flagged(c, k1, flags, k0, ne, &m)) != XT_OK) break;
-      dfree(c, flags);
-      flags = nullptr;
-    }
-    // k0[0..m) = unique oriented edges, sorted
-    s = finish_csr(c, k0, k1, m, nv, b, g);
+    // rows grouped by their low end: a radix sort on the low end's b bits
+    uint32_t *rows_s = lo, *cols_s = hi;
+    if (ne > 0 && (s = sort_pairs_db<uint32_t>(c, lo, lo2, hi, hi2, ne, b, &rows_s, &cols_s)) != XT_OK) break;
+    const bool in_k0 = cols_s == hi;  // the sorted rows are in k0
+    s = rows_to_csr(c, rows_s, cols_s, ne, nv, b, in_k0 ? k1 : k0, in_k0 ? k0 : k1, g);
   } while (0);
   dfree(c, k0);
   dfree(c, k1);
-  dfree(c, flags);
   dfree(c, deg);
   if (s != XT_OK) free_graph_device(g);
   return s;
