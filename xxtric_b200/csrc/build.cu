@@ -101,10 +101,23 @@ __global__ void k_relabel_edges(uint64_t *__restrict__ keys, int64_t m, int b, c
   }
 }
 
-// (lo, hi) in input ids -> (row, col) = (low rank, high rank), in place
+// (lo, hi) in input ids -> (row, col) = (low rank, high rank), in place.
+// Four rows a thread through 16-byte loads and stores where both arrays
+// are 16-byte aligned (then eight table lookups are in flight at once), one
+// at a time otherwise and for the last m % 4.
 __global__ void k_relabel_split(uint32_t *__restrict__ lo, uint32_t *__restrict__ hi, int64_t m,
                                 const int32_t *__restrict__ o2n) {
-  XT_GRID_STRIDE(i, m) {
+  const bool vec = ((reinterpret_cast<uintptr_t>(lo) | reinterpret_cast<uintptr_t>(hi)) & 15) == 0;
+  const int64_t m4 = vec ? m / 4 : 0;
+  XT_GRID_STRIDE(i, m4) {
+    const uint4 l = reinterpret_cast<const uint4 *>(lo)[i], h = reinterpret_cast<const uint4 *>(hi)[i];
+    const uint32_t a0 = o2n[l.x], a1 = o2n[l.y], a2 = o2n[l.z], a3 = o2n[l.w];
+    const uint32_t c0 = o2n[h.x], c1 = o2n[h.y], c2 = o2n[h.z], c3 = o2n[h.w];
+    reinterpret_cast<uint4 *>(lo)[i] = make_uint4(min(a0, c0), min(a1, c1), min(a2, c2), min(a3, c3));
+    reinterpret_cast<uint4 *>(hi)[i] = make_uint4(max(a0, c0), max(a1, c1), max(a2, c2), max(a3, c3));
+  }
+  XT_GRID_STRIDE(j, m - 4 * m4) {
+    const int64_t i = 4 * m4 + j;
     const uint32_t a = uint32_t(o2n[lo[i]]), c = uint32_t(o2n[hi[i]]);
     lo[i] = a < c ? a : c;
     hi[i] = a < c ? c : a;
@@ -286,13 +299,14 @@ __global__ void k_rows_warp(const int32_t *__restrict__ list, const unsigned lon
 // A sorted row of L entries (src) -> its unique entries without the self
 // loop, compacted into dst, which may be src itself: a chunk's entries are
 // all read before the scan's barrier, and an entry moves only down, so no
-// write reaches an entry a later chunk still reads. All kRowCtaThreads
-// threads of the CTA call it; returns the unique length.
+// write reaches an entry a later chunk still reads. All T threads of the
+// CTA call it; returns the unique length.
+template <int T>
 __device__ int64_t cta_unique(const uint32_t *src, int64_t L, uint32_t r, uint32_t *dst) {
-  using Scan = cub::BlockScan<int, kRowCtaThreads>;
+  using Scan = cub::BlockScan<int, T>;
   __shared__ typename Scan::TempStorage ts;
   int64_t q = 0;
-  for (int64_t c0 = 0; c0 < L; c0 += kRowCtaThreads) {
+  for (int64_t c0 = 0; c0 < L; c0 += T) {
     const int64_t e = c0 + threadIdx.x;
     const uint32_t x = e < L ? src[e] : kNoCol;
     const uint32_t p = (e > 0 && e < L) ? src[e - 1] : kNoCol;
@@ -306,25 +320,88 @@ __device__ int64_t cta_unique(const uint32_t *src, int64_t L, uint32_t r, uint32
   return q;
 }
 
-// the CTA list: a CTA per row, bitonic sort in shared memory (the launch
-// gives as many entries as the list's longest row needs, a power of two)
-__global__ void __launch_bounds__(kRowCtaThreads) k_rows_cta(const int32_t *__restrict__ list,
-                                                             const unsigned long long *__restrict__ n,
-                                                             const int64_t *__restrict__ rstart,
-                                                             uint32_t *__restrict__ bk, int64_t *__restrict__ ulen) {
+// Bitonic stages on a 1,024-entry chunk in a warp's registers, striped
+// (entry k * 32 + lane in v[k]): chunk_presort runs the network's sizes 2 to
+// 512 (directions from the entry's place in the chunk); chunk_merge runs the
+// strides 512 to 1 of one larger size, whose direction (asc) is the same
+// for the whole chunk.
+__device__ __forceinline__ void chunk_presort(uint32_t (&v)[32], int lane) {
+#pragma unroll
+  for (int size = 2; size <= 512; size <<= 1) {
+#pragma unroll
+    for (int stride = size >> 1; stride > 0; stride >>= 1) {
+      if (stride >= 32) {
+        const int ks = stride >> 5;
+#pragma unroll
+        for (int k = 0; k < 32; k++)
+          if ((k & ks) == 0) cmpx(v[k], v[k | ks], ((k * 32) & size) == 0);
+      } else {
+        const bool lower = (lane & stride) == 0;
+#pragma unroll
+        for (int k = 0; k < 32; k++) {
+          const uint32_t o = __shfl_xor_sync(0xffffffffu, v[k], stride);
+          const bool asc = ((k * 32 + lane) & size) == 0;
+          v[k] = (lower == asc) ? min(v[k], o) : max(v[k], o);
+        }
+      }
+    }
+  }
+}
+__device__ __forceinline__ void chunk_merge(uint32_t (&v)[32], int lane, bool asc) {
+#pragma unroll
+  for (int ks = 16; ks > 0; ks >>= 1)
+#pragma unroll
+    for (int k = 0; k < 32; k++)
+      if ((k & ks) == 0) cmpx(v[k], v[k | ks], asc);
+#pragma unroll
+  for (int stride = 16; stride > 0; stride >>= 1) {
+    const bool lower = (lane & stride) == 0;
+#pragma unroll
+    for (int k = 0; k < 32; k++) {
+      const uint32_t o = __shfl_xor_sync(0xffffffffu, v[k], stride);
+      v[k] = (lower == asc) ? min(v[k], o) : max(v[k], o);
+    }
+  }
+}
+
+// The CTA list: a CTA per row, N = the power of two at or above L (2,048 to
+// kRowCtaMax) entries in shared memory (the launch gives as many as the
+// list's longest row needs). Each warp sorts 1,024-entry chunks in
+// registers (the network's sizes up to 1,024); each larger size then runs
+// its strides of 1,024 and up in shared memory and the rest chunk by chunk
+// in registers again.
+constexpr int kCtaSortThreads = 512;
+__global__ void __launch_bounds__(kCtaSortThreads) k_rows_cta(const int32_t *__restrict__ list,
+                                                              const unsigned long long *__restrict__ n,
+                                                              const int64_t *__restrict__ rstart,
+                                                              uint32_t *__restrict__ bk, int64_t *__restrict__ ulen) {
   extern __shared__ uint32_t srow[];
+  constexpr int W = kCtaSortThreads / 32;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int64_t cnt = int64_t(*n);
   for (int64_t i = blockIdx.x; i < cnt; i += gridDim.x) {
     const int32_t r = list[i];
     const int64_t a = rstart[r];
     const int L = int(rstart[r + 1] - a);
-    int N = 2;
+    int N = 2048;
     while (N < L) N <<= 1;
-    for (int e = threadIdx.x; e < N; e += kRowCtaThreads) srow[e] = e < L ? bk[a + e] : kNoCol;
+    const int nc = N >> 10;
+    for (int c = warp; c < nc; c += W) {
+      uint32_t v[32];
+#pragma unroll
+      for (int k = 0; k < 32; k++) {
+        const int e = (c << 10) + k * 32 + lane;
+        v[k] = e < L ? bk[a + e] : kNoCol;
+      }
+      chunk_presort(v, lane);
+      chunk_merge(v, lane, (c & 1) == 0);
+#pragma unroll
+      for (int k = 0; k < 32; k++) srow[(c << 10) + k * 32 + lane] = v[k];
+    }
     __syncthreads();
-    for (int size = 2; size <= N; size <<= 1)
-      for (int stride = size >> 1; stride > 0; stride >>= 1) {
-        for (int j = threadIdx.x; j < N / 2; j += kRowCtaThreads) {
+    for (int size = 2048; size <= N; size <<= 1) {
+      for (int stride = size >> 1; stride >= 1024; stride >>= 1) {
+        for (int j = threadIdx.x; j < N / 2; j += kCtaSortThreads) {
           const int x = ((j & ~(stride - 1)) << 1) | (j & (stride - 1)), y = x + stride;
           uint32_t u = srow[x], w = srow[y];
           cmpx(u, w, (x & size) == 0);
@@ -333,7 +410,17 @@ __global__ void __launch_bounds__(kRowCtaThreads) k_rows_cta(const int32_t *__re
         }
         __syncthreads();
       }
-    const int64_t q = cta_unique(srow, L, uint32_t(r), bk + a);
+      for (int c = warp; c < nc; c += W) {
+        uint32_t v[32];
+#pragma unroll
+        for (int k = 0; k < 32; k++) v[k] = srow[(c << 10) + k * 32 + lane];
+        chunk_merge(v, lane, ((c << 10) & size) == 0);
+#pragma unroll
+        for (int k = 0; k < 32; k++) srow[(c << 10) + k * 32 + lane] = v[k];
+      }
+      __syncthreads();
+    }
+    const int64_t q = cta_unique<kCtaSortThreads>(srow, L, uint32_t(r), bk + a);
     if (threadIdx.x == 0) ulen[r] = q;
     __syncthreads();  // srow is refilled by the next row
   }
@@ -369,30 +456,72 @@ __global__ void __launch_bounds__(kRowCtaThreads) k_rows_scatter_unique(const in
     const int64_t r = spans[4 * i], a = spans[4 * i + 1], L = spans[4 * i + 2], o = spans[4 * i + 3];
     for (int64_t j = threadIdx.x; j < L; j += blockDim.x) bk[a + j] = uint32_t(keys[o + j]);
     __syncthreads();
-    const int64_t q = cta_unique(bk + a, L, uint32_t(r), bk + a);
+    const int64_t q = cta_unique<kRowCtaThreads>(bk + a, L, uint32_t(r), bk + a);
     if (threadIdx.x == 0) ulen[r] = q;
   }
 }
 
-// Unique rows -> the out-CSR: a group of G lanes per row copies its ulen
-// columns to col[off[r]..], keys[off[r]..] (row << b | col) and
-// colp[poff[r]..], and fills the rest of its padded span with kPadSentinel.
-template <int G>
-__global__ void k_rows_emit(const int64_t *__restrict__ rstart, const uint32_t *__restrict__ bk, int64_t nv, int b,
+// Suffix-length class, longest first: 127 - c where c is the length itself
+// below 32 and four classes per octave above, so records of one head sort
+// into runs of similar length.
+__device__ __forceinline__ uint32_t len_class_desc(int64_t len) {
+  uint32_t c;
+  if (len < 32) {
+    c = uint32_t(len);
+  } else {
+    const int lg = 63 - __clzll(len);
+    c = 32u + 4u * uint32_t(lg - 5) + uint32_t((len >> (lg - 2)) & 3);
+  }
+  return 127u - (c < 127u ? c : 127u);
+}
+
+// Unique rows -> the out-CSR and the unsorted in-records. A warp takes 32
+// consecutive rows, whose padded spans are contiguous in colp (and their
+// columns in col): it walks those spans 32 entries at a time, each lane
+// finding its entry's row among the 32 by a binary search over the rows'
+// padded starts, held one per lane, so the writes coalesce however short the
+// rows are. Entry t of row u is column v = bk[rstart[u] + t] while t <
+// ulen[u] (kPadSentinel after it); its out-CSR position p = off[u] + t also
+// gets the in-record of edge u->v (the suffix after t: colp[poff[u] + t + 1,
+// poff[u] + ulen[u])) and its sort key, v << lb | the suffix length's class
+// (lb of its 7 bits, as many as fit beside v in 31 bits).
+__global__ void k_rows_emit(const int64_t *__restrict__ rstart, const uint32_t *__restrict__ bk, int64_t nv, int lb,
                             const int64_t *__restrict__ off, const int64_t *__restrict__ poff,
-                            int32_t *__restrict__ col, int32_t *__restrict__ colp, uint64_t *__restrict__ keys) {
-  const int t = threadIdx.x & (G - 1);
-  const int64_t groups = int64_t(gridDim.x) * (blockDim.x / G);
-  for (int64_t r = (blockIdx.x * int64_t(blockDim.x) + threadIdx.x) / G; r < nv; r += groups) {
-    const int64_t a = rstart[r], o = off[r], len = off[r + 1] - o, p = poff[r], plen = poff[r + 1] - p;
-    for (int64_t j = t; j < plen; j += G) {
-      if (j < len) {
-        const uint32_t x = bk[a + j];
-        col[o + j] = int32_t(x);
-        colp[p + j] = int32_t(x);
-        keys[o + j] = (uint64_t(r) << b) | x;
-      } else {
-        colp[p + j] = kPadSentinel;
+                            int32_t *__restrict__ col, int32_t *__restrict__ colp, uint32_t *__restrict__ ik,
+                            InRec *__restrict__ rec) {
+  const int lane = threadIdx.x & 31;
+  const int64_t w0 = (blockIdx.x * int64_t(blockDim.x) + threadIdx.x) >> 5;
+  const int64_t nw = (int64_t(gridDim.x) * blockDim.x) >> 5;
+  for (int64_t base = w0 * 32; base < nv; base += nw * 32) {
+    const int64_t r = base + lane, rc = r < nv ? r : nv;  // lanes past nv: empty rows at the end
+    const int64_t o = off[rc], len = off[r < nv ? r + 1 : nv] - o, p = poff[rc];
+    const int64_t a = r < nv ? rstart[r] : 0;
+    const int64_t p0 = __shfl_sync(0xffffffffu, p, 0);
+    const int64_t pend = poff[base + 32 < nv ? base + 32 : nv];
+    for (int64_t q0 = p0; q0 < pend; q0 += 32) {
+      const int64_t q = q0 + lane;
+      int j = 0;  // the last row starting at or before q
+#pragma unroll
+      for (int step = 16; step; step >>= 1)
+        if (__shfl_sync(0xffffffffu, p, j + step) <= q) j += step;
+      const int64_t pj = __shfl_sync(0xffffffffu, p, j), lj = __shfl_sync(0xffffffffu, len, j);
+      const int64_t oj = __shfl_sync(0xffffffffu, o, j), aj = __shfl_sync(0xffffffffu, a, j);
+      if (q < pend) {
+        const int64_t t = q - pj;
+        if (t < lj) {
+          const uint32_t x = bk[aj + t];
+          const int64_t sl = lj - t - 1;
+          col[oj + t] = int32_t(x);
+          colp[q] = int32_t(x);
+          ik[oj + t] = (x << lb) | (lb > 0 ? len_class_desc(sl) >> (7 - lb) : 0u);
+          InRec e;
+          e.s = q + 1;
+          e.len = int32_t(sl);
+          e.u = int32_t(base + j);
+          rec[oj + t] = e;
+        } else {
+          colp[q] = kPadSentinel;
+        }
       }
     }
   }
@@ -512,20 +641,6 @@ __global__ void k_pad_fill(const uint64_t *__restrict__ keys, int64_t m, int b, 
     if (i + 1 == off[row + 1])
       for (int64_t t = q + 1, e = poff[row + 1]; t < e; t++) colp[t] = kPadSentinel;
   }
-}
-
-// Suffix-length class, longest first: 127 - c where c is the length itself
-// below 32 and four classes per octave above, so records of one head sort
-// into runs of similar length.
-__device__ __forceinline__ uint32_t len_class_desc(int64_t len) {
-  uint32_t c;
-  if (len < 32) {
-    c = uint32_t(len);
-  } else {
-    const int lg = 63 - __clzll(len);
-    c = 32u + 4u * uint32_t(lg - 5) + uint32_t((len >> (lg - 2)) & 3);
-  }
-  return 127u - (c < 127u ? c : 127u);
 }
 
 // (head << lb | length class) sort key for every out-CSR position, and the
@@ -785,16 +900,16 @@ static xt_status finish_csr(Ctx *c, uint64_t *keys, uint64_t *spare, int64_t m, 
 // The out-CSR and the in-records from n rows grouped by their low end:
 // rows_s (the low ends, ascending) and cols_s (the high ends, in any order
 // within a row; repeats and self loops allowed). kbuf: n 8-byte entries
-// disjoint from cols_s, which take the sorted unique keys (row << b | col)
-// the in-records start from. spare: n 8-byte entries (holding cols_s), the
-// in-record sort's scratch once the out-CSR is written.
+// disjoint from cols_s, which take the in-record sort's keys (both of its
+// buffers).
 static xt_status rows_to_csr(Ctx *c, const uint32_t *rows_s, uint32_t *cols_s, int64_t n, int64_t nv, int b,
-                             uint64_t *kbuf, uint64_t *spare, Graph *g) {
+                             uint64_t *kbuf, Graph *g) {
   const int B = 256;
   int64_t *rstart = nullptr, *ulen = nullptr, *spans = nullptr;
   int32_t *lists = nullptr;
   unsigned long long *nl = nullptr;
   uint64_t *hk = nullptr;
+  InRec *r0 = nullptr, *r1 = nullptr;
   void *tmp = nullptr;
   xt_status s = XT_OK;
   do {
@@ -832,14 +947,14 @@ static xt_status rows_to_csr(Ctx *c, const uint32_t *rows_s, uint32_t *cols_s, i
     }
     if (s != XT_OK) break;
     if (hn[6]) {
-      int N = 2;
+      int N = 2048;
       while (uint64_t(N) < hn[kLists]) N <<= 1;
       const int smem = N * int(sizeof(uint32_t));
       if ((s = cuda_status(c, cudaFuncSetAttribute(k_rows_cta, cudaFuncAttributeMaxDynamicSharedMemorySize, smem),
                            "attr")) != XT_OK)
         break;
-      const int64_t blocks = std::min<int64_t>(int64_t(hn[6]), int64_t(c->sm_count) * 2);
-      k_rows_cta<<<counted(c, dim3(unsigned(blocks))), kRowCtaThreads, smem, c->stream>>>(
+      const int64_t blocks = std::min<int64_t>(int64_t(hn[6]), int64_t(c->sm_count) * 4);
+      k_rows_cta<<<counted(c, dim3(unsigned(blocks))), kCtaSortThreads, smem, c->stream>>>(
           lists + rl.base[6], nl + 6, rstart, cols_s, ulen);
       if ((s = cuda_status(c, cudaGetLastError(), "row sort")) != XT_OK) break;
     }
@@ -907,18 +1022,29 @@ static xt_status rows_to_csr(Ctx *c, const uint32_t *rows_s, uint32_t *cols_s, i
     if ((s = cuda_status(c, cudaStreamSynchronize(c->stream), "sync")) != XT_OK) break;
     if ((s = dalloc_n(c, &g->d_colp, size_t(total > 0 ? total : 8))) != XT_OK) break;
     g->colp_len = total;
-    constexpr int G = 8;
-    k_rows_emit<G><<<counted(c, grid_for(nv * G, B, c->sm_count)), B, 0, c->stream>>>(
-        rstart, cols_s, nv, b, g->d_off, g->d_poff, g->d_col, g->d_colp, kbuf);
-    if ((s = cuda_status(c, cudaGetLastError(), "row emit")) != XT_OK) break;
     if ((s = dalloc_n(c, &g->d_ioff, size_t(nv + 1))) != XT_OK) break;
     if (m == 0) {
       if ((s = dalloc_n(c, &g->d_irec, 1)) != XT_OK) break;
       s = cuda_status(c, cudaMemsetAsync(g->d_ioff, 0, sizeof(int64_t) * (nv + 1), c->stream), "memset");
       break;
     }
-    // the buckets in spare are dead: it becomes the in-record sort's scratch
-    s = build_in_records(c, kbuf, spare, m, nv, b, g);
+    // the out-CSR, with the in-records in position order and their sort keys
+    // (head << lb | class, in kbuf), sorted by head and then class (stable:
+    // records of one (head, class) stay in position order)
+    const int lb = b + 7 <= 31 ? 7 : 31 - b;
+    uint32_t *kin = reinterpret_cast<uint32_t *>(kbuf), *kalt = kin + m;
+    if ((s = dalloc_n(c, &r0, size_t(m))) != XT_OK) break;
+    if ((s = dalloc_n(c, &r1, size_t(m))) != XT_OK) break;
+    k_rows_emit<<<counted(c, grid_for(nv, B, c->sm_count)), B, 0, c->stream>>>(rstart, cols_s, nv, lb, g->d_off,
+                                                                               g->d_poff, g->d_col, g->d_colp, kin, r0);
+    if ((s = cuda_status(c, cudaGetLastError(), "row emit")) != XT_OK) break;
+    uint32_t *ks = nullptr;
+    InRec *rs = nullptr;
+    if ((s = sort_pairs_db<InRec>(c, kin, kalt, r0, r1, m, b + lb, &ks, &rs)) != XT_OK) break;
+    if ((s = keys_to_csr<uint32_t>(c, ks, m, nv, lb, g->d_ioff, nullptr)) != XT_OK) break;
+    g->d_irec = rs;
+    if (rs == r0) r0 = nullptr;
+    else r1 = nullptr;
   } while (0);
   dfree(c, rstart);
   dfree(c, ulen);
@@ -927,6 +1053,8 @@ static xt_status rows_to_csr(Ctx *c, const uint32_t *rows_s, uint32_t *cols_s, i
   dfree(c, nl);
   dfree(c, hk);
   dfree(c, tmp);
+  dfree(c, r0);
+  dfree(c, r1);
   return s;
 }
 
@@ -980,17 +1108,18 @@ xt_status build_from_edges(Ctx *c, int64_t nv, int64_t ne, const int32_t *d_src,
   g->orient = orient;
   const int b = bits_for(nv);
   const int B = 256;
-  // k0 = the rows' low ends then their high ends (4 bytes each); k1 = the
-  // same for the sort's other buffers
+  // k0 = the rows' low ends then, from the next 16-byte boundary, their
+  // high ends (4 bytes each); k1 = the same for the sort's other buffers
   uint64_t *k0 = nullptr, *k1 = nullptr;
   int32_t *deg = nullptr;
   xt_status s = XT_OK;
   const size_t n1 = size_t(ne > 0 ? ne : 1);
+  const int64_t ne4 = (ne + 3) & ~int64_t(3);
   do {
-    if ((s = dalloc_n(c, &k0, n1)) != XT_OK) break;
-    if ((s = dalloc_n(c, &k1, n1)) != XT_OK) break;
-    uint32_t *lo = reinterpret_cast<uint32_t *>(k0), *hi = lo + ne;
-    uint32_t *lo2 = reinterpret_cast<uint32_t *>(k1), *hi2 = lo2 + ne;
+    if ((s = dalloc_n(c, &k0, n1 + 2)) != XT_OK) break;
+    if ((s = dalloc_n(c, &k1, n1 + 2)) != XT_OK) break;
+    uint32_t *lo = reinterpret_cast<uint32_t *>(k0), *hi = lo + ne4;
+    uint32_t *lo2 = reinterpret_cast<uint32_t *>(k1), *hi2 = lo2 + ne4;
     if (orient == XT_ORIENT_DEGREE) {
       if ((s = dalloc_n(c, &deg, size_t(nv))) != XT_OK) break;
       if ((s = cuda_status(c, cudaMemsetAsync(deg, 0, sizeof(int32_t) * nv, c->stream), "memset")) != XT_OK) break;
@@ -1017,7 +1146,7 @@ xt_status build_from_edges(Ctx *c, int64_t nv, int64_t ne, const int32_t *d_src,
     uint32_t *rows_s = lo, *cols_s = hi;
     if (ne > 0 && (s = sort_pairs_db<uint32_t>(c, lo, lo2, hi, hi2, ne, b, &rows_s, &cols_s)) != XT_OK) break;
     const bool in_k0 = cols_s == hi;  // the sorted rows are in k0
-    s = rows_to_csr(c, rows_s, cols_s, ne, nv, b, in_k0 ? k1 : k0, in_k0 ? k0 : k1, g);
+    s = rows_to_csr(c, rows_s, cols_s, ne, nv, b, in_k0 ? k1 : k0, g);
   } while (0);
   dfree(c, k0);
   dfree(c, k1);

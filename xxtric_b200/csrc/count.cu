@@ -28,6 +28,8 @@
 // Inside a task, lanes walk whole suffixes in aligned 32-byte pairs of the
 // padded column array, with no masking (see stream_kind).
 #include <cub/cub.cuh>
+#include <thrust/iterator/counting_iterator.h>
+#include <thrust/iterator/transform_iterator.h>
 
 #include "xt_internal.cuh"
 
@@ -159,9 +161,13 @@ static unsigned grid_for(int64_t n, int block, int sm_count) {
 
 // ---- plan kernels -----------------------------------------------------------
 
-__global__ void k_inrec_work(const InRec *__restrict__ rec, int64_t ne, int64_t *__restrict__ w) {
-  XT_GRID_STRIDE(e, ne) w[e] = rec[e].len;
-}
+// in-record e's candidates (its suffix length), 0 past the last record: the
+// input of the plan's prefix sum, read straight from the records
+struct RecLen {
+  const InRec *rec;
+  int64_t ne;
+  __host__ __device__ int64_t operator()(int64_t e) const { return e < ne ? int64_t(rec[e].len) : 0; }
+};
 
 // Graph statistics in one pass over the vertices: st[0] the largest degree
 // (out + in), st[1] the largest out-degree, st[2] the largest in-degree,
@@ -1234,22 +1240,31 @@ xt_status make_plan(Graph *g) {
   g->plan = pl;
   const int64_t nv = g->nv, ne = g->ne;
   const int B = 256;
-  int64_t *w = nullptr, *P = nullptr, *nb = nullptr, *nw = nullptr, *nt = nullptr, *nbp = nullptr, *nwp = nullptr,
+  int64_t *P = nullptr, *nb = nullptr, *nw = nullptr, *nt = nullptr, *nbp = nullptr, *nwp = nullptr,
           *ntp = nullptr;
   unsigned long long *stats = nullptr;
   xt_status s = XT_OK;
   do {
     if ((s = dalloc_n(c, &pl->d_cursor, 3)) != XT_OK) break;
     if ((s = dalloc_n(c, &stats, 4)) != XT_OK) break;
-    if ((s = dalloc_n(c, &w, size_t(ne + 1))) != XT_OK) break;
     if ((s = dalloc_n(c, &P, size_t(ne + 1))) != XT_OK) break;
     if ((s = cuda_status(c, cudaMemsetAsync(stats, 0, 4 * sizeof(unsigned long long), c->stream), "memset")) !=
         XT_OK)
       break;
     k_vertex_stats<<<counted(c, grid_for(nv, B, c->sm_count)), B, 0, c->stream>>>(g->d_off, g->d_ioff, nv, stats);
     // suffix lengths, prefix-summed in head order
-    k_inrec_work<<<counted(c, grid_for(ne, B, c->sm_count)), B, 0, c->stream>>>(g->d_irec, ne, w);
-    if ((s = exclusive_scan(c, w, P, ne + 1)) != XT_OK) break;
+    {
+      const auto lens = thrust::make_transform_iterator(thrust::counting_iterator<int64_t>(0), RecLen{g->d_irec, ne});
+      size_t bytes = 0;
+      if ((s = cuda_status(c, cub::DeviceScan::ExclusiveSum(nullptr, bytes, lens, P, ne + 1, c->stream), "scan")) !=
+          XT_OK)
+        break;
+      void *tmp = nullptr;
+      if ((s = dalloc(c, &tmp, bytes)) != XT_OK) break;
+      s = cuda_status(c, cub::DeviceScan::ExclusiveSum(tmp, bytes, lens, P, ne + 1, c->stream), "scan");
+      dfree(c, tmp);
+      if (s != XT_OK) break;
+    }
     // persistent grids: every CTA that fits on the device at once
     int occ[3] = {0, 0, 0};
     for (int mode = 0; mode < 3 && s == XT_OK; mode++) {
@@ -1367,7 +1382,6 @@ xt_status make_plan(Graph *g) {
       dfree(c, tmp);
     }
   } while (0);
-  dfree(c, w);
   dfree(c, P);
   dfree(c, nb);
   dfree(c, nw);
