@@ -76,6 +76,8 @@ typedef struct {
   int64_t footprint_bytes; /* bytes of the arrays the count reads, each counted once: offsets and
                               in-record offsets 16(nv+1), columns 4|E+|, padded columns, in-records
                               16|E+|: the DRAM traffic of a count that never re-reads */
+  int64_t cluster_tasks;   /* global count: the tasks of its thread-block cluster tier (see
+                              xt_graph_set_cluster); 0 when no head needs it */
 } xt_graph_info;
 
 /* ---- context ------------------------------------------------------------
@@ -229,6 +231,22 @@ xt_status xt_graph_set_tiers(xt_graph *g, int64_t lane_work, int64_t warp_work);
  * costs issue slots on graphs whose suffixes are; the autotuner tries both.
  * Re-captures a captured graph. */
 xt_status xt_graph_set_prefetch(xt_graph *g, int on);
+/* Global count, cluster tier: with on != 0 a head with more out-neighbours
+ * than one CTA's member set holds (2,048; the id orientation gives hubs
+ * many) is counted by a thread-block cluster of 8 CTAs whose shared
+ * memories hold up to 16,384 of them between them, each candidate looked up
+ * in the table of the CTA whose id range holds it through distributed
+ * shared memory, and the cluster's counts summed there. With 0 (the
+ * default) such a head is counted by CTA tasks over parts of 2,048 members,
+ * each streaming all of its in-records: on the B200 that is the faster of
+ * the two (Chung-Lu n=4.19M under the id orientation: 343 ms against 704 ms
+ * with clusters), because a lookup in another CTA's shared memory costs far
+ * more than the re-streamed candidates it saves. The reference's
+ * counterpart is the cluster kernel of counting.cu:1043-1143
+ * (cluster.map_shared_rank reduction). The per-vertex and per-edge counts
+ * always use the CTA parts. Counts are identical either way. Re-plans (and
+ * re-captures a captured graph). */
+xt_status xt_graph_set_cluster(xt_graph *g, int on);
 /* Test hook, no counterpart in the reference: caps the eviction chain of the
  * global count's cuckoo member sets at `iters` steps (negative: the default
  * of 64). With 0 or 1 nearly every hashed set falls back to linear probing,

@@ -312,6 +312,43 @@ def test_builder_rows_of_every_tier(ctx):
         g.free()
 
 
+def test_cluster_tier_vs_cta_parts(ctx, torch_cuda):
+    # Under the id orientation the hubs of a skewed graph have more
+    # out-neighbours than one CTA's member set holds (2,048): by default
+    # every count runs them as CTA tasks over parts of 2,048 members; with
+    # the cluster tier on, the global count runs them on thread-block
+    # clusters (members spread over 8 CTAs' shared memories, up to 16,384 a
+    # part). Default, on, off, on again, and a captured replay: every count
+    # the oracle's.
+    torch = torch_cuda
+    n = 1 << 17
+    cdf, m = xt.chunglu_cdf(n, 2.1, 32.0, 65536.0)
+    s = torch.empty(m, dtype=torch.int32, device="cuda")
+    d = torch.empty_like(s)
+    ctx.gen_chunglu(cdf, m, 5, s, d)
+    off, tails = oracle.canon_csr(n, s.cpu().numpy().astype(np.int64), d.cpu().numpy().astype(np.int64))
+    expect, opv = oracle.count_merge(off, tails, per_vertex=True)
+    g = ctx.graph_from_device_edges(n, m, s, d, xt.ORIENT_ID)
+    assert g.info()["cluster_tasks"] == 0  # CTA parts by default
+    assert g.count() == expect
+    g.set_cluster(True)
+    inf = g.info()
+    assert inf["max_out_degree"] > 16384, inf  # some hub spans two cluster parts
+    assert inf["cluster_tasks"] > 0, inf
+    assert g.count() == expect
+    t, pv = g.count(per_vertex=True)
+    assert t == expect and (pv == opv).all()
+    g.set_cluster(False)
+    assert g.info()["cluster_tasks"] == 0
+    assert g.count() == expect
+    g.set_cluster(True)
+    assert g.info()["cluster_tasks"] == inf["cluster_tasks"]
+    g.capture()
+    assert g.count() == expect
+    assert g.count() == expect
+    g.free()
+
+
 def test_count_device_reference_layout(ctx, torch_cuda):
     torch = torch_cuda
     off, tails = canon("amazon0302")

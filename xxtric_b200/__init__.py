@@ -50,7 +50,7 @@ class GraphInfo(ctypes.Structure):
     _fields_ = [("nv", _i64), ("n_input", _i64), ("n_edges", _i64), ("max_degree", _i64),
                 ("max_out_degree", _i64), ("max_in_degree", _i64), ("wedge_work", _i64),
                 ("stream_work", _i64), ("alg_bytes", _i64), ("tail_alg_bytes", _i64),
-                ("orient", _i32), ("reserved", _i32), ("footprint_bytes", _i64)]
+                ("orient", _i32), ("reserved", _i32), ("footprint_bytes", _i64), ("cluster_tasks", _i64)]
 
     def as_dict(self) -> dict:
         return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}
@@ -94,6 +94,7 @@ _proto("xt_graph_capture", _int, _vp)
 _proto("xt_graph_set_tuning", _int, _vp, _i64, _i64, _i64)
 _proto("xt_graph_set_tiers", _int, _vp, _i64, _i64)
 _proto("xt_graph_set_prefetch", _int, _vp, _int)
+_proto("xt_graph_set_cluster", _int, _vp, _int)
 _proto("xt_gen_rgg", _int, _vp, _i64, _int, _dbl, _i64, _P(_i64), _vp, _vp)
 _proto("xt_graph_from_vite", _int, _vp, ctypes.c_char_p, _int, _int, _int, _P(_vp))
 _proto("xt_graph_from_rgg", _int, _vp, _i64, _int, _dbl, _int, _P(_vp))
@@ -126,7 +127,7 @@ EXPORTED = ["xt_strerror", "xt_last_error", "xt_open", "xt_close", "xt_set_strea
             "xt_graph_from_csr", "xt_graph_from_edges", "xt_graph_from_device_edges", "xt_graph_get_info",
             "xt_graph_get_csr", "xt_graph_free", "xt_count", "xt_count_async", "xt_count_edges", "xt_count_edges_async", "xt_count_device",
             "xt_count_device_static", "xt_graph_from_batch", "xt_graph_from_device_batch", "xt_graph_groups",
-            "xt_count_groups", "xt_count_groups_async", "xt_batch_count", "xt_graph_capture", "xt_graph_set_tuning", "xt_graph_set_tiers", "xt_graph_set_prefetch",
+            "xt_count_groups", "xt_count_groups_async", "xt_batch_count", "xt_graph_capture", "xt_graph_set_tuning", "xt_graph_set_tiers", "xt_graph_set_prefetch", "xt_graph_set_cluster",
             "xt_graph_debug_cuckoo_iters",
             "xt_mem_stats", "xt_serve_estimate", "xt_serve_open", "xt_serve_submit", "xt_serve_poll",
             "xt_serve_wait", "xt_serve_get_stats", "xt_serve_close", "xt_serve_batches", "xt_tsv_read", "xt_tsv_write",
@@ -537,6 +538,10 @@ class DeviceGraph:
     def set_prefetch(self, on: bool) -> None:
         """Bulk L2 prefetch of each in-record's suffix one batch ahead (global count)."""
         _check(_L.xt_graph_set_prefetch(self._h, int(on)), "xt_graph_set_prefetch", self.ctx)
+
+    def set_cluster(self, on: bool) -> None:
+        """Global count: heads over a CTA's member set on thread-block clusters, or CTA parts (default)."""
+        _check(_L.xt_graph_set_cluster(self._h, int(on)), "xt_graph_set_cluster", self.ctx)
 
     def debug_cuckoo_iters(self, iters: int) -> None:
         """Test hook: cap the cuckoo member sets' eviction chains (-1: default)."""

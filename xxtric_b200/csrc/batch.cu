@@ -456,6 +456,14 @@ xt_status set_prefetch(Graph *g, int on) {
   return XT_OK;
 }
 
+static xt_status set_cluster(Graph *g, int on) {
+  const bool was_captured = g->exec != nullptr;
+  g->cluster_tier = on ? 1 : 0;
+  XT_TRY(make_plan(g));
+  if (was_captured) XT_TRY(capture_count(g));
+  return XT_OK;
+}
+
 xt_status set_tuning(Graph *g, int64_t block_work, int64_t warp_work, int64_t bitmap_bits) {
   const bool was_captured = g->exec != nullptr;
   g->tune_block_work = block_work > 0 ? block_work : 0;
@@ -756,6 +764,12 @@ xt_status xt_graph_set_prefetch(xt_graph *gr, int on) {
   if (!gr || !gr->g.ctx) return XT_ERR_INVALID;
   cudaSetDevice(gr->g.ctx->device);
   return set_prefetch(&gr->g, on);
+}
+
+xt_status xt_graph_set_cluster(xt_graph *gr, int on) {
+  if (!gr || !gr->g.ctx) return XT_ERR_INVALID;
+  cudaSetDevice(gr->g.ctx->device);
+  return set_cluster(&gr->g, on);
 }
 
 xt_status xt_graph_autotune(xt_graph *gr, int reps, const char *cache_path, char *report, int64_t report_len) {

@@ -27,6 +27,7 @@
 // warp tasks, then the lane tasks, each from its own global atomic cursor.
 // Inside a task, lanes walk whole suffixes in aligned 32-byte pairs of the
 // padded column array, with no masking (see stream_kind).
+#include <cooperative_groups.h>
 #include <cub/cub.cuh>
 #include <thrust/iterator/counting_iterator.h>
 #include <thrust/iterator/transform_iterator.h>
@@ -71,9 +72,17 @@ constexpr int kBlockWords = 8192;  // CTA region: 8192-slot hash or 2^18-bit bit
 constexpr int kWarpWords = kBlockWords / kWarps;  // 1024: a 1024-slot hash or a 32K-bit bitmap
 constexpr int kWarpDmax = kWarpWords / 4;         // hash load factor <= 1/4
 constexpr int64_t kWarpWork = XT_WARP_WORK;
-constexpr int kBlockDmax = 2048;
+#ifndef XT_BLOCK_DMAX
+#define XT_BLOCK_DMAX 2048
+#endif
+constexpr int kBlockDmax = XT_BLOCK_DMAX;
 // the warps' member counters share the CTA's
 static_assert(kWarps * kWarpDmax <= kBlockDmax, "warp member counters exceed the CTA's");
+// Cluster tier (global count): a head whose members overflow a CTA's set
+// (more than kBlockDmax, as the id orientation gives hubs) is counted by a
+// cluster of kCluster CTAs holding up to kClusterDmax members per part
+constexpr int kCluster = 8;
+constexpr int kClusterDmax = kCluster * kBlockDmax;
 constexpr int64_t kBlockWorkMin = int64_t(1) << 14;
 constexpr int64_t kBlockWorkMax = int64_t(1) << XT_BLOCK_WORK_LOG2;
 
@@ -142,8 +151,12 @@ struct Plan {
   Task *d_wt = nullptr;
   int64_t n_ttask = 0;         // lane tasks: one head per lane
   int32_t *d_tt = nullptr;
-  unsigned long long *d_cursor = nullptr;  // [0] CTA, [1] warp, [2] lane task cursors
-  int grid_global = 0, grid_pv = 0, grid_es = 0;
+  unsigned long long *d_cursor = nullptr;  // [0] CTA, [1] warp, [2] lane, [3] cluster task cursors
+  int64_t n_ctask = 0;         // cluster tasks (global count)
+  Task *d_ct = nullptr;
+  int64_t n_btask0 = 0;        // the CTA tasks of the other heads, which the global count
+  Task *d_bt0 = nullptr;       //   runs beside the cluster tasks
+  int grid_global = 0, grid_pv = 0, grid_es = 0, grid_cluster = 0;
   int64_t block_work = 0, warp_work = 0;   // the thresholds the plan was made with
   int64_t bitmap_bits = 0;
 };
@@ -332,6 +345,62 @@ __global__ void k_task_gather(const Task *__restrict__ bt, const int32_t *__rest
   XT_GRID_STRIDE(i, n) out[i] = bt[idx[i]];
 }
 
+// Global count, cluster tier: the cluster tasks of head v, for the heads
+// whose CTA tasks would split N+(v) into parts (more than kBlockDmax
+// members): parts of kClusterDmax members x chunks of kCluster * block_work
+// items. Returns how many (0 for every other head).
+__device__ __forceinline__ int64_t cluster_tasks(int64_t v, const int64_t *__restrict__ off,
+                                                 const int64_t *__restrict__ ioff, const int64_t *__restrict__ P,
+                                                 const PlanParams pp, int64_t &parts, int64_t &chunks,
+                                                 int64_t &work) {
+  int64_t nb, nw, nt, bparts, bchunks;
+  classify(v, off, ioff, P, pp, nb, nw, nt, bparts, bchunks, work);
+  parts = chunks = 0;
+  if (nb == 0 || bparts <= 1) return 0;
+  parts = (off[v + 1] - off[v] + kClusterDmax - 1) / kClusterDmax;
+  const int64_t cw = pp.block_work * kCluster;
+  chunks = (work + cw - 1) / cw;
+  return parts * chunks;
+}
+
+__global__ void k_plan_ccount(int64_t nv, const int64_t *__restrict__ off, const int64_t *__restrict__ ioff,
+                              const int64_t *__restrict__ P, const PlanParams pp, int64_t *__restrict__ nc_out) {
+  XT_GRID_STRIDE(v, nv) {
+    int64_t parts, chunks, work;
+    nc_out[v] = cluster_tasks(v, off, ioff, P, pp, parts, chunks, work);
+  }
+}
+
+__global__ void k_plan_cfill(int64_t nv, const int64_t *__restrict__ off, const int64_t *__restrict__ ioff,
+                             const int64_t *__restrict__ P, const PlanParams pp, const int64_t *__restrict__ nc_pos,
+                             Task *__restrict__ ct) {
+  XT_GRID_STRIDE(v, nv) {
+    int64_t parts, chunks, work;
+    const int64_t n = cluster_tasks(v, off, ioff, P, pp, parts, chunks, work);
+    if (!n) continue;
+    const int64_t k0 = ioff[v], k1 = ioff[v + 1], base = P[k0];
+    int64_t t = nc_pos[v], prev = k0;
+    for (int64_t c = 0; c < chunks; c++) {
+      const int64_t kend = (c + 1 == chunks) ? k1 : lower_bound_i64(P, prev, k1, base + (work * (c + 1)) / chunks);
+      if (kend <= prev) continue;
+      const int32_t lg_s = lanes_log2(kend - prev, P[kend] - P[prev], kWarps * kCluster, pp);
+      for (int64_t p = 0; p < parts; p++) {
+        const int64_t r0 = off[v] + p * kClusterDmax;
+        const int64_t r1 = min(off[v + 1], r0 + kClusterDmax);
+        ct[t++] = make_task(v, prev, kend, r0, r1, lg_s);
+      }
+      prev = kend;
+    }
+    for (; t < nc_pos[v] + n; t++) ct[t] = make_task(v, k1, k1, off[v], off[v] + 1, 0);  // empty chunks: no-ops
+  }
+}
+
+// the CTA tasks of heads that are not cluster heads (at most kBlockDmax members)
+struct NotClusterHead {
+  const int64_t *off;
+  __host__ __device__ bool operator()(const Task &t) const { return off[t.v + 1] - off[t.v] <= kBlockDmax; }
+};
+
 // ---- membership structures --------------------------------------------------
 
 __device__ __forceinline__ uint32_t hash_slot(int32_t x, int shift) {
@@ -397,10 +466,12 @@ struct Members {
   int shift;        // hash: 32 - log2(slots)
   bool bitmap;
   bool cuckoo;      // hash kept as a cuckoo table (global-count warp tasks)
+  uint32_t ctab;    // cluster tier: the shared-window address of the CTAs' tables
+  int32_t cb[kCluster - 1];  // cluster tier: the first member of CTAs 1 .. kCluster-1
 };
 
 // Member-set kinds, one specialised streaming loop each.
-constexpr int kKindHash = 0, kKindBitmap = 1, kKindCuckoo = 2;
+constexpr int kKindHash = 0, kKindBitmap = 1, kKindCuckoo = 2, kKindCluster = 3;
 
 // Chooses the structure for members mem[0, n) (ascending) that fits `words`
 // words (a bitmap only while the members' id range is at most bitmap_bits)
@@ -574,8 +645,44 @@ __device__ __forceinline__ uint32_t cuckoo_test(const Members &m, int32_t w) {
   return uint32_t(x == key) | uint32_t(y == key);
 }
 
+// the shared::cluster address of the same shared-memory offset in CTA
+// `rank` of this cluster
+__device__ __forceinline__ uint32_t cluster_addr(uint32_t local, uint32_t rank) {
+  uint32_t r;
+  asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(local), "r"(rank));
+  return r;
+}
+__device__ __forceinline__ int32_t ld_cluster(uint32_t addr) {
+  int32_t v;
+  asm volatile("ld.shared::cluster.s32 %0, [%1];" : "=r"(v) : "r"(addr));
+  return v;
+}
+
+// cluster membership: CTA c of the cluster holds the members from cb[c-1]
+// up to cb[c] in a linear-probing table (at most kBlockDmax members in
+// kBlockWords slots, so every probe chain ends at an empty slot); w is
+// looked up in the table of the CTA whose range holds it
+__device__ __forceinline__ uint32_t cluster_test(const Members &m, int32_t w) {
+  if (uint32_t(w - m.lo) > uint32_t(m.hi - m.lo)) return 0u;  // sentinels too
+  uint32_t owner = 0;
+#pragma unroll
+  for (int c = 0; c < kCluster - 1; c++) owner += uint32_t(w >= m.cb[c]);
+  const uint32_t base = cluster_addr(m.ctab, owner);
+  uint32_t h = hash_slot(w, m.shift);
+  while (true) {
+    const int32_t k = ld_cluster(base + 4u * h);
+    if (k == w) return 1u;
+    if (k == kEmpty) return 0u;
+    h = (h + 1) & m.mask;
+  }
+}
+
 template <bool PV, int KIND>
 __device__ __forceinline__ int probe_pair(const int4 a, const int4 b, const Members &m) {
+  if (KIND == kKindCluster) {
+    return int((cluster_test(m, a.x) + cluster_test(m, a.y)) + (cluster_test(m, a.z) + cluster_test(m, a.w)) +
+               (cluster_test(m, b.x) + cluster_test(m, b.y)) + (cluster_test(m, b.z) + cluster_test(m, b.w)));
+  }
   if (KIND == kKindBitmap) {
     return int((bitmap_test(m, a.x) + bitmap_test(m, a.y)) + (bitmap_test(m, a.z) + bitmap_test(m, a.w)) +
                (bitmap_test(m, b.x) + bitmap_test(m, b.y)) + (bitmap_test(m, b.z) + bitmap_test(m, b.w)));
@@ -663,7 +770,7 @@ __device__ __forceinline__ int64_t stream_kind(const InRec *__restrict__ rec, co
                                                int64_t k0, int64_t kend, int lg_s, int *cursor, const Members &m,
                                                int64_t *__restrict__ pv, unsigned int *__restrict__ es,
                                                const int64_t *__restrict__ off, const int64_t *__restrict__ poff,
-                                               int lane) {
+                                               int lane, int bstride = 1, int boff = 0) {
   constexpr bool PV = MODE != 0;
   const int S = 1 << lg_s;
   const int bsz = 32 >> lg_s;
@@ -680,7 +787,9 @@ __device__ __forceinline__ int64_t stream_kind(const InRec *__restrict__ rec, co
     }
     int c = 0;
     if (lane == 0) c = atomicAdd(cursor, bsz);
-    return __shfl_sync(0xffffffffu, c, 0);
+    // batch c / bsz of this caller is batch (c / bsz) * bstride + boff of the
+    // task (a cluster's CTAs take every kCluster-th batch each)
+    return __shfl_sync(0xffffffffu, c, 0) * bstride + boff * bsz;
   };
   auto fetch = [&](int32_t base) -> int4 {
     const int32_t r = base + j;
@@ -791,6 +900,8 @@ struct CountArgs {
   int64_t n_wt;
   const int32_t *tt;  // lane tasks (heads)
   int64_t n_tt;
+  const Task *ct;  // cluster tasks
+  int64_t n_ct;
   unsigned long long *cursor;     // [0] CTA, [1] warp, [2] lane task cursors
   unsigned long long *global;     // the total
   int64_t *pv;                    // per-vertex counts (per-vertex mode)
@@ -1194,6 +1305,113 @@ __global__ void __launch_bounds__(kThreads, MODE == 0 ? kMinBlocks : 3) k_count(
 
 // dynamic shared memory: member words; in modes 1 and 2 also hash counters
 // or bitmap word starts, and bitmap member counters
+// ---- the cluster tier (global count) ---------------------------------------
+//
+// A cluster of kCluster CTAs counts one cluster task at a time: the part's
+// members (up to kClusterDmax, ascending) are split into kCluster contiguous
+// runs, CTA c hashing run c into its own table, and every candidate is
+// looked up in the table of the CTA whose id range holds it, through
+// distributed shared memory. CTA 0 claims each task and publishes it, and a
+// cursor for the task's record batches, in its shared memory (two buffers,
+// so it can publish the next task while the others still stream the
+// current one); all CTAs of the cluster read the same task sequence, so
+// they reach the same cluster barriers and leave together when it is empty.
+// Counts: warp shuffles, the CTA's warps, then the cluster's CTAs summed in
+// CTA 0's shared memory, one global add per cluster.
+// record batches: every kCluster-th batch of the task from each CTA's own
+// cursor (781 ms on the graph above) or all from one cursor in CTA 0's shared
+// memory (823 ms)
+#ifndef XT_CLUSTER_SHARED_CURSOR
+#define XT_CLUSTER_SHARED_CURSOR 0
+#endif
+// 4 CTAs of 256 threads per SM (64 registers): Chung-Lu n=4.19M under the id
+// orientation 704 ms, against 781 ms at 2 and 784 ms at 3
+#ifndef XT_CLUSTER_MINB
+#define XT_CLUSTER_MINB 4
+#endif
+__global__ void __cluster_dims__(kCluster, 1, 1) __launch_bounds__(kThreads, XT_CLUSTER_MINB)
+    k_count_cluster(const CountArgs a) {
+  namespace cg = cooperative_groups;
+  cg::cluster_group cluster = cg::this_cluster();
+  const unsigned rank = cluster.block_rank();
+  extern __shared__ int32_t smem[];
+  int32_t *table = smem;  // kBlockWords slots
+  __shared__ Task s_ct[2];
+  __shared__ int s_cbatch[2];
+  __shared__ unsigned long long s_cred[kCluster];
+  __shared__ unsigned long long s_wred[kWarps];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int32_t *__restrict__ col = a.col;
+  const Task *ct0 = cluster.map_shared_rank(s_ct, 0);
+  int *cb0 = cluster.map_shared_rank(s_cbatch, 0);
+  unsigned long long *red0 = cluster.map_shared_rank(s_cred, 0);
+  int lg = 6;
+  while ((2 << lg) <= kBlockWords) lg++;
+  int64_t acc = 0;
+  for (int cur = 0;; cur ^= 1) {
+    if (rank == 0 && tid == 0) {
+      const unsigned long long i = atomicAdd(&a.cursor[3], 1ull);
+      Task t;
+      if (int64_t(i) < a.n_ct) {
+        t = a.ct[i];
+      } else {
+        t.k0 = t.r0 = 0;
+        t.v = t.nmem = t.lg_s = 0;
+        t.nrec = -1;
+      }
+      s_ct[cur] = t;
+    }
+    if (tid == 0) s_cbatch[cur] = 0;
+    cluster.sync();  // the task is published, and every CTA is done with the previous one
+    const Task t = ct0[cur];
+    if (t.nrec < 0) break;
+    // this CTA's run of the part's members into its table
+    const int per = (t.nmem + kCluster - 1) / kCluster;
+    const int m0 = min(t.nmem, int(rank) * per), m1 = min(t.nmem, m0 + per);
+    for (int i = 4 * tid; i < kBlockWords; i += 4 * kThreads)
+      *reinterpret_cast<int4 *>(table + i) = make_int4(kEmpty, kEmpty, kEmpty, kEmpty);
+    __syncthreads();
+    Members m;
+    m.words = table;
+    m.idx = nullptr;
+    m.mcnt = nullptr;
+    m.mask = (1u << lg) - 1;
+    m.shift = 32 - lg;
+    m.base = m.nwords = 0;
+    m.bitmap = m.cuckoo = false;
+    m.ctab = smem_u32(table);
+    for (int i = m0 + tid; i < m1; i += kThreads) hash_insert(table, m.mask, m.shift, col[t.r0 + i]);
+    m.lo = col[t.r0];
+    m.hi = col[t.r0 + t.nmem - 1];
+#pragma unroll
+    for (int c = 1; c < kCluster; c++) m.cb[c - 1] = c * per < t.nmem ? col[t.r0 + c * per] : 0x7fffffff;
+    cluster.sync();  // every table is built
+#if XT_CLUSTER_SHARED_CURSOR
+    const int64_t h = stream_kind<0, kKindCluster, false>(a.rec, a.colp, t.k0, t.k0 + t.nrec, t.lg_s, cb0 + cur, m,
+                                                          nullptr, nullptr, a.off, a.poff, lane);
+#else
+    const int64_t h = stream_kind<0, kKindCluster, false>(a.rec, a.colp, t.k0, t.k0 + t.nrec, t.lg_s, s_cbatch + cur,
+                                                          m, nullptr, nullptr, a.off, a.poff, lane, kCluster, rank);
+#endif
+    acc += h;
+    if (a.group) credit_group(a, t.v, h, lane);
+  }
+  for (int o = 16; o; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+  if (lane == 0) s_wred[warp] = (unsigned long long)acc;
+  __syncthreads();
+  if (tid == 0) {
+    unsigned long long tot = 0;
+    for (int w = 0; w < kWarps; w++) tot += s_wred[w];
+    red0[rank] = tot;
+  }
+  cluster.sync();  // every CTA's sum is in CTA 0
+  if (rank == 0 && tid == 0) {
+    unsigned long long tot = 0;
+    for (int r = 0; r < kCluster; r++) tot += s_cred[r];
+    if (tot) atomicAdd(a.global, tot);
+  }
+}
+
 static size_t count_smem_bytes(bool pv) {
   return pv ? sizeof(int32_t) * (kBlockWords + kBlockDmax) + sizeof(uint16_t) * kBlockWords
             : sizeof(int32_t) * kBlockWords;
@@ -1222,6 +1440,8 @@ void free_plan(Graph *g) {
   if (!g->plan) return;
   Ctx *c = g->ctx;
   dfree(c, g->plan->d_bt);
+  dfree(c, g->plan->d_ct);
+  dfree(c, g->plan->d_bt0);
   dfree(c, g->plan->d_wt);
   dfree(c, g->plan->d_tt);
   dfree(c, g->plan->d_cursor);
@@ -1231,6 +1451,66 @@ void free_plan(Graph *g) {
 
 static xt_status d2h(Ctx *c, void *h, const void *d, size_t bytes) {
   return cuda_status(c, cudaMemcpyAsync(h, d, bytes, cudaMemcpyDeviceToHost, c->stream), "D2H");
+}
+
+// The cluster tasks (d_ct) and the CTA tasks of the other heads (d_bt0,
+// chunk-major order kept), and the cluster kernel's persistent grid.
+static xt_status plan_cluster(Ctx *c, Graph *g, Plan *pl, const int64_t *P, const PlanParams &pp) {
+  const int64_t nv = g->nv;
+  const int B = 256;
+  int64_t *nc = nullptr, *ncp = nullptr, *d_num = nullptr;
+  void *tmp = nullptr;
+  xt_status s = XT_OK;
+  do {
+    if ((s = dalloc_n(c, &nc, size_t(nv + 1))) != XT_OK) break;
+    if ((s = dalloc_n(c, &ncp, size_t(nv + 1))) != XT_OK) break;
+    k_plan_ccount<<<counted(c, grid_for(nv, B, c->sm_count)), B, 0, c->stream>>>(nv, g->d_off, g->d_ioff, P, pp, nc);
+    if ((s = cuda_status(c, cudaMemsetAsync(nc + nv, 0, sizeof(int64_t), c->stream), "memset")) != XT_OK) break;
+    if ((s = exclusive_scan(c, nc, ncp, nv + 1)) != XT_OK) break;
+    int64_t n = 0;
+    if ((s = d2h(c, &n, ncp + nv, sizeof(int64_t))) != XT_OK) break;
+    if ((s = cuda_status(c, cudaStreamSynchronize(c->stream), "sync")) != XT_OK) break;
+    if (n == 0) break;
+    if ((s = dalloc_n(c, &pl->d_ct, size_t(n))) != XT_OK) break;
+    k_plan_cfill<<<counted(c, grid_for(nv, B, c->sm_count)), B, 0, c->stream>>>(nv, g->d_off, g->d_ioff, P, pp, ncp,
+                                                                                pl->d_ct);
+    if ((s = cuda_status(c, cudaGetLastError(), "k_plan_cfill")) != XT_OK) break;
+    if ((s = dalloc_n(c, &pl->d_bt0, size_t(pl->n_btask))) != XT_OK) break;
+    if ((s = dalloc_n(c, &d_num, 1)) != XT_OK) break;
+    size_t bytes = 0;
+    const NotClusterHead keep{g->d_off};
+    if ((s = cuda_status(c, cub::DeviceSelect::If(nullptr, bytes, pl->d_bt, pl->d_bt0, d_num, pl->n_btask, keep,
+                                                  c->stream), "task select")) != XT_OK)
+      break;
+    if ((s = dalloc(c, &tmp, bytes)) != XT_OK) break;
+    if ((s = cuda_status(c, cub::DeviceSelect::If(tmp, bytes, pl->d_bt, pl->d_bt0, d_num, pl->n_btask, keep,
+                                                  c->stream), "task select")) != XT_OK)
+      break;
+    int64_t n0 = 0;
+    if ((s = d2h(c, &n0, d_num, sizeof(int64_t))) != XT_OK) break;
+    if ((s = cuda_status(c, cudaStreamSynchronize(c->stream), "sync")) != XT_OK) break;
+    // persistent grid: every cluster that fits on the device at once
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(kCluster);
+    cfg.blockDim = dim3(kThreads);
+    cfg.dynamicSmemBytes = sizeof(int32_t) * kBlockWords;
+    int clusters = 0;
+    if ((s = cuda_status(c, cudaOccupancyMaxActiveClusters(&clusters, k_count_cluster, &cfg), "cluster occupancy")) !=
+        XT_OK)
+      break;
+    if (clusters < 1) {
+      s = set_error(c, XT_ERR_CUDA, "no thread-block cluster of the cluster tier fits on this device");
+      break;
+    }
+    pl->n_ctask = n;
+    pl->n_btask0 = n0;
+    pl->grid_cluster = kCluster * int(std::min<int64_t>(clusters, n));
+  } while (0);
+  dfree(c, nc);
+  dfree(c, ncp);
+  dfree(c, d_num);
+  dfree(c, tmp);
+  return s;
 }
 
 xt_status make_plan(Graph *g) {
@@ -1245,7 +1525,7 @@ xt_status make_plan(Graph *g) {
   unsigned long long *stats = nullptr;
   xt_status s = XT_OK;
   do {
-    if ((s = dalloc_n(c, &pl->d_cursor, 3)) != XT_OK) break;
+    if ((s = dalloc_n(c, &pl->d_cursor, 4)) != XT_OK) break;
     if ((s = dalloc_n(c, &stats, 4)) != XT_OK) break;
     if ((s = dalloc_n(c, &P, size_t(ne + 1))) != XT_OK) break;
     if ((s = cuda_status(c, cudaMemsetAsync(stats, 0, 4 * sizeof(unsigned long long), c->stream), "memset")) !=
@@ -1381,6 +1661,11 @@ xt_status make_plan(Graph *g) {
       dfree(c, i2);
       dfree(c, tmp);
     }
+    if (s != XT_OK) break;
+    // global count: heads whose members overflow a CTA's set go to the
+    // cluster tier instead of CTA tasks over parts of their members
+    if (g->cluster_tier != 0 && g->max_out_degree > kBlockDmax && pl->n_btask > 0)
+      s = plan_cluster(c, g, pl, P, pp);
   } while (0);
   dfree(c, P);
   dfree(c, nb);
@@ -1393,6 +1678,8 @@ xt_status make_plan(Graph *g) {
   if (s != XT_OK) free_plan(g);
   return s;
 }
+
+int64_t cluster_task_count(const Graph *g) { return g->plan ? g->plan->n_ctask : 0; }
 
 // After a count has finished on the context stream: XT_ERR_TIMEOUT if a
 // CTA's bounded wait for its staged members gave up (the count is then
@@ -1419,7 +1706,7 @@ xt_status count_graph(Graph *g, int64_t *d_global, int64_t *d_pv, int64_t *d_gro
   // pairs of columns are read with 32-byte vector loads
   if (reinterpret_cast<uintptr_t>(g->d_colp) % 32 != 0)
     return set_error(c, XT_ERR_CUDA, "padded column array is not 32-byte aligned");
-  XT_CUDA(c, cudaMemsetAsync(pl->d_cursor, 0, 3 * sizeof(unsigned long long), c->stream));
+  XT_CUDA(c, cudaMemsetAsync(pl->d_cursor, 0, 4 * sizeof(unsigned long long), c->stream));
   XT_CUDA(c, cudaMemsetAsync(d_global, 0, sizeof(int64_t), c->stream));
   if (d_groups) {
     if (!g->d_group) return set_error(c, XT_ERR_INVALID, "per-group counts need a graph built as a batch");
@@ -1450,6 +1737,8 @@ xt_status count_graph(Graph *g, int64_t *d_global, int64_t *d_pv, int64_t *d_gro
   a.n_wt = pl->n_wtask;
   a.tt = pl->d_tt;
   a.n_tt = pl->n_ttask;
+  a.ct = pl->d_ct;
+  a.n_ct = pl->n_ctask;
   a.cursor = pl->d_cursor;
   a.global = reinterpret_cast<unsigned long long *>(d_global);
   a.pv = pv_int;
@@ -1464,10 +1753,20 @@ xt_status count_graph(Graph *g, int64_t *d_global, int64_t *d_pv, int64_t *d_gro
       k_count<2, false><<<counted(c, pl->grid_es), kThreads, count_smem_bytes(true), c->stream>>>(a);
     else if (d_pv)
       k_count<1, false><<<counted(c, pl->grid_pv), kThreads, count_smem_bytes(true), c->stream>>>(a);
-    else if (g->prefetch_suffix > 0)
-      k_count<0, true><<<counted(c, pl->grid_global), kThreads, count_smem_bytes(false), c->stream>>>(a);
-    else
-      k_count<0, false><<<counted(c, pl->grid_global), kThreads, count_smem_bytes(false), c->stream>>>(a);
+    else {
+      // cluster heads leave the CTA task list to the cluster tier
+      CountArgs a0 = a;
+      if (pl->n_ctask > 0) {
+        a0.bt = pl->d_bt0;
+        a0.n_bt = pl->n_btask0;
+      }
+      if (g->prefetch_suffix > 0)
+        k_count<0, true><<<counted(c, pl->grid_global), kThreads, count_smem_bytes(false), c->stream>>>(a0);
+      else
+        k_count<0, false><<<counted(c, pl->grid_global), kThreads, count_smem_bytes(false), c->stream>>>(a0);
+      if (pl->n_ctask > 0)
+        k_count_cluster<<<counted(c, dim3(pl->grid_cluster)), kThreads, sizeof(int32_t) * kBlockWords, c->stream>>>(a);
+    }
   }
   if (d_support && g->ne > 0)
     k_widen<<<counted(c, grid_for(g->ne, 256, c->sm_count)), 256, 0, c->stream>>>(es, g->ne, d_support);

@@ -112,6 +112,8 @@ struct Graph {
   int64_t tune_warp_work = 0;
   int64_t tune_bitmap_bits = 0;
   int prefetch_suffix = 0;      // global count: bulk L2 prefetch of each record's suffix (1) or not (0)
+  int cluster_tier = 0;         // global count: heads over a CTA's member set on thread-block clusters (1) or
+                                //   as CTA tasks over parts of their members (0, the default: faster)
   int cuckoo_iters = -1;        // test hook: cuckoo eviction chain limit (-1: the default)
   int64_t tier_lane_work = -1;  // tier limits (-1: automatic, 0: tier off)
   int64_t tier_warp_work = -1;
@@ -168,6 +170,8 @@ xt_status count_graph(Graph *g, int64_t *d_global, int64_t *d_pv, int64_t *d_gro
 // Synchronises the context stream and reports a count whose bounded device
 // wait gave up (XT_ERR_TIMEOUT); the synchronous count calls end with it.
 xt_status count_status(Ctx *c);
+// tasks of the global count's thread-block cluster tier in the graph's plan (0 without a plan)
+int64_t cluster_task_count(const Graph *g);
 
 }  // namespace xt
 
