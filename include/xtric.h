@@ -43,6 +43,9 @@ typedef enum {
  * XT_ORIENT_DEGREE ranks by (degree, id); the global count is identical. */
 typedef enum { XT_ORIENT_ID = 0, XT_ORIENT_DEGREE = 1 } xt_orient;
 
+/* lane-tier intersection kinds (xt_graph_set_lane_intersect) */
+typedef enum { XT_LANE_BSEARCH = 0, XT_LANE_MERGE = 1 } xt_lane_intersect;
+
 /* xt_graph_from_csr flag: the CSR is already canonical (rows sorted, no
  * duplicates, symmetric, no self loops), the contract under which the
  * reference reads vite files (graph.hpp:294-395), so deduplication is skipped.
@@ -247,6 +250,17 @@ xt_status xt_graph_set_prefetch(xt_graph *g, int on);
  * always use the CTA parts. Counts are identical either way. Re-plans (and
  * re-captures a captured graph). */
 xt_status xt_graph_set_cluster(xt_graph *g, int on);
+/* Lane tier intersection (heads counted one per lane, see
+ * xt_graph_set_tiers): each candidate of an in-record's suffix is found in
+ * N+(v) from the position after the previous one, by binary search
+ * (XT_LANE_BSEARCH, the default) or by stepping forward, a two-pointer merge
+ * of the two ascending lists (XT_LANE_MERGE), cheaper when N+(v) is short
+ * next to the suffixes. The binary search is the reference's own
+ * (count_if_edge_exists, counting.cu:95-131; check_edgelist,
+ * xxtric.hpp:516-588); the reference has no merge. The autotuner tries both
+ * where the plan has lane tasks. Counts are identical. Re-captures a
+ * captured graph. */
+xt_status xt_graph_set_lane_intersect(xt_graph *g, int kind);
 /* Test hook, no counterpart in the reference: caps the eviction chain of the
  * global count's cuckoo member sets at `iters` steps (negative: the default
  * of 64). With 0 or 1 nearly every hashed set falls back to linear probing,

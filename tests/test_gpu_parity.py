@@ -441,9 +441,10 @@ TIERS = [(1 << 40, 0), (0, 1 << 40), (0, 0), (64, 4096), (-1, -1)]
 
 @pytest.mark.parametrize("kind", ["rmat", "chunglu"])
 def test_each_tier_alone_vs_oracle(ctx, torch_cuda, kind):
-    # Lane tasks (binary search in the row), warp tasks and CTA tasks each
-    # count the whole graph alone, then mixed; totals, per-vertex counts and
-    # a captured replay after a re-plan all equal the oracle's.
+    # Lane tasks (binary search in the row, or a two-pointer merge), warp
+    # tasks and CTA tasks each count the whole graph alone, then mixed;
+    # totals, per-vertex counts and a captured replay after a re-plan all
+    # equal the oracle's.
     torch = torch_cuda
     if kind == "rmat":
         n, m = 1 << 14, 16 << 14
@@ -466,6 +467,12 @@ def test_each_tier_alone_vs_oracle(ctx, torch_cuda, kind):
                 t, pv = g.count(per_vertex=True)
                 assert t == expect, (orient, lane_work, warp_work)
                 assert (pv == opv).all(), (orient, lane_work, warp_work)
+                # the lane tier's two-pointer merge instead of its binary search
+                g.set_lane_intersect(xt.LANE_MERGE)
+                t, pv = g.count(per_vertex=True)
+                assert t == expect and (pv == opv).all(), (orient, lane_work, warp_work, "merge")
+                assert g.count() == expect, (orient, lane_work, warp_work, "merge")
+                g.set_lane_intersect(xt.LANE_BSEARCH)
                 # the global-count kernel: cuckoo member sets, their linear-
                 # probing fallback (chains capped at 0 and 1 evictions) and
                 # the bulk suffix prefetch
@@ -534,6 +541,9 @@ def test_edge_support_every_tier(ctx, torch_cuda):
                 if ref is None:
                     ref = oracle_support_of(off, tails, a, b)
                 assert (sup == ref).all(), (orient, lane_work, warp_work)
+                g.set_lane_intersect(xt.LANE_MERGE)
+                assert (g.edge_support()[2] == ref).all(), (orient, lane_work, warp_work, "merge")
+                g.set_lane_intersect(xt.LANE_BSEARCH)
             # the device-output form gives the same supports, in csr() order
             t, host = g.count_edges()
             dg = torch.zeros(1, dtype=torch.int64, device="cuda")

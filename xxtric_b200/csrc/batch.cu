@@ -456,6 +456,12 @@ xt_status set_prefetch(Graph *g, int on) {
   return XT_OK;
 }
 
+static xt_status set_lane_merge(Graph *g, int on) {
+  g->lane_merge = on ? 1 : 0;
+  if (g->exec) XT_TRY(capture_count(g));  // the launch's arguments inside the captured graph change
+  return XT_OK;
+}
+
 static xt_status set_cluster(Graph *g, int on) {
   const bool was_captured = g->exec != nullptr;
   g->cluster_tier = on ? 1 : 0;
@@ -513,7 +519,7 @@ static std::string tune_key(const Graph *g) {
   };
   char buf[512];
   // the schedule revision keeps timings of an older kernel from being reused
-  snprintf(buf, sizeof buf, "sched8|%s|sm%d|orient%d|nv2^%d|ne2^%d|work2^%d|groups%lld", p.name, p.multiProcessorCount,
+  snprintf(buf, sizeof buf, "sched9|%s|sm%d|orient%d|nv2^%d|ne2^%d|work2^%d|groups%lld", p.name, p.multiProcessorCount,
            g->orient, lg(g->nv), lg(g->ne), lg(g->stream_work), (long long)g->n_groups);
   for (char *q = buf; *q; q++)
     if (*q == ' ') *q = '_';
@@ -534,12 +540,13 @@ xt_status autotune(Graph *g, int reps, const char *cache_path, std::string *repo
       while (fgets(line, sizeof line, f)) {
         char k[300];
         long long bw, ww, bb;
-        int pf;
+        int pf, lm;
         double ms;
-        if (sscanf(line, "%299s %lld %lld %lld %d %lf", k, &bw, &ww, &bb, &pf, &ms) == 6 && key == k) {
+        if (sscanf(line, "%299s %lld %lld %lld %d %d %lf", k, &bw, &ww, &bb, &pf, &lm, &ms) == 7 && key == k) {
           fclose(f);
           if (report) *report = "{\"cached\": true, \"key\": \"" + key + "\"}";
           XT_TRY(set_prefetch(g, pf));
+          XT_TRY(set_lane_merge(g, lm));
           return set_tuning(g, bw, ww, bb);
         }
       }
@@ -549,6 +556,7 @@ xt_status autotune(Graph *g, int reps, const char *cache_path, std::string *repo
   int64_t best[3] = {0, 0, 0};
   double best_ms = 0;
   XT_TRY(set_prefetch(g, 0));
+  XT_TRY(set_lane_merge(g, 0));
   XT_TRY(set_tuning(g, 0, 0, 0));
   XT_TRY(time_count(g, reps, &best_ms));
   std::string rep = "{\"key\": \"" + key + "\", \"trials\": [";
@@ -590,16 +598,31 @@ xt_status autotune(Graph *g, int reps, const char *cache_path, std::string *repo
     }
     XT_TRY(set_prefetch(g, best_pf));
   }
+  // the lane tier's intersection: binary search or two-pointer merge (only
+  // where the plan has lane tasks)
+  int best_lm = 0;
+  if (lane_task_count(g) > 0) {
+    XT_TRY(set_lane_merge(g, 1));
+    double ms = 0;
+    XT_TRY(time_count(g, reps, &ms));
+    snprintf(buf, sizeof buf, ", {\"lane_merge\": 1, \"ms\": %.4f}", ms);
+    rep += buf;
+    if (ms < best_ms) {
+      best_ms = ms;
+      best_lm = 1;
+    }
+    XT_TRY(set_lane_merge(g, best_lm));
+  }
   snprintf(buf, sizeof buf,
            "], \"best\": {\"block_work\": %lld, \"warp_work\": %lld, \"bitmap_bits\": %lld, \"prefetch\": %d, "
-           "\"ms\": %.4f}}",
-           (long long)best[0], (long long)best[1], (long long)best[2], best_pf, best_ms);
+           "\"lane_merge\": %d, \"ms\": %.4f}}",
+           (long long)best[0], (long long)best[1], (long long)best[2], best_pf, best_lm, best_ms);
   rep += buf;
   if (report) *report = rep;
   if (cache_path && *cache_path) {
     if (FILE *f = fopen(cache_path, "a")) {
-      fprintf(f, "%s %lld %lld %lld %d %.4f\n", key.c_str(), (long long)best[0], (long long)best[1],
-              (long long)best[2], best_pf, best_ms);
+      fprintf(f, "%s %lld %lld %lld %d %d %.4f\n", key.c_str(), (long long)best[0], (long long)best[1],
+              (long long)best[2], best_pf, best_lm, best_ms);
       fclose(f);
     }
   }
@@ -764,6 +787,12 @@ xt_status xt_graph_set_prefetch(xt_graph *gr, int on) {
   if (!gr || !gr->g.ctx) return XT_ERR_INVALID;
   cudaSetDevice(gr->g.ctx->device);
   return set_prefetch(&gr->g, on);
+}
+
+xt_status xt_graph_set_lane_intersect(xt_graph *gr, int kind) {
+  if (!gr || !gr->g.ctx || (kind != XT_LANE_BSEARCH && kind != XT_LANE_MERGE)) return XT_ERR_INVALID;
+  cudaSetDevice(gr->g.ctx->device);
+  return set_lane_merge(&gr->g, kind == XT_LANE_MERGE);
 }
 
 xt_status xt_graph_set_cluster(xt_graph *gr, int on) {

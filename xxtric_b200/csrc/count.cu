@@ -28,6 +28,7 @@
 // Inside a task, lanes walk whole suffixes in aligned 32-byte pairs of the
 // padded column array, with no masking (see stream_kind).
 #include <cooperative_groups.h>
+#include <type_traits>
 #include <cub/cub.cuh>
 #include <thrust/iterator/counting_iterator.h>
 #include <thrust/iterator/transform_iterator.h>
@@ -902,6 +903,7 @@ struct CountArgs {
   int64_t n_tt;
   const Task *ct;  // cluster tasks
   int64_t n_ct;
+  int lane_merge;  // lane tasks: members found by a two-pointer merge (1) or binary search (0)
   unsigned long long *cursor;     // [0] CTA, [1] warp, [2] lane task cursors
   unsigned long long *global;     // the total
   int64_t *pv;                    // per-vertex counts (per-vertex mode)
@@ -1240,56 +1242,70 @@ __global__ void __launch_bounds__(kThreads, MODE == 0 ? kMinBlocks : 3) k_count(
     }
   }
 
-  // ---- lane tasks: one small head per lane, members binary-searched ----
-  while (true) {
-    unsigned long long base = 0;
-    if (lane == 0) base = atomicAdd(&cursor[2], 32ull);
-    base = __shfl_sync(0xffffffffu, base, 0);
-    if (int64_t(base) >= a.n_tt) break;
-    const int64_t i = int64_t(base) + lane;
-    if (i >= a.n_tt) continue;
-    const int32_t v = a.tt[i];
-    const int64_t r0 = off[v], r1 = off[v + 1];
-    const int32_t lo = col[r0], hi = col[r1 - 1];
-    int64_t hv = 0;
-    const int32_t *__restrict__ colp = a.colp;
-    for (int64_t k = ioff[v]; k < ioff[v + 1]; k++) {
-      const InRec r = rec[k];
-      // per-edge mode: row u's shift from padded to unpadded positions
-      const int64_t dpos = MODE == 2 ? off[r.u] - a.poff[r.u] : 0;
-      int64_t b = r0;  // members below b are below every remaining candidate
-      int32_t hu = 0;
-      for (int64_t p = r.s; p < r.s + r.len; p++) {
-        const int32_t w = colp[p];
-        if (w > hi) break;  // the suffix ascends
-        if (w < lo) continue;
-        int64_t x = b, y = r1;
-        while (x < y) {
-          const int64_t mid = (x + y) >> 1;
-          if (col[mid] < w) x = mid + 1;
-          else y = mid;
-        }
-        b = x;
-        if (col[x] == w) {  // x < r1: w <= hi
-          hu++;
-          if (MODE == 1) atomicAdd(reinterpret_cast<unsigned long long *>(&pv[w]), 1ull);
-          if (MODE == 2) {
-            atomicAdd(&es[p + dpos], 1u);  // the edge u->w
-            atomicAdd(&es[x], 1u);  // the edge v->w
+  // ---- lane tasks: one small head per lane ----
+  // Each candidate w of a record's suffix is found in N+(v) (ascending) from
+  // the position after the previous one: by binary search (MERGE = false),
+  // or by stepping forward, a two-pointer merge of the suffix with N+(v)
+  // (MERGE = true; a.lane_merge, which the autotuner tries).
+  auto lane_tasks = [&](auto merge_tag) {
+    constexpr bool MERGE = decltype(merge_tag)::value;
+    while (true) {
+      unsigned long long base = 0;
+      if (lane == 0) base = atomicAdd(&cursor[2], 32ull);
+      base = __shfl_sync(0xffffffffu, base, 0);
+      if (int64_t(base) >= a.n_tt) break;
+      const int64_t i = int64_t(base) + lane;
+      if (i >= a.n_tt) continue;
+      const int32_t v = a.tt[i];
+      const int64_t r0 = off[v], r1 = off[v + 1];
+      const int32_t lo = col[r0], hi = col[r1 - 1];
+      int64_t hv = 0;
+      const int32_t *__restrict__ colp = a.colp;
+      for (int64_t k = ioff[v]; k < ioff[v + 1]; k++) {
+        const InRec r = rec[k];
+        // per-edge mode: row u's shift from padded to unpadded positions
+        const int64_t dpos = MODE == 2 ? off[r.u] - a.poff[r.u] : 0;
+        int64_t b = r0;  // members below b are below every remaining candidate
+        int32_t hu = 0;
+        for (int64_t p = r.s; p < r.s + r.len; p++) {
+          const int32_t w = colp[p];
+          if (w > hi) break;  // the suffix ascends
+          if (w < lo) continue;
+          int64_t x = b;
+          if (MERGE) {
+            while (col[x] < w) x++;  // stops by r1 - 1: w <= hi
+          } else {
+            int64_t y = r1;
+            while (x < y) {
+              const int64_t mid = (x + y) >> 1;
+              if (col[mid] < w) x = mid + 1;
+              else y = mid;
+            }
           }
-          b = x + 1;
+          b = x;
+          if (col[x] == w) {  // x < r1: w <= hi
+            hu++;
+            if (MODE == 1) atomicAdd(reinterpret_cast<unsigned long long *>(&pv[w]), 1ull);
+            if (MODE == 2) {
+              atomicAdd(&es[p + dpos], 1u);  // the edge u->w
+              atomicAdd(&es[x], 1u);  // the edge v->w
+            }
+            b = x + 1;
+          }
         }
+        hv += hu;
+        if (MODE == 1 && hu) atomicAdd(reinterpret_cast<unsigned long long *>(&pv[r.u]), (unsigned long long)hu);
+        if (MODE == 2 && hu) atomicAdd(&es[r.s - 1 + dpos], unsigned(hu));  // the edge u->v
       }
-      hv += hu;
-      if (MODE == 1 && hu) atomicAdd(reinterpret_cast<unsigned long long *>(&pv[r.u]), (unsigned long long)hu);
-      if (MODE == 2 && hu) atomicAdd(&es[r.s - 1 + dpos], unsigned(hu));  // the edge u->v
+      acc += hv;
+      if (hv) {
+        if (MODE == 1) atomicAdd(reinterpret_cast<unsigned long long *>(&pv[v]), (unsigned long long)hv);
+        if (a.group) atomicAdd(&a.group_out[a.group[v]], (unsigned long long)hv);
+      }
     }
-    acc += hv;
-    if (hv) {
-      if (MODE == 1) atomicAdd(reinterpret_cast<unsigned long long *>(&pv[v]), (unsigned long long)hv);
-      if (a.group) atomicAdd(&a.group_out[a.group[v]], (unsigned long long)hv);
-    }
-  }
+  };
+  if (a.lane_merge) lane_tasks(std::true_type{});
+  else lane_tasks(std::false_type{});
 
   // ---- reduce ----
   for (int o = 16; o; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
@@ -1680,6 +1696,7 @@ xt_status make_plan(Graph *g) {
 }
 
 int64_t cluster_task_count(const Graph *g) { return g->plan ? g->plan->n_ctask : 0; }
+int64_t lane_task_count(const Graph *g) { return g->plan ? g->plan->n_ttask : 0; }
 
 // After a count has finished on the context stream: XT_ERR_TIMEOUT if a
 // CTA's bounded wait for its staged members gave up (the count is then
@@ -1739,6 +1756,7 @@ xt_status count_graph(Graph *g, int64_t *d_global, int64_t *d_pv, int64_t *d_gro
   a.n_tt = pl->n_ttask;
   a.ct = pl->d_ct;
   a.n_ct = pl->n_ctask;
+  a.lane_merge = g->lane_merge;
   a.cursor = pl->d_cursor;
   a.global = reinterpret_cast<unsigned long long *>(d_global);
   a.pv = pv_int;

@@ -112,6 +112,7 @@ struct Graph {
   int64_t tune_warp_work = 0;
   int64_t tune_bitmap_bits = 0;
   int prefetch_suffix = 0;      // global count: bulk L2 prefetch of each record's suffix (1) or not (0)
+  int lane_merge = 0;            // lane tasks: two-pointer merge (1) or binary search (0) over N+(v)
   int cluster_tier = 0;         // global count: heads over a CTA's member set on thread-block clusters (1) or
                                 //   as CTA tasks over parts of their members (0, the default: faster)
   int cuckoo_iters = -1;        // test hook: cuckoo eviction chain limit (-1: the default)
@@ -172,6 +173,8 @@ xt_status count_graph(Graph *g, int64_t *d_global, int64_t *d_pv, int64_t *d_gro
 xt_status count_status(Ctx *c);
 // tasks of the global count's thread-block cluster tier in the graph's plan (0 without a plan)
 int64_t cluster_task_count(const Graph *g);
+// lane tasks in the graph's plan (0 without a plan)
+int64_t lane_task_count(const Graph *g);
 
 }  // namespace xt
 
