@@ -71,14 +71,14 @@ typedef struct {
                              suffix of N+(u) after each out-neighbour) */
   int64_t alg_bytes;      /* bytes the count's loads request, repeats included (a suffix streamed by
                              several heads counts each time; L2 serves many of the repeats):
-                             16(nv+1) offsets + 4|E+| member columns + 16|E+| in-records +
+                             16(nv+1) offsets + 4|E+| member columns + 8|E+| in-records +
                              4 stream_work candidate columns */
   int64_t tail_alg_bytes; /* the tail-grouped figure: 8(nv+1) + 4|E+| + sum (16 + 4 d+(v)) */
   int32_t orient;         /* xt_orient used */
   int32_t reserved;
   int64_t footprint_bytes; /* bytes of the arrays the count reads, each counted once: offsets and
                               in-record offsets 16(nv+1), columns 4|E+|, padded columns, in-records
-                              16|E+|: the DRAM traffic of a count that never re-reads */
+                              8|E+|: the DRAM traffic of a count that never re-reads */
   int64_t cluster_tasks;   /* global count: the tasks of its thread-block cluster tier (see
                               xt_graph_set_cluster); 0 when no head needs it */
 } xt_graph_info;

@@ -514,11 +514,7 @@ __global__ void k_rows_emit(const int64_t *__restrict__ rstart, const uint32_t *
           col[oj + t] = int32_t(x);
           colp[q] = int32_t(x);
           ik[oj + t] = (x << lb) | (lb > 0 ? len_class_desc(sl) >> (7 - lb) : 0u);
-          InRec e;
-          e.s = q + 1;
-          e.len = int32_t(sl);
-          e.u = int32_t(base + j);
-          rec[oj + t] = e;
+          rec[oj + t] = make_inrec(q + 1, sl);
         } else {
           colp[q] = kPadSentinel;
         }
@@ -659,11 +655,7 @@ __global__ void k_in_keys(const uint64_t *__restrict__ keys, int b, const int64_
     uint32_t k = uint32_t(e & mask) << lb;
     if (lb > 0) k |= len_class_desc(len) >> (7 - lb);
     ik[p] = k;
-    InRec r;
-    r.s = poff[u] + (p - a) + 1;  // the suffix, in the padded column array
-    r.len = int32_t(len);
-    r.u = u;
-    recp[p] = r;
+    recp[p] = make_inrec(poff[u] + (p - a) + 1, len);  // the suffix, in the padded column array
   }
 }
 
@@ -832,8 +824,8 @@ static xt_status build_in_records(Ctx *c, uint64_t *keys, uint64_t *spare, int64
   const int lb = b + 7 <= 31 ? 7 : 31 - b;  // key = head << lb | class, 31 bits at most
   uint32_t *kin = reinterpret_cast<uint32_t *>(spare), *kalt = kin + m;
   InRec *r0 = nullptr, *r1 = nullptr;
-  xt_status s = dalloc_n(c, &r0, size_t(m));
-  if (s == XT_OK) s = dalloc_n(c, &r1, size_t(m));
+  xt_status s = dalloc_n(c, &r0, size_t(m) + 2);
+  if (s == XT_OK) s = dalloc_n(c, &r1, size_t(m) + 2);
   if (s == XT_OK) {
     // the sorted keys still hold each position's row and column
     k_in_keys<<<counted(c, grid_for(m, B, c->sm_count)), B, 0, c->stream>>>(keys, b, g->d_off, g->d_poff, m, lb,
@@ -881,6 +873,7 @@ static xt_status finish_csr(Ctx *c, uint64_t *keys, uint64_t *spare, int64_t m, 
     if (s == XT_OK) s = cuda_status(c, cudaStreamSynchronize(c->stream), "sync");
     dfree(c, plen);
     XT_TRY(s);
+    if (total >= kMaxColp) return set_error(c, XT_ERR_OVERFLOW, "2^35 or more padded columns: beyond what the in-records address");
     XT_TRY(dalloc_n(c, &g->d_colp, size_t(total > 0 ? total : 8)));
     g->colp_len = total;
     if (total > 0)
@@ -890,7 +883,7 @@ static xt_status finish_csr(Ctx *c, uint64_t *keys, uint64_t *spare, int64_t m, 
   }
   XT_TRY(dalloc_n(c, &g->d_ioff, size_t(nv + 1)));
   if (m == 0) {
-    XT_TRY(dalloc_n(c, &g->d_irec, 1));
+    XT_TRY(dalloc_n(c, &g->d_irec, 2));
     XT_CUDA(c, cudaMemsetAsync(g->d_ioff, 0, sizeof(int64_t) * (nv + 1), c->stream));
     return XT_OK;
   }
@@ -1020,11 +1013,15 @@ static xt_status rows_to_csr(Ctx *c, const uint32_t *rows_s, uint32_t *cols_s, i
                                             c->stream), "D2H")) != XT_OK)
       break;
     if ((s = cuda_status(c, cudaStreamSynchronize(c->stream), "sync")) != XT_OK) break;
+    if (total >= kMaxColp) {
+      s = set_error(c, XT_ERR_OVERFLOW, "2^35 or more padded columns: beyond what the in-records address");
+      break;
+    }
     if ((s = dalloc_n(c, &g->d_colp, size_t(total > 0 ? total : 8))) != XT_OK) break;
     g->colp_len = total;
     if ((s = dalloc_n(c, &g->d_ioff, size_t(nv + 1))) != XT_OK) break;
     if (m == 0) {
-      if ((s = dalloc_n(c, &g->d_irec, 1)) != XT_OK) break;
+      if ((s = dalloc_n(c, &g->d_irec, 2)) != XT_OK) break;
       s = cuda_status(c, cudaMemsetAsync(g->d_ioff, 0, sizeof(int64_t) * (nv + 1), c->stream), "memset");
       break;
     }
@@ -1033,8 +1030,8 @@ static xt_status rows_to_csr(Ctx *c, const uint32_t *rows_s, uint32_t *cols_s, i
     // records of one (head, class) stay in position order)
     const int lb = b + 7 <= 31 ? 7 : 31 - b;
     uint32_t *kin = reinterpret_cast<uint32_t *>(kbuf), *kalt = kin + m;
-    if ((s = dalloc_n(c, &r0, size_t(m))) != XT_OK) break;
-    if ((s = dalloc_n(c, &r1, size_t(m))) != XT_OK) break;
+    if ((s = dalloc_n(c, &r0, size_t(m) + 2)) != XT_OK) break;
+    if ((s = dalloc_n(c, &r1, size_t(m) + 2)) != XT_OK) break;
     k_rows_emit<<<counted(c, grid_for(nv, B, c->sm_count)), B, 0, c->stream>>>(rstart, cols_s, nv, lb, g->d_off,
                                                                                g->d_poff, g->d_col, g->d_colp, kin, r0);
     if ((s = cuda_status(c, cudaGetLastError(), "row emit")) != XT_OK) break;
@@ -1244,6 +1241,8 @@ void free_graph_device(Graph *g) {
   dfree(g->ctx, g->d_col);
   dfree(g->ctx, g->d_ioff);
   dfree(g->ctx, g->d_irec);
+  dfree(g->ctx, g->d_irec_u);
+  g->d_irec_u = nullptr;
   dfree(g->ctx, g->d_colp);
   dfree(g->ctx, g->d_poff);
   dfree(g->ctx, g->d_perm);

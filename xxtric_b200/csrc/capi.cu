@@ -281,10 +281,10 @@ xt_status xt_graph_get_info(const xt_graph *gr, xt_graph_info *info) {
   info->max_in_degree = g.max_in_degree;
   info->wedge_work = g.wedge_work;
   info->stream_work = g.stream_work;
-  info->alg_bytes = 16 * (g.nv + 1) + 20 * g.ne + 4 * g.stream_work;
+  info->alg_bytes = 16 * (g.nv + 1) + 4 * g.ne + int64_t(sizeof(InRec)) * g.ne + 4 * g.stream_work;
   info->tail_alg_bytes = 8 * (g.nv + 1) + 4 * g.ne + 16 * g.ne + 4 * g.wedge_work;
   info->orient = g.orient;
-  info->footprint_bytes = 16 * (g.nv + 1) + 20 * g.ne + 4 * g.colp_len;
+  info->footprint_bytes = 16 * (g.nv + 1) + 4 * g.ne + int64_t(sizeof(InRec)) * g.ne + 4 * g.colp_len;
   info->cluster_tasks = cluster_task_count(&g);
   return XT_OK;
 }

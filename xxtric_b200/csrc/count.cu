@@ -180,7 +180,7 @@ static unsigned grid_for(int64_t n, int block, int sm_count) {
 struct RecLen {
   const InRec *rec;
   int64_t ne;
-  __host__ __device__ int64_t operator()(int64_t e) const { return e < ne ? int64_t(rec[e].len) : 0; }
+  __host__ __device__ int64_t operator()(int64_t e) const { return e < ne ? int64_t(rec_len(rec[e])) : 0; }
 };
 
 // Graph statistics in one pass over the vertices: st[0] the largest degree
@@ -593,7 +593,7 @@ __device__ __forceinline__ void zero_words(int32_t *w, int n, int t, int nt) {
 // stored longest first, so the lanes of a batch run for about as many steps.
 constexpr int32_t kSentinel = kPadSentinel;  // negative: below every member, and not kEmpty
 // positions inside one suffix are int32: out-degrees stay below this
-constexpr int64_t kMaxOutDegree = int64_t(1) << 30;
+constexpr int64_t kMaxOutDegree = kMaxRecLen;  // and the in-records' length field
 
 // One 256-bit load per lane (sm_100 vector width; the column array is
 // 256-byte aligned, so every pair is 32-byte aligned): one L1 wavefront per
@@ -767,8 +767,9 @@ __device__ __forceinline__ int probe_pair_counted(const int4 a, const int4 b, co
 // slots where much is (R-MAT s24: 28.55 -> 30.4 ms), so it is chosen per
 // graph (xt_graph_set_prefetch, the autotuner)
 template <int MODE, int KIND, bool PF>
-__device__ __forceinline__ int64_t stream_kind(const InRec *__restrict__ rec, const int32_t *__restrict__ colp,
-                                               int64_t k0, int64_t kend, int lg_s, int *cursor, const Members &m,
+__device__ __forceinline__ int64_t stream_kind(const InRec *__restrict__ rec, const int32_t *__restrict__ rec_u,
+                                               const int32_t *__restrict__ colp, int64_t k0, int64_t kend, int lg_s,
+                                               int *cursor, const Members &m,
                                                int64_t *__restrict__ pv, unsigned int *__restrict__ es,
                                                const int64_t *__restrict__ off, const int64_t *__restrict__ poff,
                                                int lane, int bstride = 1, int boff = 0) {
@@ -779,6 +780,7 @@ __device__ __forceinline__ int64_t stream_kind(const InRec *__restrict__ rec, co
   const int32_t nrec = int32_t(kend - k0);
   const int4 sent = make_int4(kSentinel, kSentinel, kSentinel, kSentinel);
   rec += k0;
+  if (PV) rec_u += k0;
   int32_t seq = 0;
   auto claim = [&]() -> int32_t {
     if (!cursor) {
@@ -792,9 +794,11 @@ __device__ __forceinline__ int64_t stream_kind(const InRec *__restrict__ rec, co
     // task (a cluster's CTAs take every kCluster-th batch each)
     return __shfl_sync(0xffffffffu, c, 0) * bstride + boff * bsz;
   };
+  // a record as {pair, lw, 0, u} (u only in the per-vertex and per-edge modes)
   auto fetch = [&](int32_t base) -> int4 {
     const int32_t r = base + j;
-    return r < nrec ? __ldg(reinterpret_cast<const int4 *>(rec) + r) : make_int4(0, 0, 0, -1);
+    const uint2 x = r < nrec ? __ldg(reinterpret_cast<const uint2 *>(rec) + r) : make_uint2(0u, 0u);
+    return make_int4(int(x.x), int(x.y), 0, (PV && r < nrec) ? __ldg(rec_u + r) : -1);
   };
   // records are loaded two batches ahead (an L2 prefetch of the next batch's
   // suffixes cost more instructions than the latency it hid: s24 38.5 ms
@@ -807,15 +811,16 @@ __device__ __forceinline__ int64_t stream_kind(const InRec *__restrict__ rec, co
   while (kb < nrec) {  // warp-uniform
     const int32_t nnkb = claim();
     const int4 nn4 = fetch(nnkb);
-    if (PF && k == 0 && n4.z > 0) {
+    const int32_t nlen = int32_t(uint32_t(n4.y) & uint32_t(kMaxRecLen - 1));
+    if (PF && k == 0 && nlen > 0) {
       // the next batch's suffix into L2 while this batch streams (its record
       // arrived a batch ago): one bulk prefetch per record, at most 64 KB
-      const int64_t ns = int64_t(uint32_t(n4.x)) | (int64_t(n4.y) << 32);
-      const int64_t nb = int64_t((int32_t(ns & 7) + n4.z + 7) >> 3) * 32;
-      prefetch_l2(colp + (ns & ~int64_t(7)), uint32_t(nb < 65536 ? nb : 65536));
+      const int64_t nb = int64_t((int32_t(uint32_t(n4.y) >> kRecLenBits) + nlen + 7) >> 3) * 32;
+      prefetch_l2(colp + (int64_t(uint32_t(n4.x)) << 3), uint32_t(nb < 65536 ? nb : 65536));
     }
-    const int64_t s = int64_t(uint32_t(r4.x)) | (int64_t(r4.y) << 32);
-    const int32_t np = r4.z > 0 ? (int32_t(s & 7) + r4.z + 7) >> 3 : 0;  // pairs of the suffix
+    const int64_t s = (int64_t(uint32_t(r4.x)) << 3) | int64_t(uint32_t(r4.y) >> kRecLenBits);
+    const int32_t len = int32_t(uint32_t(r4.y) & uint32_t(kMaxRecLen - 1));
+    const int32_t np = len > 0 ? (int32_t(s & 7) + len + 7) >> 3 : 0;  // pairs of the suffix
     const int32_t cnt = np > k ? ((np - k + S - 1) >> lg_s) : 0;            // this lane's
     const int32_t steps = int32_t(__reduce_max_sync(0xffffffffu, uint32_t(cnt)));
     // per-edge mode: column positions of the unpadded CSR, row u's shift
@@ -873,17 +878,18 @@ __device__ __forceinline__ int64_t stream_kind(const InRec *__restrict__ rec, co
 }
 
 template <int MODE, bool PF>
-__device__ __forceinline__ int64_t stream_suffixes(const InRec *__restrict__ rec, const int32_t *__restrict__ colp,
-                                                   int64_t k0, int64_t kend, int lg_s, int *cursor, const Members &m,
+__device__ __forceinline__ int64_t stream_suffixes(const InRec *__restrict__ rec, const int32_t *__restrict__ rec_u,
+                                                   const int32_t *__restrict__ colp, int64_t k0, int64_t kend,
+                                                   int lg_s, int *cursor, const Members &m,
                                                    int64_t *__restrict__ pv, unsigned int *__restrict__ es,
                                                    const int64_t *__restrict__ off, const int64_t *__restrict__ poff,
                                                    int lane) {
   // the membership kind is fixed per task: one specialised loop each
   if (m.bitmap)
-    return stream_kind<MODE, kKindBitmap, PF>(rec, colp, k0, kend, lg_s, cursor, m, pv, es, off, poff, lane);
+    return stream_kind<MODE, kKindBitmap, PF>(rec, rec_u, colp, k0, kend, lg_s, cursor, m, pv, es, off, poff, lane);
   if (MODE == 0 && kWarpCuckoo && m.cuckoo)
-    return stream_kind<MODE, kKindCuckoo, PF>(rec, colp, k0, kend, lg_s, cursor, m, pv, es, off, poff, lane);
-  return stream_kind<MODE, kKindHash, PF>(rec, colp, k0, kend, lg_s, cursor, m, pv, es, off, poff, lane);
+    return stream_kind<MODE, kKindCuckoo, PF>(rec, rec_u, colp, k0, kend, lg_s, cursor, m, pv, es, off, poff, lane);
+  return stream_kind<MODE, kKindHash, PF>(rec, rec_u, colp, k0, kend, lg_s, cursor, m, pv, es, off, poff, lane);
 }
 
 // ---- the count kernel ---------------------------------------------------------
@@ -895,6 +901,7 @@ struct CountArgs {
   const int64_t *poff;  // padded row starts
   const int64_t *ioff;
   const InRec *rec;
+  const int32_t *rec_u;  // the records' tails (per-vertex and per-edge modes)
   const Task *bt;  // CTA tasks
   int64_t n_bt;
   const Task *wt;  // warp tasks
@@ -990,6 +997,16 @@ __device__ __forceinline__ Task claim_task(unsigned long long *cursor, const Tas
   return tasks[i];
 }
 
+// one warp: the task's records to L2, from the 16-byte boundary at or below
+// the first (a record is 8 bytes; the record array's 16 bytes of slack keep
+// the rounded-up end inside it), in pieces of at most 64 KB
+__device__ __forceinline__ void prefetch_records(const InRec *__restrict__ rec, const Task &t, int lane) {
+  const uintptr_t p0 = reinterpret_cast<uintptr_t>(rec + t.k0), a0 = p0 & ~uintptr_t(15);
+  const int64_t bytes = int64_t((p0 + uintptr_t(t.nrec) * sizeof(InRec) - a0 + 15) & ~uintptr_t(15));
+  for (int64_t q = int64_t(lane) << 16; q < bytes; q += int64_t(32) << 16)
+    prefetch_l2(reinterpret_cast<const char *>(a0) + q, uint32_t(bytes - q < 65536 ? bytes - q : 65536));
+}
+
 // one warp: copies the task's members into stage and prefetches its records
 // to L2; returns where the members start in stage
 __device__ __forceinline__ int stage_task(int32_t *stage, const int32_t *__restrict__ col,
@@ -999,9 +1016,7 @@ __device__ __forceinline__ int stage_task(int32_t *stage, const int32_t *__restr
   const int nchunk = int((t.r0 + t.nmem - a0 + 3) >> 2);  // reads stay inside the column padding
   for (int i = lane; i < nchunk; i += 32) cp_async16(stage + 4 * i, col + a0 + 4 * i);
   cp_async_commit();
-  const int64_t bytes = int64_t(t.nrec) * int64_t(sizeof(InRec));
-  for (int64_t q = int64_t(lane) << 16; q < bytes; q += int64_t(32) << 16)
-    prefetch_l2(reinterpret_cast<const char *>(rec + t.k0) + q, uint32_t(bytes - q < 65536 ? bytes - q : 65536));
+  prefetch_records(rec, t, lane);
   return int(t.r0 - a0);
 }
 
@@ -1025,9 +1040,7 @@ __device__ __forceinline__ int stage_task_bulk(int32_t *stage, uint64_t *bar, co
     }
   }
   if (t.nrec < 0) return 0;
-  const int64_t bytes = int64_t(t.nrec) * int64_t(sizeof(InRec));
-  for (int64_t q = int64_t(lane) << 16; q < bytes; q += int64_t(32) << 16)
-    prefetch_l2(reinterpret_cast<const char *>(rec + t.k0) + q, uint32_t(bytes - q < 65536 ? bytes - q : 65536));
+  prefetch_records(rec, t, lane);
   return int(t.r0 & 3);
 }
 
@@ -1127,7 +1140,7 @@ __global__ void __launch_bounds__(kThreads, MODE == 0 ? kMinBlocks : 3) k_count(
         s_soff[cur ^ 1] = so;
       }
     }
-    int64_t h = stream_suffixes<MODE, PF>(rec, a.colp, t.k0, t.k0 + t.nrec, t.lg_s, &s_batch, m, pv, es, off, a.poff,
+    int64_t h = stream_suffixes<MODE, PF>(rec, a.rec_u, a.colp, t.k0, t.k0 + t.nrec, t.lg_s, &s_batch, m, pv, es, off, a.poff,
                                       lane);
     acc += h;
     if (a.group) credit_group(a, t.v, h, lane);
@@ -1177,7 +1190,7 @@ __global__ void __launch_bounds__(kThreads, MODE == 0 ? kMinBlocks : 3) k_count(
       const Task tn = claim_task(&cursor[1], a.wt, a.n_wt, lane);  // read after the stream
       int64_t h;
       if (ok) {
-        h = stream_suffixes<MODE, PF>(rec, a.colp, t.k0, t.k0 + t.nrec, t.lg_s, nullptr, m, pv, es, off, a.poff, lane);
+        h = stream_suffixes<MODE, PF>(rec, a.rec_u, a.colp, t.k0, t.k0 + t.nrec, t.lg_s, nullptr, m, pv, es, off, a.poff, lane);
         __syncwarp();
         warp_set_reset(m, mem, t.nmem, lane);
       } else {
@@ -1190,7 +1203,7 @@ __global__ void __launch_bounds__(kThreads, MODE == 0 ? kMinBlocks : 3) k_count(
         __syncwarp();
         for (int i = lane; i < t.nmem; i += 32) members_insert_at<false>(m, mem, i);
         __syncwarp();
-        h = stream_suffixes<MODE, PF>(rec, a.colp, t.k0, t.k0 + t.nrec, t.lg_s, nullptr, m, pv, es, off, a.poff, lane);
+        h = stream_suffixes<MODE, PF>(rec, a.rec_u, a.colp, t.k0, t.k0 + t.nrec, t.lg_s, nullptr, m, pv, es, off, a.poff, lane);
         __syncwarp();
         zero_words(words, kWarpWords, lane, 32);
       }
@@ -1219,7 +1232,7 @@ __global__ void __launch_bounds__(kThreads, MODE == 0 ? kMinBlocks : 3) k_count(
       for (int i = lane; i < t.nmem; i += 32) members_insert_at<PV>(m, mem, i);
       __syncwarp();
       const Task tn = claim_task(&cursor[1], a.wt, a.n_wt, lane);  // read after the stream
-      int64_t h = stream_suffixes<MODE, PF>(rec, a.colp, t.k0, t.k0 + t.nrec, t.lg_s, nullptr, m, pv, es, off, a.poff,
+      int64_t h = stream_suffixes<MODE, PF>(rec, a.rec_u, a.colp, t.k0, t.k0 + t.nrec, t.lg_s, nullptr, m, pv, es, off, a.poff,
                                         lane);
       acc += h;
       if (a.group) credit_group(a, t.v, h, lane);
@@ -1263,11 +1276,13 @@ __global__ void __launch_bounds__(kThreads, MODE == 0 ? kMinBlocks : 3) k_count(
       const int32_t *__restrict__ colp = a.colp;
       for (int64_t k = ioff[v]; k < ioff[v + 1]; k++) {
         const InRec r = rec[k];
+        const int64_t rs = rec_s(r), re = rs + rec_len(r);
+        const int32_t ru = MODE != 0 ? a.rec_u[k] : 0;
         // per-edge mode: row u's shift from padded to unpadded positions
-        const int64_t dpos = MODE == 2 ? off[r.u] - a.poff[r.u] : 0;
+        const int64_t dpos = MODE == 2 ? off[ru] - a.poff[ru] : 0;
         int64_t b = r0;  // members below b are below every remaining candidate
         int32_t hu = 0;
-        for (int64_t p = r.s; p < r.s + r.len; p++) {
+        for (int64_t p = rs; p < re; p++) {
           const int32_t w = colp[p];
           if (w > hi) break;  // the suffix ascends
           if (w < lo) continue;
@@ -1294,8 +1309,8 @@ __global__ void __launch_bounds__(kThreads, MODE == 0 ? kMinBlocks : 3) k_count(
           }
         }
         hv += hu;
-        if (MODE == 1 && hu) atomicAdd(reinterpret_cast<unsigned long long *>(&pv[r.u]), (unsigned long long)hu);
-        if (MODE == 2 && hu) atomicAdd(&es[r.s - 1 + dpos], unsigned(hu));  // the edge u->v
+        if (MODE == 1 && hu) atomicAdd(reinterpret_cast<unsigned long long *>(&pv[ru]), (unsigned long long)hu);
+        if (MODE == 2 && hu) atomicAdd(&es[rs - 1 + dpos], unsigned(hu));  // the edge u->v
       }
       acc += hv;
       if (hv) {
@@ -1403,10 +1418,10 @@ __global__ void __cluster_dims__(kCluster, 1, 1) __launch_bounds__(kThreads, XT_
     for (int c = 1; c < kCluster; c++) m.cb[c - 1] = c * per < t.nmem ? col[t.r0 + c * per] : 0x7fffffff;
     cluster.sync();  // every table is built
 #if XT_CLUSTER_SHARED_CURSOR
-    const int64_t h = stream_kind<0, kKindCluster, false>(a.rec, a.colp, t.k0, t.k0 + t.nrec, t.lg_s, cb0 + cur, m,
+    const int64_t h = stream_kind<0, kKindCluster, false>(a.rec, nullptr, a.colp, t.k0, t.k0 + t.nrec, t.lg_s, cb0 + cur, m,
                                                           nullptr, nullptr, a.off, a.poff, lane);
 #else
-    const int64_t h = stream_kind<0, kKindCluster, false>(a.rec, a.colp, t.k0, t.k0 + t.nrec, t.lg_s, s_cbatch + cur,
+    const int64_t h = stream_kind<0, kKindCluster, false>(a.rec, nullptr, a.colp, t.k0, t.k0 + t.nrec, t.lg_s, s_cbatch + cur,
                                                           m, nullptr, nullptr, a.off, a.poff, lane, kCluster, rank);
 #endif
     acc += h;
@@ -1635,7 +1650,7 @@ xt_status make_plan(Graph *g) {
     g->wedge_work = int64_t(hs[3]);
     g->stream_work = h[2];
     if (g->max_out_degree >= kMaxOutDegree) {
-      s = set_error(c, XT_ERR_OVERFLOW, "an oriented out-degree of 2^30 or more is not supported");
+      s = set_error(c, XT_ERR_OVERFLOW, "an oriented out-degree of 2^29 or more is not supported");
       break;
     }
     if ((s = dalloc_n(c, &pl->d_bt, size_t(pl->n_btask > 0 ? pl->n_btask : 1))) != XT_OK) break;
@@ -1712,6 +1727,23 @@ xt_status count_status(Ctx *c) {
   return XT_OK;
 }
 
+// the tail u of each in-record: the row whose padded span holds position
+// s - 1 (the head's own column in N+(u)); the last row starting at or before
+// it is that row, as an empty row starts where the next one does
+__global__ void k_rec_tails(const InRec *__restrict__ rec, int64_t ne, const int64_t *__restrict__ poff, int64_t nv,
+                            int32_t *__restrict__ u) {
+  XT_GRID_STRIDE(e, ne) {
+    const int64_t q = rec_s(rec[e]) - 1;
+    int64_t lo = 0, hi = nv;  // poff[lo] <= q < poff[hi]
+    while (hi - lo > 1) {
+      const int64_t mid = (lo + hi) >> 1;
+      if (poff[mid] <= q) lo = mid;
+      else hi = mid;
+    }
+    u[e] = int32_t(lo);
+  }
+}
+
 __global__ void k_widen(const unsigned int *__restrict__ in, int64_t n, int64_t *__restrict__ out) {
   XT_GRID_STRIDE(i, n) out[i] = int64_t(in[i]);
 }
@@ -1735,6 +1767,12 @@ xt_status count_graph(Graph *g, int64_t *d_global, int64_t *d_pv, int64_t *d_gro
     XT_TRY(dalloc_n(c, &es, size_t(g->ne > 0 ? g->ne : 1)));
     XT_CUDA(c, cudaMemsetAsync(es, 0, sizeof(unsigned int) * size_t(g->ne > 0 ? g->ne : 1), c->stream));
   }
+  if ((d_pv || d_support) && !g->d_irec_u && g->ne > 0) {  // the records' tails, once per graph
+    XT_TRY(dalloc_n(c, &g->d_irec_u, size_t(g->ne)));
+    k_rec_tails<<<counted(c, grid_for(g->ne, 256, c->sm_count)), 256, 0, c->stream>>>(g->d_irec, g->ne, g->d_poff,
+                                                                                      g->nv, g->d_irec_u);
+    XT_CUDA(c, cudaGetLastError());
+  }
   int64_t *pv_int = nullptr;  // per-vertex counts in internal numbering
   if (d_pv) {
     if (g->d_perm) XT_TRY(dalloc_n(c, &pv_int, size_t(g->nv)));
@@ -1748,6 +1786,7 @@ xt_status count_graph(Graph *g, int64_t *d_global, int64_t *d_pv, int64_t *d_gro
   a.poff = g->d_poff;
   a.ioff = g->d_ioff;
   a.rec = g->d_irec;
+  a.rec_u = g->d_irec_u;
   a.bt = pl->d_bt;
   a.n_bt = pl->n_btask;
   a.wt = pl->d_wt;

@@ -79,11 +79,25 @@ constexpr int32_t kPadSentinel = -2;
 // rank above v, i.e. the suffix d_colp[s, s+len) after v's own position
 // (s indexes the padded column array).
 // Every triangle (u,v,w) has its w in exactly this suffix and in N+(v).
-struct __align__(16) InRec {
-  int64_t s;
-  int32_t len;
-  int32_t u;
+// Packed in 8 bytes: pair = s / 8 (the 32-byte pair the suffix starts in)
+// and lw = len | (s % 8) << kRecLenBits, so s < 2^35 and len < 2^29. The
+// tail u is kept apart (Graph::d_irec_u), built when a per-vertex or
+// per-edge count first needs it.
+struct __align__(8) InRec {
+  uint32_t pair;
+  uint32_t lw;
 };
+constexpr int kRecLenBits = 29;
+constexpr int64_t kMaxColp = int64_t(1) << 35;      // padded columns the records can address
+constexpr int64_t kMaxRecLen = int64_t(1) << kRecLenBits;
+__host__ __device__ inline InRec make_inrec(int64_t s, int64_t len) {
+  InRec r;
+  r.pair = uint32_t(s >> 3);
+  r.lw = uint32_t(len) | (uint32_t(s & 7) << kRecLenBits);
+  return r;
+}
+__host__ __device__ inline int64_t rec_s(InRec r) { return (int64_t(r.pair) << 3) | int64_t(r.lw >> kRecLenBits); }
+__host__ __device__ inline int32_t rec_len(InRec r) { return int32_t(r.lw & uint32_t(kMaxRecLen - 1)); }
 
 struct Graph {
   Ctx *ctx = nullptr;
@@ -98,7 +112,9 @@ struct Graph {
   int64_t *d_off = nullptr;   // out-CSR offsets, nv+1
   int32_t *d_col = nullptr;   // out-CSR columns N+(u), ne (+kColPad), rows ascending
   int64_t *d_ioff = nullptr;  // in-record offsets per head v, nv+1
-  InRec *d_irec = nullptr;    // one record per edge u->v, grouped by v
+  InRec *d_irec = nullptr;    // one record per edge u->v, grouped by v (ne + 2: the last 16 bytes are slack
+                              //   for 16-byte aligned bulk prefetches)
+  int32_t *d_irec_u = nullptr;  // the tail u of each record, built on first use (per-vertex, per-edge)
   // The columns again, each row starting on an 8-column (32-byte) boundary
   // and padded with kPadSentinel: the count streams suffixes from here in
   // whole 32-byte pairs without masking. d_poff[u] is row u's start.
