@@ -31,12 +31,13 @@ using Clock = std::chrono::steady_clock;
 // Upper bound of the device bytes held while a query of nv vertices and ne
 // edge rows is copied in, built and counted. The builder's largest phases:
 // its row sort (8 B/row copied in, 8 B/row union ids for batches, 16 B/row
-// key buffers, 1 B/row flags, 8 B/row sort scratch: 41 B/row) and the
-// in-record gather (the same 16 B/row key buffers, plus per unique edge
-// 4 B columns, 4 B padded columns, 16 B records in out-position order and
-// 16 B records grouped by head: up to 72 B/row with the input and union ids
-// held). Vertex arrays stay below 120 B/vertex through the plan. 80 B/row
-// leaves room for CUB's scratch on top of these.
+// of row ends in two sort buffers, 8 B/row of sort scratch: 40 B/row) and
+// the in-record sort (the same 16 B/row buffers, plus per unique edge 4 B
+// columns, 4 B padded columns and two 8 B record arrays: up to 52 B/row with
+// the input and union ids held; 72 B/row with the 16-byte records this
+// bound was first written for). Vertex arrays stay below 120 B/vertex
+// through the plan. 80 B/row leaves room for CUB's scratch on top of these;
+// tests/test_gpu_serve.py checks it against the measured peak.
 int64_t serve_estimate(int64_t nv, int64_t ne) {
   if (nv < 0 || ne < 0) return -1;
   return 80 * ne + 120 * nv + (int64_t(4) << 20);
