@@ -18,7 +18,11 @@ second (|E+| per step / step time).
           int32 edge list copied from pinned host memory, built into the
           oriented CSR on the device, counted, the count read back.
 N > 1 GPUs (torchrun): independent replicas, one graph per GPU, no data-path
-collective; value = all ranks' edges / the slowest rank's time.
+collective; value = all ranks' edges / the slowest rank's time. With
+--shard, the GPUs count ONE graph together instead: every rank holds the
+graph and counts its shard of the schedule (xxtric_b200.shards), and an NCCL
+all-reduce of the count closes each step; value = the graph's edges / the
+slowest rank's time (strong scaling).
 
 Other single-graph workloads, same line: chunglu (the heavy-skew Chung-Lu
 graph, n = 4,194,304, exponent 2.1, mean degree 64, max expected 131,072;
@@ -240,9 +244,11 @@ class Workload:
         cfg = {"workload": self.name, **self.extra}
         return oracle.ref_rgg(RGG_N, RGG_RANKS, self.radius), "the workload graph itself", cfg
 
-    def config(self, world: int, info: dict | None) -> dict:
+    def config(self, world: int, info: dict | None, shard: bool = False) -> dict:
+        par = (f"edge-sharded x{world} (NCCL all-reduce)" if shard else f"replicas x{world}") if world > 1 \
+            else "single GPU"
         c = {"workload": self.name, **self.extra, "seed": SEED, "orient": "degree",
-             "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+             "parallelism": par,
              "l2": ("inputs larger than L2 (CSR + transpose > 126 MB), no flush" if self.key != "rgg" else
                     "graph (~10 MB) fits in L2: back-to-back counts, no flush (launch-bound size)")}
         if info:
@@ -391,9 +397,20 @@ def run_xtric(args) -> None:
     # outputs (the kernels k_count<1> / k_count<2>), for profiling them
     d_pv = torch.zeros(n, dtype=torch.int64, device="cuda") if args.mode == "per-vertex" else None
     d_sup = torch.zeros(max(1, info["n_edges"]), dtype=torch.int64, device="cuda") if args.mode == "per-edge" else None
+    d_shard = None
+    if args.shard:
+        from xxtric_b200 import shards
+        d_shard = torch.zeros(1 + (n if d_pv is not None else info["n_edges"] if d_sup is not None else 0),
+                              dtype=torch.int64, device="cuda")
 
     def count_step():
-        if d_sup is not None:
+        if args.shard:  # this rank's shard, then the all-reduce of the parts
+            if d_sup is not None:
+                shards.count_edges_sharded(g, out=d_shard)
+            else:
+                shards.count_sharded(g, per_vertex=d_pv is not None, out=d_shard)
+            d_count.copy_(d_shard[:1])
+        elif d_sup is not None:
             g.count_edges_async(d_count, d_sup)
         else:
             g.count_async(d_count, d_pv)
@@ -427,10 +444,16 @@ def run_xtric(args) -> None:
     counts.append(int(d_count.item()))
     if len(set(counts)) != 1:
         raise RuntimeError(f"count changed between steps: {counts}")
-    value, total_edges, t_max = replicas.aggregate(info["n_edges"] * args.steps, t_total)
+    if args.shard:  # one graph counted by all ranks together
+        t_max = replicas.reduce_max(t_total)
+        value = info["n_edges"] * args.steps / t_max
+    else:
+        value, total_edges, t_max = replicas.aggregate(info["n_edges"] * args.steps, t_total)
 
     extra = {"mode": args.mode}
-    del d_pv, d_sup
+    if args.shard:
+        extra["sharding"] = {"shards": world, "collective": "NCCL all-reduce of the int64 parts" if world > 1 else None}
+    del d_pv, d_sup, d_shard
     if args.workload == "rmat24" and args.mode == "global" and not args.no_forms:
         # the per-vertex and per-edge kernels on the same graph
         pv = torch.zeros(n, dtype=torch.int64, device="cuda")
@@ -461,9 +484,9 @@ def run_xtric(args) -> None:
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": 1e3 * t_max / args.steps, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic",
-        "config": wl.config(world, info), "triangles": counts[0],
-        "triangles_per_s": counts[0] * args.steps * world / t_max,
+        "scaling": "strong" if args.shard else "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic",
+        "config": wl.config(world, info, args.shard), "triangles": counts[0],
+        "triangles_per_s": counts[0] * args.steps * (1 if args.shard else world) / t_max,
         "roofline": roofline, "e2e": e2e, "gpu_launches": launches, "clocks": clocks, **extra,
     }
 
@@ -505,12 +528,20 @@ def run_e2e(args, ctx, stream, torch, n, ne, src, dst, g, counts, info) -> dict:
     torch.cuda.empty_cache()
     hs, hd = h_src.numpy(), h_dst.numpy()
     e2e_counts = []
+    d_part = torch.zeros(1, dtype=torch.int64, device="cuda") if args.shard else None
+
+    def count_of(g2):
+        if args.shard:  # this rank's shard + the all-reduce, the sum read back
+            from xxtric_b200 import shards
+            return shards.count_sharded(g2, out=d_part)[0]
+        return g2.count()
+
     # untimed builds first: the stream-ordered pool grows over the first few
     # builds of a size (two warm-up builds left the next two at 172 and 125 ms
     # of build against 81-83 ms steady)
     for _ in range(4):
         g2 = ctx.graph_from_edges(n, hs, hd, xt.ORIENT_DEGREE)
-        e2e_counts.append(g2.count())
+        e2e_counts.append(count_of(g2))
         g2.free()
     replicas.barrier()
     torch.cuda.synchronize()
@@ -521,7 +552,7 @@ def run_e2e(args, ctx, stream, torch, n, ne, src, dst, g, counts, info) -> dict:
         h0 = time.perf_counter()
         g2 = ctx.graph_from_edges(n, hs, hd, xt.ORIENT_DEGREE)  # H2D + build + orient + plan
         h1 = time.perf_counter()
-        e2e_counts.append(g2.count())                          # count + D2H of the result
+        e2e_counts.append(count_of(g2))                        # count + D2H of the result
         h2 = time.perf_counter()
         g2.free()
         marks[i + 1].record(stream)
@@ -532,7 +563,10 @@ def run_e2e(args, ctx, stream, torch, n, ne, src, dst, g, counts, info) -> dict:
     e2e_step_ms = [marks[i].elapsed_time(marks[i + 1]) for i in range(args.e2e_steps)]
     if set(e2e_counts) != set(counts):
         raise RuntimeError(f"end-to-end count {e2e_counts} differs from {counts}")
-    e2e_value, _, _ = replicas.aggregate(info["n_edges"] * args.e2e_steps, t_e2e)
+    if args.shard:
+        e2e_value = info["n_edges"] * args.e2e_steps / replicas.reduce_max(t_e2e)
+    else:
+        e2e_value, _, _ = replicas.aggregate(info["n_edges"] * args.e2e_steps, t_e2e)
 
     return {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 2 * 4 * ne, "d2h_bytes_per_step": 8,
             "ms_per_step": 1e3 * t_e2e / args.e2e_steps, "steps": args.e2e_steps,
@@ -977,6 +1011,9 @@ def main() -> None:
     ap.add_argument("--mode", choices=["global", "per-vertex", "per-edge"], default="global",
                     help="the count the timed step runs: the global count (the headline), or with per-vertex or "
                          "per-edge counts into device memory")
+    ap.add_argument("--shard", action="store_true",
+                    help="N > 1: count one graph on all GPUs together (each rank a shard of the schedule, then an "
+                         "NCCL all-reduce) instead of independent replicas")
     ap.add_argument("--no-e2e", action="store_true",
                     help="skip the end-to-end leg (profiler captures of the count kernel)")
     args = ap.parse_args()

@@ -157,6 +157,23 @@ xt_status xt_count_edges(xt_graph *g, int64_t *global, int64_t *support);
  * d_support holds n_edges int64 entries and is overwritten */
 xt_status xt_count_edges_async(xt_graph *g, int64_t *d_global, int64_t *d_support);
 
+/* ---- edge-sharded counting over several GPUs -------------------------------
+ * Replace the per-GPU share of the reference's multi-GPU count
+ * (TriangleCounting::count, xxtric-gpu-vmm-mpi.hpp:89-129: every GPU counts
+ * its part, then MPI_Reduce sums the parts on rank 0). Here every GPU holds
+ * the whole graph (one process per GPU, each built from the same input) and
+ * counts one shard of the count's schedule: the tasks of every tier (CTA,
+ * warp and lane tasks, cluster tasks) whose index is shard modulo nshards.
+ * Every triangle falls in exactly one task, so the nshards shards' global
+ * counts, per-vertex counts and per-edge supports each sum to those of
+ * xt_count / xt_count_edges; a caller sums them with one all-reduce
+ * (xxtric_b200.shards does it over NCCL). Asynchronous on the context
+ * stream, device outputs overwritten with the shard's part (d_per_vertex:
+ * nv int64, nullable; d_support: n_edges int64 in xt_graph_get_csr order).
+ * XT_ERR_INVALID unless 0 <= shard < nshards. */
+xt_status xt_count_shard_async(xt_graph *g, int shard, int nshards, int64_t *d_global, int64_t *d_per_vertex);
+xt_status xt_count_edges_shard_async(xt_graph *g, int shard, int nshards, int64_t *d_global, int64_t *d_support);
+
 /* Replaces the kernel launcher single_gpu_count(nv, d_indices, d_edge_list,
  * d_local_count) (counting.cuh:259-265, counting.cu:537-577): the reference's
  * device CSR (int64 offsets, int64 tails; rows sorted, deduped, symmetric)

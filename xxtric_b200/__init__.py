@@ -83,6 +83,8 @@ _proto("xt_count", _int, _vp, _vp, _vp)
 _proto("xt_count_async", _int, _vp, _vp, _vp)
 _proto("xt_count_edges", _int, _vp, _vp, _vp)
 _proto("xt_count_edges_async", _int, _vp, _vp, _vp)
+_proto("xt_count_shard_async", _int, _vp, _int, _int, _vp, _vp)
+_proto("xt_count_edges_shard_async", _int, _vp, _int, _int, _vp, _vp)
 _proto("xt_count_device", _int, _i64, _vp, _vp, _vp, _int, _vp)
 _proto("xt_count_device_static", _int, _i64, _vp, _vp, _vp, _int, _vp)
 _proto("xt_graph_from_batch", _int, _vp, _i64, _vp, _vp, _vp, _vp, _int, _P(_vp))
@@ -127,7 +129,8 @@ _proto("xt_rgg_generate", _int, _i64, _int, _dbl, _dbl, _u64, _i64, _P(_i64), _v
 EXPORTED = ["xt_strerror", "xt_last_error", "xt_open", "xt_close", "xt_set_stream", "xt_debug_fail_alloc",
             "xt_launch_count", "xt_synchronize", "xt_graph_get_perm",
             "xt_graph_from_csr", "xt_graph_from_edges", "xt_graph_from_device_edges", "xt_graph_get_info",
-            "xt_graph_get_csr", "xt_graph_free", "xt_count", "xt_count_async", "xt_count_edges", "xt_count_edges_async", "xt_count_device",
+            "xt_graph_get_csr", "xt_graph_free", "xt_count", "xt_count_async", "xt_count_edges", "xt_count_edges_async",
+            "xt_count_shard_async", "xt_count_edges_shard_async", "xt_count_device",
             "xt_count_device_static", "xt_graph_from_batch", "xt_graph_from_device_batch", "xt_graph_groups",
             "xt_count_groups", "xt_count_groups_async", "xt_batch_count", "xt_graph_capture", "xt_graph_set_tuning", "xt_graph_set_tiers", "xt_graph_set_prefetch", "xt_graph_set_cluster", "xt_graph_set_lane_intersect",
             "xt_graph_debug_cuckoo_iters",
@@ -514,6 +517,18 @@ class DeviceGraph:
         """Global count and per-edge supports into device memory (d_support:
         n_edges int64 entries), queued on the context stream."""
         _check(_L.xt_count_edges_async(self._h, _ptr(d_global), _ptr(d_support)), "xt_count_edges_async", self.ctx)
+
+    def count_shard_async(self, shard: int, nshards: int, d_global, d_per_vertex=None) -> None:
+        """Shard `shard` of `nshards` of the count (every nshards-th task of the
+        schedule) into device memory, queued on the context stream; the
+        shards' outputs sum to count_async's."""
+        _check(_L.xt_count_shard_async(self._h, int(shard), int(nshards), _ptr(d_global), _ptr(d_per_vertex)),
+               "xt_count_shard_async", self.ctx)
+
+    def count_edges_shard_async(self, shard: int, nshards: int, d_global, d_support) -> None:
+        """Shard `shard` of `nshards` of the per-edge count (see count_shard_async)."""
+        _check(_L.xt_count_edges_shard_async(self._h, int(shard), int(nshards), _ptr(d_global), _ptr(d_support)),
+               "xt_count_edges_shard_async", self.ctx)
 
     @property
     def groups(self) -> int:

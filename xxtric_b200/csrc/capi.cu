@@ -382,6 +382,18 @@ xt_status xt_count_edges_async(xt_graph *gr, int64_t *d_global, int64_t *d_suppo
   return count_graph(&gr->g, d_global, nullptr, nullptr, d_support);
 }
 
+xt_status xt_count_shard_async(xt_graph *gr, int shard, int nshards, int64_t *d_global, int64_t *d_pv) {
+  if (!gr || !d_global) return XT_ERR_INVALID;
+  cudaSetDevice(gr->g.ctx->device);
+  return count_graph(&gr->g, d_global, d_pv, nullptr, nullptr, shard, nshards);
+}
+
+xt_status xt_count_edges_shard_async(xt_graph *gr, int shard, int nshards, int64_t *d_global, int64_t *d_support) {
+  if (!gr || !d_global || (gr->g.ne > 0 && !d_support)) return XT_ERR_INVALID;
+  cudaSetDevice(gr->g.ctx->device);
+  return count_graph(&gr->g, d_global, nullptr, nullptr, d_support, shard, nshards);
+}
+
 xt_status xt_count_device(int64_t nv, const int64_t *d_indices, const int64_t *d_edge_list, int64_t *d_count,
                           int accumulate, void *stream) {
   if (nv < 1 || !d_indices || !d_count) return XT_ERR_INVALID;

@@ -474,6 +474,21 @@ struct Members {
 // Member-set kinds, one specialised streaming loop each.
 constexpr int kKindHash = 0, kKindBitmap = 1, kKindCuckoo = 2, kKindCluster = 3;
 
+// Per-vertex and per-edge modes: a bitmap word packs 16 member bits (low
+// half) with the index of the word's first member (high half), so a hit
+// finds its member's counter from the one word it loaded (the index plus the
+// popcount of the set bits below) instead of a second shared load from a
+// separate index array; the bitmap then spans half the ids a 32-bit word
+// does (2^17 for a CTA). 0 keeps 32 member bits a word and the index apart.
+#ifndef XT_PV_PACKED
+#define XT_PV_PACKED 0
+#endif
+template <bool PV>
+struct BitmapWord {
+  static constexpr int kShift = (PV && XT_PV_PACKED) ? 4 : 5;  // log2 of the ids a word covers
+  static constexpr uint32_t kBits = (1u << kShift) - 1u;
+};
+
 // Chooses the structure for members mem[0, n) (ascending) that fits `words`
 // words (a bitmap only while the members' id range is at most bitmap_bits)
 // and returns how many words must be cleared. In the per-vertex and
@@ -482,14 +497,15 @@ constexpr int kKindHash = 0, kKindBitmap = 1, kKindCuckoo = 2, kKindCluster = 3;
 // the index of the member in each used slot.
 template <bool PV>
 __device__ __forceinline__ int members_layout(Members &m, const int32_t *mem, int n, int words, int64_t bitmap_bits) {
+  constexpr int sh = BitmapWord<PV>::kShift;
   m.lo = mem[0];
   m.hi = mem[n - 1];
   m.cuckoo = false;
   const int64_t range = int64_t(m.hi) - int64_t(m.lo) + 1;
-  const int64_t nw = int64_t(m.hi >> 5) - int64_t(m.lo >> 5) + 1;
+  const int64_t nw = int64_t(m.hi >> sh) - int64_t(m.lo >> sh) + 1;
   m.bitmap = nw + 1 <= int64_t(words) && range <= bitmap_bits;
   if (m.bitmap) {
-    m.base = uint32_t(m.lo >> 5);
+    m.base = uint32_t(m.lo >> sh);
     m.nwords = uint32_t(nw);
     m.mask = 0;
     m.shift = 0;
@@ -514,9 +530,17 @@ template <bool PV>
 __device__ __forceinline__ void members_insert_at(const Members &m, const int32_t *mem, int i) {
   const int32_t x = mem[i];
   if (m.bitmap) {
-    const uint32_t wd = uint32_t(x >> 5) - m.base;
-    atomicOr(reinterpret_cast<unsigned int *>(&m.words[wd]), 1u << (x & 31));
-    if (PV && (i == 0 || uint32_t(mem[i - 1] >> 5) - m.base != wd)) m.idx[wd] = uint16_t(i);
+    constexpr int sh = BitmapWord<PV>::kShift;
+    const uint32_t wd = uint32_t(x >> sh) - m.base;
+    const bool first = PV && (i == 0 || uint32_t(mem[i - 1] >> sh) - m.base != wd);
+    if (PV && XT_PV_PACKED) {
+      // the word's first member also writes its index into the high half
+      atomicOr(reinterpret_cast<unsigned int *>(&m.words[wd]),
+               (1u << (uint32_t(x) & BitmapWord<PV>::kBits)) | (first ? uint32_t(i) << 16 : 0u));
+    } else {
+      atomicOr(reinterpret_cast<unsigned int *>(&m.words[wd]), 1u << (x & 31));
+      if (first) m.idx[wd] = uint16_t(i);
+    }
   } else {
     const uint32_t slot = hash_insert(m.words, m.mask, m.shift, x);
     if (PV) m.idx[slot] = uint16_t(i);
@@ -723,22 +747,26 @@ __device__ __forceinline__ int probe_one(const Members &m, int32_t w, unsigned i
     // and then unused) and the increment is predicated on the hit. R-MAT s24
     // 63.8 -> 60.4 ms; the per-edge mode keeps its branch (its predicated
     // global increments measured 97.0 -> 98.8 ms)
-    uint32_t i = uint32_t(w >> 5) - m.base;
+    constexpr int sh = BitmapWord<true>::kShift;
+    uint32_t i = uint32_t(w >> sh) - m.base;
     i = i < m.nwords ? i : m.nwords;
     const uint32_t x = uint32_t(m.words[i]);
-    const uint32_t bit = uint32_t(w) & 31u;
+    const uint32_t bit = uint32_t(w) & BitmapWord<true>::kBits;
     const uint32_t hit = (x >> bit) & 1u;
-    const uint32_t k = uint32_t(m.idx[i]) + uint32_t(__popc(x & ((1u << bit) - 1u)));
+    const uint32_t first = XT_PV_PACKED ? (x >> 16) : uint32_t(m.idx[i]);
+    const uint32_t k = first + uint32_t(__popc(x & ((1u << bit) - 1u)));
     red_shared_add1_if(smem_u32(m.mcnt) + 4u * k, hit);
     return int(hit);
   }
   if (KIND == kKindBitmap) {
-    uint32_t i = uint32_t(w >> 5) - m.base;
+    constexpr int sh = BitmapWord<true>::kShift;
+    uint32_t i = uint32_t(w >> sh) - m.base;
     i = i < m.nwords ? i : m.nwords;
     const uint32_t x = uint32_t(m.words[i]);
-    const uint32_t bit = uint32_t(w) & 31u;
+    const uint32_t bit = uint32_t(w) & BitmapWord<true>::kBits;
     if (!((x >> bit) & 1u)) return 0;  // the guard word is zero: i < nwords below
-    atomicAdd(&m.mcnt[m.idx[i] + __popc(x & ((1u << bit) - 1u))], 1);
+    const uint32_t first = XT_PV_PACKED ? (x >> 16) : uint32_t(m.idx[i]);
+    atomicAdd(&m.mcnt[first + __popc(x & ((1u << bit) - 1u))], 1);
   } else if (!hash_test<true>(m, w)) {
     return 0;
   }
@@ -760,7 +788,8 @@ __device__ __forceinline__ int probe_pair_counted(const int4 a, const int4 b, co
 // warps of a CTA task) or taken in order (cursor null); returns this lane's
 // hits. Per-vertex mode (MODE 1) credits each record's hits to its owner u;
 // per-edge mode (MODE 2) credits them to the record's own edge u->v and each
-// hit to the edge u->w at the candidate's column.
+// hit to the edge u->w at the candidate's column, both at padded column
+// positions (no per-record load of the tail or its row offsets).
 // PF: a bulk L2 prefetch of each record's suffix one batch ahead (one per
 // record, by the record's first lane): it pays where little of the graph is
 // re-read from L2 (the 4,096-graph batch: 40.3 -> 34.6 ms) and costs issue
@@ -780,7 +809,7 @@ __device__ __forceinline__ int64_t stream_kind(const InRec *__restrict__ rec, co
   const int32_t nrec = int32_t(kend - k0);
   const int4 sent = make_int4(kSentinel, kSentinel, kSentinel, kSentinel);
   rec += k0;
-  if (PV) rec_u += k0;
+  if (MODE == 1) rec_u += k0;
   int32_t seq = 0;
   auto claim = [&]() -> int32_t {
     if (!cursor) {
@@ -794,11 +823,11 @@ __device__ __forceinline__ int64_t stream_kind(const InRec *__restrict__ rec, co
     // task (a cluster's CTAs take every kCluster-th batch each)
     return __shfl_sync(0xffffffffu, c, 0) * bstride + boff * bsz;
   };
-  // a record as {pair, lw, 0, u} (u only in the per-vertex and per-edge modes)
+  // a record as {pair, lw, 0, u} (u only in the per-vertex mode)
   auto fetch = [&](int32_t base) -> int4 {
     const int32_t r = base + j;
     const uint2 x = r < nrec ? __ldg(reinterpret_cast<const uint2 *>(rec) + r) : make_uint2(0u, 0u);
-    return make_int4(int(x.x), int(x.y), 0, (PV && r < nrec) ? __ldg(rec_u + r) : -1);
+    return make_int4(int(x.x), int(x.y), 0, (MODE == 1 && r < nrec) ? __ldg(rec_u + r) : -1);
   };
   // records are loaded two batches ahead (an L2 prefetch of the next batch's
   // suffixes cost more instructions than the latency it hid: s24 38.5 ms
@@ -823,8 +852,6 @@ __device__ __forceinline__ int64_t stream_kind(const InRec *__restrict__ rec, co
     const int32_t np = len > 0 ? (int32_t(s & 7) + len + 7) >> 3 : 0;  // pairs of the suffix
     const int32_t cnt = np > k ? ((np - k + S - 1) >> lg_s) : 0;            // this lane's
     const int32_t steps = int32_t(__reduce_max_sync(0xffffffffu, uint32_t(cnt)));
-    // per-edge mode: column positions of the unpadded CSR, row u's shift
-    const int64_t dpos = (MODE == 2 && np > 0) ? off[r4.w] - poff[r4.w] : 0;
     int64_t P = (s >> 3) + k;
     int4 xa = sent, xb = sent;
     if (cnt > 0) load_pair(colp, P, xa, xb);
@@ -836,7 +863,7 @@ __device__ __forceinline__ int64_t stream_kind(const InRec *__restrict__ rec, co
       const int64_t pa = P;  // the pair in a, b
       P += S;
       if (it + 1 < cnt) load_pair(colp, P, xa, xb);  // next step's pair in flight during the probes
-      if (PV) h += probe_pair_counted<MODE, KIND>(a, b, m, es, 8 * pa + dpos);
+      if (PV) h += probe_pair_counted<MODE, KIND>(a, b, m, es, 8 * pa);
       else h += probe_pair<false, KIND>(a, b, m);
     }
     (void)steps;
@@ -855,7 +882,7 @@ __device__ __forceinline__ int64_t stream_kind(const InRec *__restrict__ rec, co
         xa = sent;
         xb = sent;
       }
-      if (PV) h += probe_pair_counted<MODE, KIND>(a, b, m, es, 8 * pa + dpos);
+      if (PV) h += probe_pair_counted<MODE, KIND>(a, b, m, es, 8 * pa);
       else h += probe_pair<false, KIND>(a, b, m);
     }
 #endif
@@ -866,7 +893,7 @@ __device__ __forceinline__ int64_t stream_kind(const InRec *__restrict__ rec, co
         if (o < S) hr += __shfl_down_sync(0xffffffffu, hr, o, S);
       if (MODE == 1 && k == 0 && hr && r4.w >= 0)
         atomicAdd(reinterpret_cast<unsigned long long *>(&pv[r4.w]), (unsigned long long)hr);
-      if (MODE == 2 && k == 0 && hr) atomicAdd(&es[s - 1 + dpos], unsigned(hr));  // the edge u->v
+      if (MODE == 2 && k == 0 && hr) atomicAdd(&es[s - 1], unsigned(hr));  // the edge u->v
     }
     hits += h;
     kb = nkb;
@@ -911,6 +938,7 @@ struct CountArgs {
   const Task *ct;  // cluster tasks
   int64_t n_ct;
   int lane_merge;  // lane tasks: members found by a two-pointer merge (1) or binary search (0)
+  int64_t stride;  // task lists hold every stride-th task of the schedule (a shard of it), else 1
   unsigned long long *cursor;     // [0] CTA, [1] warp, [2] lane task cursors
   unsigned long long *global;     // the total
   int64_t *pv;                    // per-vertex counts (per-vertex mode)
@@ -981,9 +1009,11 @@ constexpr int kStageCta = kBlockDmax + 8;   // members, from r0 rounded down to 
 constexpr int kStageWarp = kWarpDmax + 8;
 constexpr int kStageInts = (kStageCta > kWarps * kStageWarp) ? kStageCta : kWarps * kStageWarp;
 
-// the next task from `cursor` (warp-uniform); nrec = -1 when none is left
+// the next task from `cursor` (warp-uniform); nrec = -1 when none is left.
+// A shard's list is every stride-th task of the schedule's (tasks points at
+// its first, n counts its own).
 __device__ __forceinline__ Task claim_task(unsigned long long *cursor, const Task *__restrict__ tasks, int64_t n,
-                                           int lane) {
+                                           int64_t stride, int lane) {
   unsigned long long i = 0;
   if (lane == 0) i = atomicAdd(cursor, 1ull);
   i = __shfl_sync(0xffffffffu, i, 0);
@@ -994,7 +1024,7 @@ __device__ __forceinline__ Task claim_task(unsigned long long *cursor, const Tas
     t.nrec = -1;
     return t;
   }
-  return tasks[i];
+  return tasks[int64_t(i) * stride];
 }
 
 // one warp: the task's records to L2, from the 16-byte boundary at or below
@@ -1085,7 +1115,7 @@ __global__ void __launch_bounds__(kThreads, MODE == 0 ? kMinBlocks : 3) k_count(
   __syncthreads();
   uint32_t stage_parity = 0;
   if (warp == 0) {
-    const Task t0 = claim_task(&cursor[0], a.bt, a.n_bt, lane);
+    const Task t0 = claim_task(&cursor[0], a.bt, a.n_bt, a.stride, lane);
     const int so = stage_task_bulk(s_stage, &s_stage_bar, col, rec, t0, lane);
     if (lane == 0) {
       s_task[0] = t0;
@@ -1133,7 +1163,7 @@ __global__ void __launch_bounds__(kThreads, MODE == 0 ? kMinBlocks : 3) k_count(
       __syncthreads();
     }
     if (warp == 0) {  // stage is free again: bring in the next task
-      const Task tn = claim_task(&cursor[0], a.bt, a.n_bt, lane);
+      const Task tn = claim_task(&cursor[0], a.bt, a.n_bt, a.stride, lane);
       const int so = stage_task_bulk(s_stage, &s_stage_bar, col, rec, tn, lane);
       if (lane == 0) {
         s_task[cur ^ 1] = tn;
@@ -1158,9 +1188,10 @@ __global__ void __launch_bounds__(kThreads, MODE == 0 ? kMinBlocks : 3) k_count(
       for (int i = tid; i < t.nmem; i += kThreads)
         if (bmcnt[i]) atomicAdd(reinterpret_cast<unsigned long long *>(&pv[col[t.r0 + i]]), (unsigned long long)bmcnt[i]);
     }
-    if (MODE == 2) {
+    if (MODE == 2) {  // the counts sit at padded positions: this part's start in row v
+      const int64_t pr0 = a.poff[t.v] + (t.r0 - off[t.v]);
       for (int i = tid; i < t.nmem; i += kThreads)
-        if (bmcnt[i]) atomicAdd(&es[t.r0 + i], unsigned(bmcnt[i]));
+        if (bmcnt[i]) atomicAdd(&es[pr0 + i], unsigned(bmcnt[i]));
     }
     if (PV) __syncthreads();
   }
@@ -1173,7 +1204,7 @@ __global__ void __launch_bounds__(kThreads, MODE == 0 ? kMinBlocks : 3) k_count(
     // the whole 1,024-word slice per task.
     int32_t *wstage = s_stage + warp * kStageWarp;
     int32_t *words = bwords + warp * kWarpWords;
-    Task t = claim_task(&cursor[1], a.wt, a.n_wt, lane);
+    Task t = claim_task(&cursor[1], a.wt, a.n_wt, a.stride, lane);
     int so = stage_task(wstage, col, rec, t, lane);
     zero_words(words, kWarpWords, lane, 32);
     while (true) {
@@ -1187,7 +1218,7 @@ __global__ void __launch_bounds__(kThreads, MODE == 0 ? kMinBlocks : 3) k_count(
       m.mcnt = nullptr;
       const bool ok = warp_set_build(m, mem, t.nmem, kWarpWords, a.bitmap_bits, a.cuckoo_iters, lane);
       __syncwarp();
-      const Task tn = claim_task(&cursor[1], a.wt, a.n_wt, lane);  // read after the stream
+      const Task tn = claim_task(&cursor[1], a.wt, a.n_wt, a.stride, lane);  // read after the stream
       int64_t h;
       if (ok) {
         h = stream_suffixes<MODE, PF>(rec, a.rec_u, a.colp, t.k0, t.k0 + t.nrec, t.lg_s, nullptr, m, pv, es, off, a.poff, lane);
@@ -1215,7 +1246,7 @@ __global__ void __launch_bounds__(kThreads, MODE == 0 ? kMinBlocks : 3) k_count(
     }
   } else {
     int32_t *wstage = s_stage + warp * kStageWarp;
-    Task t = claim_task(&cursor[1], a.wt, a.n_wt, lane);
+    Task t = claim_task(&cursor[1], a.wt, a.n_wt, a.stride, lane);
     int so = stage_task(wstage, col, rec, t, lane);
     while (true) {
       cp_async_wait_all();
@@ -1231,7 +1262,7 @@ __global__ void __launch_bounds__(kThreads, MODE == 0 ? kMinBlocks : 3) k_count(
       __syncwarp();
       for (int i = lane; i < t.nmem; i += 32) members_insert_at<PV>(m, mem, i);
       __syncwarp();
-      const Task tn = claim_task(&cursor[1], a.wt, a.n_wt, lane);  // read after the stream
+      const Task tn = claim_task(&cursor[1], a.wt, a.n_wt, a.stride, lane);  // read after the stream
       int64_t h = stream_suffixes<MODE, PF>(rec, a.rec_u, a.colp, t.k0, t.k0 + t.nrec, t.lg_s, nullptr, m, pv, es, off, a.poff,
                                         lane);
       acc += h;
@@ -1246,8 +1277,9 @@ __global__ void __launch_bounds__(kThreads, MODE == 0 ? kMinBlocks : 3) k_count(
       }
       if (MODE == 2) {
         __syncwarp();
+        const int64_t pr0 = a.poff[t.v] + (t.r0 - off[t.v]);
         for (int i = lane; i < t.nmem; i += 32)
-          if (m.mcnt[i]) atomicAdd(&es[t.r0 + i], unsigned(m.mcnt[i]));
+          if (m.mcnt[i]) atomicAdd(&es[pr0 + i], unsigned(m.mcnt[i]));
       }
       __syncwarp();
       so = stage_task(wstage, col, rec, tn, lane);
@@ -1275,9 +1307,11 @@ __global__ void __launch_bounds__(kThreads, MODE == 0 ? kMinBlocks : 3) k_count(
       if (int64_t(base) >= a.n_tt) break;
       const int64_t i = int64_t(base) + lane;
       if (i >= a.n_tt) continue;
-      const int32_t v = a.tt[i];
+      const int32_t v = a.tt[i * a.stride];
       const int64_t r0 = off[v], r1 = off[v + 1];
       const int32_t lo = col[r0], hi = col[r1 - 1];
+      // per-edge mode: the counts sit at padded positions; row v's shift
+      const int64_t vshift = MODE == 2 ? a.poff[v] - r0 : 0;
       // a head of at most kLaneRegs members (not in the per-edge mode, which
       // needs each hit's position) keeps them in registers: a candidate is
       // then kLaneRegs compares, no dependent load
@@ -1290,9 +1324,7 @@ __global__ void __launch_bounds__(kThreads, MODE == 0 ? kMinBlocks : 3) k_count(
       for (int64_t k = ioff[v]; k < ioff[v + 1]; k++) {
         const InRec r = rec[k];
         const int64_t rs = rec_s(r), re = rs + rec_len(r);
-        const int32_t ru = MODE != 0 ? a.rec_u[k] : 0;
-        // per-edge mode: row u's shift from padded to unpadded positions
-        const int64_t dpos = MODE == 2 ? off[ru] - a.poff[ru] : 0;
+        const int32_t ru = MODE == 1 ? a.rec_u[k] : 0;
         int64_t b = r0;  // members below b are below every remaining candidate
         int32_t hu = 0;
         for (int64_t p = rs; p < re; p++) {
@@ -1323,15 +1355,15 @@ __global__ void __launch_bounds__(kThreads, MODE == 0 ? kMinBlocks : 3) k_count(
             hu++;
             if (MODE == 1) atomicAdd(reinterpret_cast<unsigned long long *>(&pv[w]), 1ull);
             if (MODE == 2) {
-              atomicAdd(&es[p + dpos], 1u);  // the edge u->w
-              atomicAdd(&es[x], 1u);  // the edge v->w
+              atomicAdd(&es[p], 1u);  // the edge u->w
+              atomicAdd(&es[x + vshift], 1u);  // the edge v->w
             }
             if (!regs) b = x + 1;
           }
         }
         hv += hu;
         if (MODE == 1 && hu) atomicAdd(reinterpret_cast<unsigned long long *>(&pv[ru]), (unsigned long long)hu);
-        if (MODE == 2 && hu) atomicAdd(&es[rs - 1 + dpos], unsigned(hu));  // the edge u->v
+        if (MODE == 2 && hu) atomicAdd(&es[rs - 1], unsigned(hu));  // the edge u->v
       }
       acc += hv;
       if (hv) {
@@ -1405,7 +1437,7 @@ __global__ void __cluster_dims__(kCluster, 1, 1) __launch_bounds__(kThreads, XT_
       const unsigned long long i = atomicAdd(&a.cursor[3], 1ull);
       Task t;
       if (int64_t(i) < a.n_ct) {
-        t = a.ct[i];
+        t = a.ct[int64_t(i) * a.stride];
       } else {
         t.k0 = t.r0 = 0;
         t.v = t.nmem = t.lg_s = 0;
@@ -1765,12 +1797,34 @@ __global__ void k_rec_tails(const InRec *__restrict__ rec, int64_t ne, const int
   }
 }
 
-__global__ void k_widen(const unsigned int *__restrict__ in, int64_t n, int64_t *__restrict__ out) {
-  XT_GRID_STRIDE(i, n) out[i] = int64_t(in[i]);
+// per-edge counts from padded positions (row u at poff[u]) to the out-CSR's
+// (row u at off[u]), widened to 64 bits: a warp per row
+__global__ void k_es_unpad(const unsigned int *__restrict__ esp, const int64_t *__restrict__ off,
+                           const int64_t *__restrict__ poff, int64_t nv, int64_t *__restrict__ out) {
+  const int lane = threadIdx.x & 31;
+  const int64_t nw = (int64_t(gridDim.x) * blockDim.x) >> 5;
+  for (int64_t u = (int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5; u < nv; u += nw) {
+    const int64_t r0 = off[u], len = off[u + 1] - r0, p0 = poff[u];
+    for (int64_t i = lane; i < len; i += 32) out[r0 + i] = int64_t(esp[p0 + i]);
+  }
 }
 
-xt_status count_graph(Graph *g, int64_t *d_global, int64_t *d_pv, int64_t *d_groups, int64_t *d_support) {
+// tasks of a list of n that fall to shard `shard` of nshards (every
+// nshards-th, from index shard on)
+static int64_t shard_len(int64_t n, int shard, int nshards) {
+  return n > shard ? (n - shard + nshards - 1) / nshards : 0;
+}
+// the shard's first task of a list of n (null when the shard has none)
+template <typename T>
+static const T *shard_first(const T *p, int64_t n, int shard) {
+  return p && n > shard ? p + shard : nullptr;
+}
+
+xt_status count_graph(Graph *g, int64_t *d_global, int64_t *d_pv, int64_t *d_groups, int64_t *d_support, int shard,
+                      int nshards) {
   Ctx *c = g->ctx;
+  if (nshards < 1 || shard < 0 || shard >= nshards)
+    return set_error(c, XT_ERR_INVALID, "shard must lie in [0, nshards) and nshards be at least 1");
   if (!g->plan) XT_TRY(make_plan(g));
   Plan *pl = g->plan;
   // pairs of columns are read with 32-byte vector loads
@@ -1783,12 +1837,16 @@ xt_status count_graph(Graph *g, int64_t *d_global, int64_t *d_pv, int64_t *d_gro
     XT_CUDA(c, cudaMemsetAsync(d_groups, 0, sizeof(int64_t) * g->n_groups, c->stream));
   }
   if (d_pv && d_support) return set_error(c, XT_ERR_INVALID, "per-vertex and per-edge counts are separate calls");
-  unsigned int *es = nullptr;  // per-edge counts, 32-bit while counting
+  // per-edge counts, 32-bit while counting, at the padded column positions
+  // (a record's suffix and its tail's edge are found there without the
+  // tail's row offsets)
+  unsigned int *es = nullptr;
   if (d_support) {
-    XT_TRY(dalloc_n(c, &es, size_t(g->ne > 0 ? g->ne : 1)));
-    XT_CUDA(c, cudaMemsetAsync(es, 0, sizeof(unsigned int) * size_t(g->ne > 0 ? g->ne : 1), c->stream));
+    const size_t n = size_t(g->colp_len > 0 ? g->colp_len : 1);
+    XT_TRY(dalloc_n(c, &es, n));
+    XT_CUDA(c, cudaMemsetAsync(es, 0, sizeof(unsigned int) * n, c->stream));
   }
-  if ((d_pv || d_support) && !g->d_irec_u && g->ne > 0) {  // the records' tails, once per graph
+  if (d_pv && !g->d_irec_u && g->ne > 0) {  // the records' tails, once per graph
     XT_TRY(dalloc_n(c, &g->d_irec_u, size_t(g->ne)));
     k_rec_tails<<<counted(c, grid_for(g->ne, 256, c->sm_count)), 256, 0, c->stream>>>(g->d_irec, g->ne, g->d_poff,
                                                                                       g->nv, g->d_irec_u);
@@ -1808,14 +1866,15 @@ xt_status count_graph(Graph *g, int64_t *d_global, int64_t *d_pv, int64_t *d_gro
   a.ioff = g->d_ioff;
   a.rec = g->d_irec;
   a.rec_u = g->d_irec_u;
-  a.bt = pl->d_bt;
-  a.n_bt = pl->n_btask;
-  a.wt = pl->d_wt;
-  a.n_wt = pl->n_wtask;
-  a.tt = pl->d_tt;
-  a.n_tt = pl->n_ttask;
-  a.ct = pl->d_ct;
-  a.n_ct = pl->n_ctask;
+  a.bt = shard_first(pl->d_bt, pl->n_btask, shard);
+  a.n_bt = shard_len(pl->n_btask, shard, nshards);
+  a.wt = shard_first(pl->d_wt, pl->n_wtask, shard);
+  a.n_wt = shard_len(pl->n_wtask, shard, nshards);
+  a.tt = shard_first(pl->d_tt, pl->n_ttask, shard);
+  a.n_tt = shard_len(pl->n_ttask, shard, nshards);
+  a.ct = shard_first(pl->d_ct, pl->n_ctask, shard);
+  a.n_ct = shard_len(pl->n_ctask, shard, nshards);
+  a.stride = nshards;
   a.lane_merge = g->lane_merge;
   a.cursor = pl->d_cursor;
   a.global = reinterpret_cast<unsigned long long *>(d_global);
@@ -1835,8 +1894,8 @@ xt_status count_graph(Graph *g, int64_t *d_global, int64_t *d_pv, int64_t *d_gro
       // cluster heads leave the CTA task list to the cluster tier
       CountArgs a0 = a;
       if (pl->n_ctask > 0) {
-        a0.bt = pl->d_bt0;
-        a0.n_bt = pl->n_btask0;
+        a0.bt = shard_first(pl->d_bt0, pl->n_btask0, shard);
+        a0.n_bt = shard_len(pl->n_btask0, shard, nshards);
       }
       if (g->prefetch_suffix > 0)
         k_count<0, true><<<counted(c, pl->grid_global), kThreads, count_smem_bytes(false), c->stream>>>(a0);
@@ -1847,7 +1906,8 @@ xt_status count_graph(Graph *g, int64_t *d_global, int64_t *d_pv, int64_t *d_gro
     }
   }
   if (d_support && g->ne > 0)
-    k_widen<<<counted(c, grid_for(g->ne, 256, c->sm_count)), 256, 0, c->stream>>>(es, g->ne, d_support);
+    k_es_unpad<<<counted(c, grid_for(g->nv * 32, 256, c->sm_count)), 256, 0, c->stream>>>(es, g->d_off, g->d_poff,
+                                                                                          g->nv, d_support);
   if (d_pv && g->d_perm)
     k_unpermute<<<counted(c, grid_for(g->nv, 256, c->sm_count)), 256, 0, c->stream>>>(pv_int, g->d_perm, g->nv, d_pv);
   cudaError_t e = cudaGetLastError();

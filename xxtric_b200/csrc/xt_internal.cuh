@@ -182,8 +182,11 @@ void free_plan(Graph *g);
 // d_groups: n_groups int64 per-group counts (graphs built as a batch), nullable.
 // d_support: ne int64, the triangles on each oriented edge in out-CSR order
 // (nullable; not together with d_pv).
+// shard / nshards: count only every nshards-th task of the schedule from
+// task `shard` on (each tier's list alike); the nshards shards' outputs sum
+// to the whole count's.
 xt_status count_graph(Graph *g, int64_t *d_global, int64_t *d_pv, int64_t *d_groups = nullptr,
-                      int64_t *d_support = nullptr);
+                      int64_t *d_support = nullptr, int shard = 0, int nshards = 1);
 // Synchronises the context stream and reports a count whose bounded device
 // wait gave up (XT_ERR_TIMEOUT); the synchronous count calls end with it.
 xt_status count_status(Ctx *c);
