@@ -474,21 +474,6 @@ struct Members {
 // Member-set kinds, one specialised streaming loop each.
 constexpr int kKindHash = 0, kKindBitmap = 1, kKindCuckoo = 2, kKindCluster = 3;
 
-// Per-vertex and per-edge modes: a bitmap word packs 16 member bits (low
-// half) with the index of the word's first member (high half), so a hit
-// finds its member's counter from the one word it loaded (the index plus the
-// popcount of the set bits below) instead of a second shared load from a
-// separate index array; the bitmap then spans half the ids a 32-bit word
-// does (2^17 for a CTA). 0 keeps 32 member bits a word and the index apart.
-#ifndef XT_PV_PACKED
-#define XT_PV_PACKED 0
-#endif
-template <bool PV>
-struct BitmapWord {
-  static constexpr int kShift = (PV && XT_PV_PACKED) ? 4 : 5;  // log2 of the ids a word covers
-  static constexpr uint32_t kBits = (1u << kShift) - 1u;
-};
-
 // Chooses the structure for members mem[0, n) (ascending) that fits `words`
 // words (a bitmap only while the members' id range is at most bitmap_bits)
 // and returns how many words must be cleared. In the per-vertex and
@@ -497,15 +482,14 @@ struct BitmapWord {
 // the index of the member in each used slot.
 template <bool PV>
 __device__ __forceinline__ int members_layout(Members &m, const int32_t *mem, int n, int words, int64_t bitmap_bits) {
-  constexpr int sh = BitmapWord<PV>::kShift;
   m.lo = mem[0];
   m.hi = mem[n - 1];
   m.cuckoo = false;
   const int64_t range = int64_t(m.hi) - int64_t(m.lo) + 1;
-  const int64_t nw = int64_t(m.hi >> sh) - int64_t(m.lo >> sh) + 1;
+  const int64_t nw = int64_t(m.hi >> 5) - int64_t(m.lo >> 5) + 1;
   m.bitmap = nw + 1 <= int64_t(words) && range <= bitmap_bits;
   if (m.bitmap) {
-    m.base = uint32_t(m.lo >> sh);
+    m.base = uint32_t(m.lo >> 5);
     m.nwords = uint32_t(nw);
     m.mask = 0;
     m.shift = 0;
@@ -530,17 +514,9 @@ template <bool PV>
 __device__ __forceinline__ void members_insert_at(const Members &m, const int32_t *mem, int i) {
   const int32_t x = mem[i];
   if (m.bitmap) {
-    constexpr int sh = BitmapWord<PV>::kShift;
-    const uint32_t wd = uint32_t(x >> sh) - m.base;
-    const bool first = PV && (i == 0 || uint32_t(mem[i - 1] >> sh) - m.base != wd);
-    if (PV && XT_PV_PACKED) {
-      // the word's first member also writes its index into the high half
-      atomicOr(reinterpret_cast<unsigned int *>(&m.words[wd]),
-               (1u << (uint32_t(x) & BitmapWord<PV>::kBits)) | (first ? uint32_t(i) << 16 : 0u));
-    } else {
-      atomicOr(reinterpret_cast<unsigned int *>(&m.words[wd]), 1u << (x & 31));
-      if (first) m.idx[wd] = uint16_t(i);
-    }
+    const uint32_t wd = uint32_t(x >> 5) - m.base;
+    atomicOr(reinterpret_cast<unsigned int *>(&m.words[wd]), 1u << (x & 31));
+    if (PV && (i == 0 || uint32_t(mem[i - 1] >> 5) - m.base != wd)) m.idx[wd] = uint16_t(i);
   } else {
     const uint32_t slot = hash_insert(m.words, m.mask, m.shift, x);
     if (PV) m.idx[slot] = uint16_t(i);
@@ -746,27 +722,24 @@ __device__ __forceinline__ int probe_one(const Members &m, int32_t w, unsigned i
     // below; idx of a word without members, or of the guard word, is stale
     // and then unused) and the increment is predicated on the hit. R-MAT s24
     // 63.8 -> 60.4 ms; the per-edge mode keeps its branch (its predicated
-    // global increments measured 97.0 -> 98.8 ms)
-    constexpr int sh = BitmapWord<true>::kShift;
-    uint32_t i = uint32_t(w >> sh) - m.base;
+    // global increments measured 97.0 -> 98.8 ms, and its member counter
+    // alone predicated 94.0 -> 95.5 ms)
+    uint32_t i = uint32_t(w >> 5) - m.base;
     i = i < m.nwords ? i : m.nwords;
     const uint32_t x = uint32_t(m.words[i]);
-    const uint32_t bit = uint32_t(w) & BitmapWord<true>::kBits;
+    const uint32_t bit = uint32_t(w) & 31u;
     const uint32_t hit = (x >> bit) & 1u;
-    const uint32_t first = XT_PV_PACKED ? (x >> 16) : uint32_t(m.idx[i]);
-    const uint32_t k = first + uint32_t(__popc(x & ((1u << bit) - 1u)));
+    const uint32_t k = uint32_t(m.idx[i]) + uint32_t(__popc(x & ((1u << bit) - 1u)));
     red_shared_add1_if(smem_u32(m.mcnt) + 4u * k, hit);
     return int(hit);
   }
   if (KIND == kKindBitmap) {
-    constexpr int sh = BitmapWord<true>::kShift;
-    uint32_t i = uint32_t(w >> sh) - m.base;
+    uint32_t i = uint32_t(w >> 5) - m.base;
     i = i < m.nwords ? i : m.nwords;
     const uint32_t x = uint32_t(m.words[i]);
-    const uint32_t bit = uint32_t(w) & BitmapWord<true>::kBits;
+    const uint32_t bit = uint32_t(w) & 31u;
     if (!((x >> bit) & 1u)) return 0;  // the guard word is zero: i < nwords below
-    const uint32_t first = XT_PV_PACKED ? (x >> 16) : uint32_t(m.idx[i]);
-    atomicAdd(&m.mcnt[first + __popc(x & ((1u << bit) - 1u))], 1);
+    atomicAdd(&m.mcnt[m.idx[i] + __popc(x & ((1u << bit) - 1u))], 1);
   } else if (!hash_test<true>(m, w)) {
     return 0;
   }
