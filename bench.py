@@ -462,6 +462,16 @@ def run_xtric(args) -> None:
         sup = torch.zeros(max(1, info["n_edges"]), dtype=torch.int64, device="cuda")
         extra["per_edge_ms"] = 1e3 * time_counts(g, stream, torch, 3, support=sup)
         del sup
+        # the reference's own precedence (vertex ids) on the same graph
+        gi = ctx.graph_from_device_edges(n, ne, src, dst, xt.ORIENT_ID)
+        if gi.count() != counts[0]:
+            raise RuntimeError("the id orientation's count differs from the degree orientation's")
+        extra["id_orientation_ms"] = 1e3 * time_counts(gi, stream, torch, 1)
+        ii = gi.info()
+        extra["id_orientation_max_out_degree"] = ii["max_out_degree"]
+        extra["candidates"] = info["stream_work"]
+        extra["id_orientation_candidates"] = ii["stream_work"]
+        gi.free()
     if args.workload == "chunglu":
         # the per-vertex kernel and the reference's id orientation on the same graph
         pv = torch.zeros(n, dtype=torch.int64, device="cuda")

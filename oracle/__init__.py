@@ -21,7 +21,8 @@ REF_DIR = os.path.join(HERE, "_ref")
 REF_TRIC = os.path.join(REF_DIR, "tric")
 REF_TRIC_OMP = os.path.join(REF_DIR, "tric_omp")
 REF_TRIC_GPU = os.path.join(REF_DIR, "tric_gpu")
-REFERENCE_TREE = "/root/reference"
+# the read-only reference checkout the recipe compiles from (override: XT_REFERENCE_TREE)
+REFERENCE_TREE = os.environ.get("XT_REFERENCE_TREE", "/root/reference")
 
 _i64p = np.ctypeslib.ndpointer(np.int64, flags="C")
 _u64p = np.ctypeslib.ndpointer(np.uint64, flags="C")

@@ -87,6 +87,11 @@ def test_scale24_properties(ctx):
     assert pv.sum() == 3 * t
     assert inf["n_edges"] == 260453894
     check_large("rmat24", t, pv, inf["n_edges"])
+    # the reference's own precedence (u < v < w by input id, xxtric.hpp:165):
+    # hubs keep up to ~200k higher neighbours, counted as CTA parts
+    gi = ctx.graph_from_device_edges(n, len(s), s, d, xt.ORIENT_ID)
+    assert gi.count() == t
+    gi.free()
     # relabel every vertex by a random permutation: same total, permuted counts
     perm = torch.randperm(n, device="cuda", dtype=torch.int64).to(torch.int32)
     ps, pd = perm[s.long()], perm[d.long()]
