@@ -278,13 +278,24 @@ xt_status xt_graph_set_cluster(xt_graph *g, int on);
  * where the plan has lane tasks. Counts are identical. Re-captures a
  * captured graph. */
 xt_status xt_graph_set_lane_intersect(xt_graph *g, int kind);
+/* No counterpart in the reference (its kernels take vertices by grid
+ * index): warp tasks, and lane tasks in groups of 32 heads, are taken from
+ * their global cursor `claim` at a time (1..64; 0, the default: 4 for a
+ * graph built as a batch, 1 otherwise). One atomic on one address per task
+ * limits schedules of many small tasks (the 4,096-graph batch: 38.2 ms a
+ * count with 1, 30.4 ms with 4); larger blocks leave a longer tail on
+ * graphs whose warp tasks are fewer (R-MAT scale 22: 4.69 ms with 1, 4.79
+ * with 4). The autotuner tries 1, 4 and 16. Counts are identical.
+ * Re-captures a captured graph. */
+xt_status xt_graph_set_claim(xt_graph *g, int claim);
 /* Test hook, no counterpart in the reference: caps the eviction chain of the
  * global count's cuckoo member sets at `iters` steps (negative: the default
  * of 64). With 0 or 1 nearly every hashed set falls back to linear probing,
  * which lets a test reach that path; counts are unchanged. */
 xt_status xt_graph_debug_cuckoo_iters(xt_graph *g, int iters);
 /* Autotuner: a coordinate search of the three thresholds, then the suffix
- * prefetch on and off, timing `reps` counts each, keeping the fastest; with
+ * prefetch on and off, the lane tier's merge and the claim block
+ * (xt_graph_set_claim), timing `reps` counts each, keeping the fastest; with
  * cache_path it first looks the
  * (GPU, graph class) key up in that text file and appends new results.
  * A JSON report of the trials goes to report (nullable). */

@@ -491,6 +491,53 @@ def test_each_tier_alone_vs_oracle(ctx, torch_cuda, kind):
             g.free()
 
 
+@pytest.mark.parametrize("kind", ["rmat", "chunglu"])
+def test_claim_blocks_vs_oracle(ctx, torch_cuda, kind):
+    # warp tasks (and groups of 32 lane heads) taken 1, 3, 4, 16 or 64 per
+    # atomic on their cursor: the same counts on every tier, in every mode,
+    # with shards (strided lists) and through a captured replay
+    torch = torch_cuda
+    if kind == "rmat":
+        n, m = 1 << 14, 16 << 14
+        s = torch.empty(m, dtype=torch.int32, device="cuda")
+        d = torch.empty_like(s)
+        ctx.gen_rmat(14, m, 11, s, d)
+    else:
+        n = 1 << 15
+        cdf, m = xt.chunglu_cdf(n, 2.1, 24.0, 8192.0)
+        s = torch.empty(m, dtype=torch.int32, device="cuda")
+        d = torch.empty_like(s)
+        ctx.gen_chunglu(cdf, m, 13, s, d)
+    off, tails = oracle.canon_csr(n, s.cpu().numpy().astype(np.int64), d.cpu().numpy().astype(np.int64))
+    expect, opv = oracle.count_merge(off, tails, per_vertex=True)
+    g = ctx.graph_from_device_edges(n, m, s, d, xt.ORIENT_DEGREE)
+    try:
+        _, ref_sup = g.count_edges()
+        dg = torch.zeros(1, dtype=torch.int64, device="cuda")
+        for lane_work, warp_work in ((1 << 40, 0), (0, 1 << 40), (-1, -1)):
+            g.set_tiers(lane_work, warp_work)
+            for claim in (1, 3, 4, 16, 64):
+                g.set_claim(claim)
+                t, pv = g.count(per_vertex=True)
+                assert t == expect and (pv == opv).all(), (lane_work, warp_work, claim)
+                t2, sup = g.count_edges()
+                assert t2 == expect and (sup == ref_sup).all(), (lane_work, warp_work, claim)
+                tot = 0
+                for k in range(3):
+                    g.count_shard_async(k, 3, dg)
+                    ctx.synchronize()
+                    tot += int(dg.item())
+                assert tot == expect, (lane_work, warp_work, claim, "shards")
+        g.set_claim(0)
+        g.capture()
+        g.set_claim(16)  # re-captures
+        assert g.count_groups()[0] == expect
+        with pytest.raises(xt.XtError):
+            g.set_claim(65)
+    finally:
+        g.free()
+
+
 def oracle_support_of(off, tails, a, b):
     """The oracle's support of undirected edges (a[i], b[i]), a < b."""
     es = oracle.edge_support(off, tails)

@@ -99,6 +99,7 @@ _proto("xt_graph_set_tiers", _int, _vp, _i64, _i64)
 _proto("xt_graph_set_prefetch", _int, _vp, _int)
 _proto("xt_graph_set_cluster", _int, _vp, _int)
 _proto("xt_graph_set_lane_intersect", _int, _vp, _int)
+_proto("xt_graph_set_claim", _int, _vp, _int)
 _proto("xt_gen_rgg", _int, _vp, _i64, _int, _dbl, _i64, _P(_i64), _vp, _vp)
 _proto("xt_graph_from_vite", _int, _vp, ctypes.c_char_p, _int, _int, _int, _P(_vp))
 _proto("xt_graph_from_rgg", _int, _vp, _i64, _int, _dbl, _int, _P(_vp))
@@ -132,7 +133,7 @@ EXPORTED = ["xt_strerror", "xt_last_error", "xt_open", "xt_close", "xt_set_strea
             "xt_graph_get_csr", "xt_graph_free", "xt_count", "xt_count_async", "xt_count_edges", "xt_count_edges_async",
             "xt_count_shard_async", "xt_count_edges_shard_async", "xt_count_device",
             "xt_count_device_static", "xt_graph_from_batch", "xt_graph_from_device_batch", "xt_graph_groups",
-            "xt_count_groups", "xt_count_groups_async", "xt_batch_count", "xt_graph_capture", "xt_graph_set_tuning", "xt_graph_set_tiers", "xt_graph_set_prefetch", "xt_graph_set_cluster", "xt_graph_set_lane_intersect",
+            "xt_count_groups", "xt_count_groups_async", "xt_batch_count", "xt_graph_capture", "xt_graph_set_tuning", "xt_graph_set_tiers", "xt_graph_set_prefetch", "xt_graph_set_cluster", "xt_graph_set_lane_intersect", "xt_graph_set_claim",
             "xt_graph_debug_cuckoo_iters",
             "xt_mem_stats", "xt_serve_estimate", "xt_serve_open", "xt_serve_submit", "xt_serve_poll",
             "xt_serve_wait", "xt_serve_get_stats", "xt_serve_close", "xt_serve_batches", "xt_tsv_read", "xt_tsv_write",
@@ -559,6 +560,10 @@ class DeviceGraph:
     def set_lane_intersect(self, kind: int) -> None:
         """Lane tier: members found by binary search (LANE_BSEARCH, default) or a two-pointer merge (LANE_MERGE)."""
         _check(_L.xt_graph_set_lane_intersect(self._h, int(kind)), "xt_graph_set_lane_intersect", self.ctx)
+
+    def set_claim(self, claim: int) -> None:
+        """Warp tasks (and groups of 32 lane tasks) taken per atomic on their cursor: 1..64, 0 automatic."""
+        _check(_L.xt_graph_set_claim(self._h, int(claim)), "xt_graph_set_claim", self.ctx)
 
     def set_cluster(self, on: bool) -> None:
         """Global count: heads over a CTA's member set on thread-block clusters, or CTA parts (default)."""

@@ -462,6 +462,12 @@ static xt_status set_lane_merge(Graph *g, int on) {
   return XT_OK;
 }
 
+static xt_status set_claim(Graph *g, int claim) {
+  g->claim_block = claim;
+  if (g->exec) XT_TRY(capture_count(g));  // the launch's arguments inside the captured graph change
+  return XT_OK;
+}
+
 static xt_status set_cluster(Graph *g, int on) {
   const bool was_captured = g->exec != nullptr;
   g->cluster_tier = on ? 1 : 0;
@@ -519,7 +525,7 @@ static std::string tune_key(const Graph *g) {
   };
   char buf[512];
   // the schedule revision keeps timings of an older kernel from being reused
-  snprintf(buf, sizeof buf, "sched9|%s|sm%d|orient%d|nv2^%d|ne2^%d|work2^%d|groups%lld", p.name, p.multiProcessorCount,
+  snprintf(buf, sizeof buf, "sched10|%s|sm%d|orient%d|nv2^%d|ne2^%d|work2^%d|groups%lld", p.name, p.multiProcessorCount,
            g->orient, lg(g->nv), lg(g->ne), lg(g->stream_work), (long long)g->n_groups);
   for (char *q = buf; *q; q++)
     if (*q == ' ') *q = '_';
@@ -529,9 +535,10 @@ static std::string tune_key(const Graph *g) {
 // Coordinate search over the schedule: the CTA task size, the warp-task work
 // limit and the largest member id range kept as a bitmap (beyond it the hash
 // is used), each swept with the others held, the best kept; then the bulk
-// suffix prefetch on and off. Results are cached per (GPU, graph class) in a
-// text file when a path is given, so a second run of the same class of graph
-// skips the search.
+// suffix prefetch on and off, the lane tier's merge, and the warp tasks
+// claimed per atomic (1, 4, 16). Results are cached per (GPU, graph class)
+// in a text file when a path is given, so a second run of the same class of
+// graph skips the search.
 xt_status autotune(Graph *g, int reps, const char *cache_path, std::string *report) {
   const std::string key = tune_key(g);
   if (cache_path && *cache_path) {
@@ -540,13 +547,15 @@ xt_status autotune(Graph *g, int reps, const char *cache_path, std::string *repo
       while (fgets(line, sizeof line, f)) {
         char k[300];
         long long bw, ww, bb;
-        int pf, lm;
+        int pf, lm, cl;
         double ms;
-        if (sscanf(line, "%299s %lld %lld %lld %d %d %lf", k, &bw, &ww, &bb, &pf, &lm, &ms) == 7 && key == k) {
+        if (sscanf(line, "%299s %lld %lld %lld %d %d %d %lf", k, &bw, &ww, &bb, &pf, &lm, &cl, &ms) == 8 &&
+            key == k) {
           fclose(f);
           if (report) *report = "{\"cached\": true, \"key\": \"" + key + "\"}";
           XT_TRY(set_prefetch(g, pf));
           XT_TRY(set_lane_merge(g, lm));
+          XT_TRY(set_claim(g, cl));
           return set_tuning(g, bw, ww, bb);
         }
       }
@@ -557,6 +566,7 @@ xt_status autotune(Graph *g, int reps, const char *cache_path, std::string *repo
   double best_ms = 0;
   XT_TRY(set_prefetch(g, 0));
   XT_TRY(set_lane_merge(g, 0));
+  XT_TRY(set_claim(g, 0));
   XT_TRY(set_tuning(g, 0, 0, 0));
   XT_TRY(time_count(g, reps, &best_ms));
   std::string rep = "{\"key\": \"" + key + "\", \"trials\": [";
@@ -613,16 +623,31 @@ xt_status autotune(Graph *g, int reps, const char *cache_path, std::string *repo
     }
     XT_TRY(set_lane_merge(g, best_lm));
   }
+  // warp (and lane) tasks claimed per atomic on their cursor: 0 is the
+  // automatic choice timed above
+  int best_cl = 0;
+  for (int cl : {1, 4, 16}) {
+    XT_TRY(set_claim(g, cl));
+    double ms = 0;
+    XT_TRY(time_count(g, reps, &ms));
+    snprintf(buf, sizeof buf, ", {\"claim\": %d, \"ms\": %.4f}", cl, ms);
+    rep += buf;
+    if (ms < best_ms) {
+      best_ms = ms;
+      best_cl = cl;
+    }
+  }
+  XT_TRY(set_claim(g, best_cl));
   snprintf(buf, sizeof buf,
            "], \"best\": {\"block_work\": %lld, \"warp_work\": %lld, \"bitmap_bits\": %lld, \"prefetch\": %d, "
-           "\"lane_merge\": %d, \"ms\": %.4f}}",
-           (long long)best[0], (long long)best[1], (long long)best[2], best_pf, best_lm, best_ms);
+           "\"lane_merge\": %d, \"claim\": %d, \"ms\": %.4f}}",
+           (long long)best[0], (long long)best[1], (long long)best[2], best_pf, best_lm, best_cl, best_ms);
   rep += buf;
   if (report) *report = rep;
   if (cache_path && *cache_path) {
     if (FILE *f = fopen(cache_path, "a")) {
-      fprintf(f, "%s %lld %lld %lld %d %d %.4f\n", key.c_str(), (long long)best[0], (long long)best[1],
-              (long long)best[2], best_pf, best_lm, best_ms);
+      fprintf(f, "%s %lld %lld %lld %d %d %d %.4f\n", key.c_str(), (long long)best[0], (long long)best[1],
+              (long long)best[2], best_pf, best_lm, best_cl, best_ms);
       fclose(f);
     }
   }
@@ -793,6 +818,12 @@ xt_status xt_graph_set_lane_intersect(xt_graph *gr, int kind) {
   if (!gr || !gr->g.ctx || (kind != XT_LANE_BSEARCH && kind != XT_LANE_MERGE)) return XT_ERR_INVALID;
   cudaSetDevice(gr->g.ctx->device);
   return set_lane_merge(&gr->g, kind == XT_LANE_MERGE);
+}
+
+xt_status xt_graph_set_claim(xt_graph *gr, int claim) {
+  if (!gr || !gr->g.ctx || claim < 0 || claim > 64) return XT_ERR_INVALID;
+  cudaSetDevice(gr->g.ctx->device);
+  return set_claim(&gr->g, claim);
 }
 
 xt_status xt_graph_set_cluster(xt_graph *gr, int on) {

@@ -912,6 +912,7 @@ struct CountArgs {
   int64_t n_ct;
   int lane_merge;  // lane tasks: members found by a two-pointer merge (1) or binary search (0)
   int64_t stride;  // task lists hold every stride-th task of the schedule (a shard of it), else 1
+  int claim;       // warp tasks (and groups of 32 lane tasks) taken from their cursor per atomic
   unsigned long long *cursor;     // [0] CTA, [1] warp, [2] lane task cursors
   unsigned long long *global;     // the total
   int64_t *pv;                    // per-vertex counts (per-vertex mode)
@@ -989,6 +990,38 @@ __device__ __forceinline__ Task claim_task(unsigned long long *cursor, const Tas
                                            int64_t stride, int lane) {
   unsigned long long i = 0;
   if (lane == 0) i = atomicAdd(cursor, 1ull);
+  i = __shfl_sync(0xffffffffu, i, 0);
+  if (int64_t(i) >= n) {
+    Task t;
+    t.k0 = t.r0 = 0;
+    t.v = t.nmem = t.lg_s = 0;
+    t.nrec = -1;
+    return t;
+  }
+  return tasks[int64_t(i) * stride];
+}
+
+// Warp tasks (and lane tasks, 32 heads a group) are claimed from their
+// global cursor `claim` at a time (lane 0 keeps the block), so the warps of
+// the whole GPU take one atomic on that one address per `claim` tasks. Where
+// tasks are many and small (the 4,096-graph batch: 38.2 -> 30.4 ms with 4)
+// that atomic is the limit; elsewhere a block lengthens the tail (R-MAT s22
+// 4.69 -> 4.79 ms with 4; s24 and Chung-Lu unchanged), so a plain graph
+// claims one at a time and a batch four (xt_graph_set_claim, the autotuner).
+struct ClaimBlock {
+  unsigned long long next = 0, end = 0;  // lane 0: the unclaimed rest of its block
+};
+__device__ __forceinline__ Task claim_task_block(ClaimBlock &cb, unsigned long long *cursor,
+                                                 const Task *__restrict__ tasks, int64_t n, int64_t stride, int claim,
+                                                 int lane) {
+  unsigned long long i = 0;
+  if (lane == 0) {
+    if (cb.next == cb.end) {
+      cb.next = atomicAdd(cursor, (unsigned long long)claim);
+      cb.end = cb.next + claim;
+    }
+    i = cb.next++;
+  }
   i = __shfl_sync(0xffffffffu, i, 0);
   if (int64_t(i) >= n) {
     Task t;
@@ -1170,6 +1203,7 @@ __global__ void __launch_bounds__(kThreads, MODE == 0 ? kMinBlocks : 3) k_count(
   }
 
   // ---- warp tasks: the CTA region split among the warps ----
+  ClaimBlock wclaim;
   if (MODE == 0 && kWarpCuckoo) {
     // The slice holds the CTA tasks' last set: zero it once. A task then
     // builds its bitmap or cuckoo table into the zeroed slice and, when done,
@@ -1177,7 +1211,7 @@ __global__ void __launch_bounds__(kThreads, MODE == 0 ? kMinBlocks : 3) k_count(
     // the whole 1,024-word slice per task.
     int32_t *wstage = s_stage + warp * kStageWarp;
     int32_t *words = bwords + warp * kWarpWords;
-    Task t = claim_task(&cursor[1], a.wt, a.n_wt, a.stride, lane);
+    Task t = claim_task_block(wclaim, &cursor[1], a.wt, a.n_wt, a.stride, a.claim, lane);
     int so = stage_task(wstage, col, rec, t, lane);
     zero_words(words, kWarpWords, lane, 32);
     while (true) {
@@ -1191,7 +1225,7 @@ __global__ void __launch_bounds__(kThreads, MODE == 0 ? kMinBlocks : 3) k_count(
       m.mcnt = nullptr;
       const bool ok = warp_set_build(m, mem, t.nmem, kWarpWords, a.bitmap_bits, a.cuckoo_iters, lane);
       __syncwarp();
-      const Task tn = claim_task(&cursor[1], a.wt, a.n_wt, a.stride, lane);  // read after the stream
+      const Task tn = claim_task_block(wclaim, &cursor[1], a.wt, a.n_wt, a.stride, a.claim, lane);  // read after the stream
       int64_t h;
       if (ok) {
         h = stream_suffixes<MODE, PF>(rec, a.rec_u, a.colp, t.k0, t.k0 + t.nrec, t.lg_s, nullptr, m, pv, es, off, a.poff, lane);
@@ -1219,7 +1253,7 @@ __global__ void __launch_bounds__(kThreads, MODE == 0 ? kMinBlocks : 3) k_count(
     }
   } else {
     int32_t *wstage = s_stage + warp * kStageWarp;
-    Task t = claim_task(&cursor[1], a.wt, a.n_wt, a.stride, lane);
+    Task t = claim_task_block(wclaim, &cursor[1], a.wt, a.n_wt, a.stride, a.claim, lane);
     int so = stage_task(wstage, col, rec, t, lane);
     while (true) {
       cp_async_wait_all();
@@ -1235,7 +1269,7 @@ __global__ void __launch_bounds__(kThreads, MODE == 0 ? kMinBlocks : 3) k_count(
       __syncwarp();
       for (int i = lane; i < t.nmem; i += 32) members_insert_at<PV>(m, mem, i);
       __syncwarp();
-      const Task tn = claim_task(&cursor[1], a.wt, a.n_wt, a.stride, lane);  // read after the stream
+      const Task tn = claim_task_block(wclaim, &cursor[1], a.wt, a.n_wt, a.stride, a.claim, lane);  // read after the stream
       int64_t h = stream_suffixes<MODE, PF>(rec, a.rec_u, a.colp, t.k0, t.k0 + t.nrec, t.lg_s, nullptr, m, pv, es, off, a.poff,
                                         lane);
       acc += h;
@@ -1273,9 +1307,18 @@ __global__ void __launch_bounds__(kThreads, MODE == 0 ? kMinBlocks : 3) k_count(
   constexpr int kLaneRegs = 8;
   auto lane_tasks = [&](auto merge_tag) {
     constexpr bool MERGE = decltype(merge_tag)::value;
+    // heads are claimed 32 * a.claim at a time (lane 0 keeps the block)
+    unsigned long long lnext = 0, lend = 0;
     while (true) {
       unsigned long long base = 0;
-      if (lane == 0) base = atomicAdd(&cursor[2], 32ull);
+      if (lane == 0) {
+        if (lnext == lend) {
+          lnext = atomicAdd(&cursor[2], 32ull * (unsigned long long)a.claim);
+          lend = lnext + 32ull * (unsigned long long)a.claim;
+        }
+        base = lnext;
+        lnext += 32;
+      }
       base = __shfl_sync(0xffffffffu, base, 0);
       if (int64_t(base) >= a.n_tt) break;
       const int64_t i = int64_t(base) + lane;
@@ -1848,6 +1891,7 @@ xt_status count_graph(Graph *g, int64_t *d_global, int64_t *d_pv, int64_t *d_gro
   a.ct = shard_first(pl->d_ct, pl->n_ctask, shard);
   a.n_ct = shard_len(pl->n_ctask, shard, nshards);
   a.stride = nshards;
+  a.claim = g->claim_block > 0 ? g->claim_block : (g->n_groups > 0 ? 4 : 1);
   a.lane_merge = g->lane_merge;
   a.cursor = pl->d_cursor;
   a.global = reinterpret_cast<unsigned long long *>(d_global);

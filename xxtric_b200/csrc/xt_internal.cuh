@@ -132,6 +132,7 @@ struct Graph {
   int cluster_tier = 0;         // global count: heads over a CTA's member set on thread-block clusters (1) or
                                 //   as CTA tasks over parts of their members (0, the default: faster)
   int cuckoo_iters = -1;        // test hook: cuckoo eviction chain limit (-1: the default)
+  int claim_block = 0;          // warp tasks taken per atomic on their cursor (0: 4 for a batch, else 1)
   int64_t tier_lane_work = -1;  // tier limits (-1: automatic, 0: tier off)
   int64_t tier_warp_work = -1;
   int32_t *d_group = nullptr;   // internal id -> group (graph of a batch), or null
