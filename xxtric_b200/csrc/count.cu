@@ -601,8 +601,18 @@ constexpr int64_t kMaxOutDegree = kMaxRecLen;  // and the in-records' length fie
 // consecutive pairs, so each load asks L2 for the 256 bytes around it (the
 // next steps' pairs) and skips L1, where a pair is never read twice (s22
 // 5.74 -> 5.62 ms, s24 32.02 -> 31.77 ms).
-__device__ __forceinline__ void load_pair(const int32_t *__restrict__ col, int64_t P, int4 &a, int4 &b) {
-  const int32_t *p = col + 8 * P;
+// Pair indices fit 32 bits (the padded columns number below 2^35): a lane
+// steps its pair index and forms the address with 32-bit arithmetic
+#ifndef XT_P32
+#define XT_P32 1
+#endif
+#if XT_P32
+using PairIdx = uint32_t;
+#else
+using PairIdx = int64_t;
+#endif
+__device__ __forceinline__ void load_pair(const int32_t *__restrict__ col, PairIdx P, int4 &a, int4 &b) {
+  const int32_t *p = col + (uint64_t(P) << 3);
   asm volatile("ld.global.nc.L1::no_allocate.L2::256B.v8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
                : "=r"(a.x), "=r"(a.y), "=r"(a.z), "=r"(a.w), "=r"(b.x), "=r"(b.y), "=r"(b.z), "=r"(b.w)
                : "l"(p));
@@ -825,7 +835,7 @@ __device__ __forceinline__ int64_t stream_kind(const InRec *__restrict__ rec, co
     const int32_t np = len > 0 ? (int32_t(s & 7) + len + 7) >> 3 : 0;  // pairs of the suffix
     const int32_t cnt = np > k ? ((np - k + S - 1) >> lg_s) : 0;            // this lane's
     const int32_t steps = int32_t(__reduce_max_sync(0xffffffffu, uint32_t(cnt)));
-    int64_t P = (s >> 3) + k;
+    PairIdx P = PairIdx(uint32_t(r4.x)) + PairIdx(k);  // r4.x = s >> 3
     int4 xa = sent, xb = sent;
     if (cnt > 0) load_pair(colp, P, xa, xb);
     int h = 0;
@@ -833,10 +843,10 @@ __device__ __forceinline__ int64_t stream_kind(const InRec *__restrict__ rec, co
     // each lane runs its own pairs and leaves the loop after its last one
     for (int32_t it = 0; it < cnt; it++) {
       const int4 a = xa, b = xb;
-      const int64_t pa = P;  // the pair in a, b
+      const PairIdx pa = P;  // the pair in a, b
       P += S;
       if (it + 1 < cnt) load_pair(colp, P, xa, xb);  // next step's pair in flight during the probes
-      if (PV) h += probe_pair_counted<MODE, KIND>(a, b, m, es, 8 * pa);
+      if (PV) h += probe_pair_counted<MODE, KIND>(a, b, m, es, 8 * int64_t(pa));
       else h += probe_pair<false, KIND>(a, b, m);
     }
     (void)steps;
@@ -844,18 +854,18 @@ __device__ __forceinline__ int64_t stream_kind(const InRec *__restrict__ rec, co
     // a lane past its last pair probes sentinels
     for (int32_t it = 0; it < steps; it++) {
       const int4 a = xa, b = xb;
-      const int64_t pa = P;  // the pair in a, b
+      const PairIdx pa = P;  // the pair in a, b
       P += S;
       if (it + 1 < cnt) {
         load_pair(colp, P, xa, xb);  // next step's pair in flight during the probes
 #if XT_PF_DIST > 1
-        if (it + XT_PF_DIST < cnt) prefetch_line_l2(colp + 8 * (P + int64_t(XT_PF_DIST - 1) * S));
+        if (it + XT_PF_DIST < cnt) prefetch_line_l2(colp + 8 * (int64_t(P) + int64_t(XT_PF_DIST - 1) * S));
 #endif
       } else {
         xa = sent;
         xb = sent;
       }
-      if (PV) h += probe_pair_counted<MODE, KIND>(a, b, m, es, 8 * pa);
+      if (PV) h += probe_pair_counted<MODE, KIND>(a, b, m, es, 8 * int64_t(pa));
       else h += probe_pair<false, KIND>(a, b, m);
     }
 #endif
